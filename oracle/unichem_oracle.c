@@ -1,0 +1,783 @@
+/*
+ * ORACLE (test infrastructure only) -- FP64 CPU restatement of UNICORN's
+ * per-cell chemistry and property hot path.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+ * this file, as the checker. The product (unicorn_b200/csrc) never links it.
+ *
+ * It follows the reference's evaluation order so that its results can be
+ * compared bit for bit with the reference routines themselves (translated
+ * mechanically to C under oracle/_ref by oracle/build_ref.py):
+ *   orc_setup            src/unicornd-mild-sd-5.f:327-483 (tables and scales)
+ *   orc_rates            src/lib/ckrates.f:92-1352        (CKRATES, per cell)
+ *   orc_omega            src/lib/solveh.f:39-57,116-1145  (h_k, RA, PRD, QDSP, QDOT)
+ *   orc_cp               src/lib/spgsolv.f:102-173        (mixture cp, TCP)
+ *   orc_props            src/unicornd-mild-sd-5.f:821-1006 (Y clip, mu, lambda, D_k)
+ *   orc_species_update   src/lib/solvesp.f:82-2915        (point-implicit update)
+ *   orc_temperature      src/lib/solveh.f:1170-1234       (T from h, Newton)
+ * The mechanism arrives as flat tables built from the reference sources by
+ * unicorn_b200/mech/extract.py and packed by oracle/oracle.py.
+ *
+ * Literal constants keep their Fortran kind: a default-REAL literal such as
+ * 82.06 in the reference is the single-precision value promoted to double,
+ * written here as F(82.06).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define LSP 52
+#define LRX 544
+#define F(x) ((double)(float)(x))
+
+/* ------------------------------------------------------------- tables */
+
+/* factor kinds of the product chains in the packed program tables */
+enum { FK_NUM = 0, FK_A = 1, FK_RC = 2, FK_Y = 3, FK_Y0 = 4, FK_SOUR = 5, FK_RA = 6, FK_SRA = 7 };
+
+typedef struct {
+    /* species data (1-based species numbers are stored 0-based here) */
+    const double *wsp, *cdia, *tlj;     /* [52] */
+    const double *poly;                 /* [52][14] NASA coefficients, POLSP(14,LSP) */
+    const double *om22;                 /* [52][12] Omega(2,2) fits, CISP(12,LSP) */
+    const double *ci11;                 /* [4][5]  CI11(4,5) stored row-major [K][n] */
+    double tpol1, tpol2;
+    /* reactions, raw DATA values (Ea in cal/mol) */
+    const double *akf, *alf, *exaf, *aklow, *allow, *ealow, *troe; /* troe [544][4] */
+    /* reverse formulas for even slots: rut (-1,0,+1), q chain (op, species) */
+    const int *rev_has, *rev_rut, *rev_off, *rev_len, *rev_op, *rev_sp;
+    /* third-body groups: g=0 TBODY, g=1..10 TB001..TB010 */
+    const int *tb_off, *tb_len, *tb_sign, *tb_sp; const double *tb_coef; const int *tb_hascoef;
+    const int *dmole_grp;               /* [544] group used by DMOLE (0 = TBODY) */
+    /* RC assembly */
+    const int *rc_has, *rc_order, *rc_tb, *rc_off, *rc_len, *rc_op, *rc_kind, *rc_idx;
+    /* SOLVEH: RA reactant lists, PRD term lists */
+    const int *ra_has, *ra_off, *ra_len, *ra_sp;
+    const int *prd_has, *prd_off, *prd_len;         /* per species, terms */
+    /* generic term store: term t has sign term_sign[t] and factors
+       [term_foff[t], term_foff[t]+term_flen[t]) in (fac_kind, fac_idx, fac_val) */
+    const int *term_sign, *term_foff, *term_flen;
+    const int *fac_kind, *fac_idx; const double *fac_val;
+    /* SOLVESP blocks (species 1..51): recompute (r, factor list), sums, multiplies */
+    const int *blk_rec_off, *blk_rec_len, *rec_r, *rec_foff, *rec_flen;
+    const int *blk_prod_has, *blk_prod_off, *blk_prod_len;
+    const int *blk_extra_off, *blk_extra_len;
+    const int *blk_loss_has, *blk_loss_off, *blk_loss_len;
+    const int *blk_mul_off, *blk_mul_len, *mul_r;
+    /* loss lists used for d(omega)/dY: from the PRD negative RA terms */
+} orc_tables;
+
+typedef struct {
+    double RTIN, RTOT, VREF, TREF, PREF, RREF, FO2IN;
+} orc_inputs;
+
+typedef struct {
+    /* /CB06/ scales and derived constants (src/unicornd-mild-sd-5.f:421-459) */
+    double ALSTR, VSTR, RSTR, PSTR, TSTR, TMSTR, AMSTR, ACSTR, DSTR, HSTR, CPSTR, AKSTR, EPSTR,
+           WMSTR, GASC, BETA1, BETA2, BETA3, BETA4, REI, PBACK, HCONV, CONVRC, CONVRM, CONVRD;
+    double WM[LSP], HFO[LSP];
+    double AKF[LRX], ALF[LRX], EXAF[LRX], AKLOW[LRX], ALLOW[LRX], EALOW[LRX], TROE[LRX][4];
+    int NRLIND, LREV;
+    double WMIK[LSP][LSP], DWMIK[LSP][LSP], WMCD[LSP][LSP];
+    double ETLJ1[LSP][LSP], ETLJ2[LSP][LSP], ETLJ3[LSP][LSP], ETLJ4[LSP][LSP];
+} orc_state;
+
+static orc_tables T;
+static orc_state S;
+
+/* ------------------------------------------------------------- set-up */
+
+/* src/unicornd-mild-sd-5.f:327-483: unit conversions, reverse slots,
+ * reference scales, non-dimensional molar masses, formation enthalpies and
+ * pair constants of the transport model. All reactions switched on (IRSW=1). */
+int orc_setup(const orc_tables *tab, const orc_inputs *in, double *scales_out)
+{
+    T = *tab;
+    const double RUCAL = F(1.9872), GASC = F(8.3144), GAMA = F(1.4);
+    S.LREV = 2;
+    S.NRLIND = 0;
+    for (int r = 0; r < LRX; ++r) {
+        S.AKF[r] = T.akf[r]; S.ALF[r] = T.alf[r]; S.EXAF[r] = T.exaf[r];
+        S.AKLOW[r] = T.aklow[r]; S.ALLOW[r] = T.allow[r]; S.EALOW[r] = T.ealow[r];
+        for (int c = 0; c < 4; ++c) S.TROE[r][c] = T.troe[r * 4 + c];
+    }
+    for (int i = 0; i < LRX; i += 2) {          /* DO 10 I=1,LRX,LREV  (main:364-413) */
+        S.EXAF[i] = S.EXAF[i] / RUCAL;
+        if (S.AKF[i] < 0) {
+            S.NRLIND += 1;
+            S.AKF[i] = -S.AKF[i];
+            S.EALOW[i] = S.EALOW[i] / RUCAL;
+        } else {
+            S.EALOW[i] = 0.0; S.AKLOW[i] = 0.0; S.ALLOW[i] = 0.0;
+            for (int c = 0; c < 4; ++c) S.TROE[i][c] = 0.0;
+        }
+        S.AKF[i + 1] = 1.0;
+        S.EXAF[i + 1] = 0.0; S.ALF[i + 1] = 0.0; S.EALOW[i + 1] = 0.0; S.AKLOW[i + 1] = 0.0;
+        S.ALLOW[i + 1] = 0.0;
+        for (int c = 0; c < 4; ++c) S.TROE[i + 1][c] = 0.0;
+    }
+    /* freestream properties and scales (main:421-453) */
+    double WMREF = 1.0 / (in->FO2IN / T.wsp[1] + (1.0 - in->FO2IN) / T.wsp[LSP - 1]) / 1000.0;
+    double AMREF = 5.69428e-07 * pow(in->TREF, F(0.62245));
+    double ACREF = 2.78763e-04 * pow(in->TREF, F(0.796783));
+    double DREF = 1.2e-04;
+    double RREF = in->PREF / (GASC / WMREF) / in->TREF;
+    S.GASC = GASC;
+    S.ALSTR = in->RTOT - in->RTIN;
+    S.VSTR = in->VREF;
+    S.RSTR = RREF;
+    S.PSTR = RREF * in->VREF * in->VREF;
+    S.PBACK = in->PREF / S.PSTR;
+    S.TSTR = in->TREF;
+    S.HSTR = in->VREF * in->VREF;
+    S.AKSTR = in->VREF * in->VREF;
+    S.EPSTR = in->VREF * in->VREF * in->VREF / S.ALSTR;
+    S.CPSTR = in->VREF * in->VREF / in->TREF;
+    S.ACSTR = ACREF;
+    S.TMSTR = S.ALSTR / in->VREF;
+    S.AMSTR = AMREF;
+    S.DSTR = DREF;
+    S.WMSTR = WMREF;
+    S.REI = AMREF / RREF / in->VREF / S.ALSTR;
+    S.BETA1 = GASC * S.RSTR * S.TSTR / S.PSTR / S.WMSTR;
+    S.BETA2 = S.TSTR * S.ACSTR / S.AMSTR / S.VSTR / S.VSTR;
+    S.BETA3 = S.RSTR * S.DSTR / S.AMSTR;
+    S.BETA4 = 0.0;
+    S.HCONV = GASC / S.WMSTR / S.HSTR;
+    /* main:457-459 */
+    S.CONVRC = F(418.68) * 1.9891e-04 * sqrt(S.TSTR / 1000.0 / S.WMSTR) / S.ACSTR;
+    S.CONVRM = F(0.1) * 2.6693e-05 * sqrt(1000.0 * S.WMSTR * S.TSTR) / S.AMSTR;
+    S.CONVRD = F(0.02628) * S.TSTR * sqrt(S.TSTR) / S.PSTR / sqrt(S.WMSTR * 1000.0) / S.DSTR;
+    /* main:461-464 */
+    for (int k = 0; k < LSP; ++k) {
+        S.WM[k] = T.wsp[k] / 1000.0 / S.WMSTR;
+        S.HFO[k] = S.HCONV * T.poly[k * 14 + 5] / S.WM[k];
+    }
+    /* main:471-483 pair constants */
+    for (int i = 0; i < LSP; ++i)
+        for (int j = 0; j < LSP; ++j) {
+            S.WMIK[i][j] = pow(S.WM[i] / S.WM[j], F(0.25));
+            if (i == j) S.WMIK[i][j] = sqrt(S.WM[i]);
+            S.DWMIK[i][j] = F(2.828427125) * sqrt(1.0 + S.WM[i] / S.WM[j]);
+            double ECDIA = F(0.5) * (T.cdia[i] + T.cdia[j]);
+            S.WMCD[i][j] = sqrt((S.WM[i] + S.WM[j]) / 2.0 / S.WM[i] / S.WM[j]) / ECDIA / ECDIA;
+            S.ETLJ1[i][j] = sqrt(T.tlj[i] * T.tlj[j]);
+            S.ETLJ2[i][j] = S.ETLJ1[i][j] * S.ETLJ1[i][j];
+            S.ETLJ3[i][j] = S.ETLJ2[i][j] * S.ETLJ1[i][j];
+            S.ETLJ4[i][j] = S.ETLJ3[i][j] * S.ETLJ1[i][j];
+        }
+    if (scales_out) {
+        double v[] = {S.ALSTR, S.VSTR, S.RSTR, S.PSTR, S.TSTR, S.TMSTR, S.AMSTR, S.ACSTR, S.DSTR,
+                      S.HSTR, S.CPSTR, S.AKSTR, S.EPSTR, S.WMSTR, S.GASC, S.BETA1, S.BETA2,
+                      S.BETA3, S.BETA4, S.REI, S.PBACK, S.HCONV, S.CONVRC, S.CONVRM, S.CONVRD};
+        memcpy(scales_out, v, sizeof(v));
+    }
+    return 0;
+}
+
+void orc_get_tables(double *wm, double *hfo, double *akf, double *exaf, double *ealow,
+                    double *pair /* [7][52][52] */)
+{
+    memcpy(wm, S.WM, sizeof(S.WM));
+    memcpy(hfo, S.HFO, sizeof(S.HFO));
+    memcpy(akf, S.AKF, sizeof(S.AKF));
+    memcpy(exaf, S.EXAF, sizeof(S.EXAF));
+    memcpy(ealow, S.EALOW, sizeof(S.EALOW));
+    memcpy(pair + 0 * LSP * LSP, S.WMIK, sizeof(S.WMIK));
+    memcpy(pair + 1 * LSP * LSP, S.DWMIK, sizeof(S.DWMIK));
+    memcpy(pair + 2 * LSP * LSP, S.WMCD, sizeof(S.WMCD));
+    memcpy(pair + 3 * LSP * LSP, S.ETLJ1, sizeof(S.ETLJ1));
+    memcpy(pair + 4 * LSP * LSP, S.ETLJ2, sizeof(S.ETLJ2));
+    memcpy(pair + 5 * LSP * LSP, S.ETLJ3, sizeof(S.ETLJ3));
+    memcpy(pair + 6 * LSP * LSP, S.ETLJ4, sizeof(S.ETLJ4));
+}
+
+/* ------------------------------------------------------------- CKRATES */
+
+typedef struct {
+    double sprf[LRX];
+    double rc[LRX];
+    double sour[6];
+    double tbody;
+} cell_rates;
+
+static double tb_value(int g, const double *y, double tbody)
+{
+    /* ckrates.f:706-731 TBnnn = TBODY + sum(coef*Y/W) (left to right) */
+    int o = T.tb_off[g], n = T.tb_len[g];
+    double acc = tbody;
+    for (int t = 0; t < n; ++t) {
+        int k = T.tb_sp[o + t];
+        double term = T.tb_hascoef[o + t] ? (T.tb_coef[o + t] * y[k]) / S.WM[k] : y[k] / S.WM[k];
+        acc = T.tb_sign[o + t] > 0 ? acc + term : acc - term;
+    }
+    return acc;
+}
+
+/* ckrates.f:92-1352 for one cell; y[k] are the 52 mass fractions */
+static void rates_cell(double tk, double rho, const double *y, double stmf, double stnd,
+                       cell_rates *o)
+{
+    double *SPRF = o->sprf;
+    memset(SPRF, 0, sizeof(o->sprf));       /* slots never written stay 0 (static local) */
+    const double C1ST = S.ALSTR / S.VSTR;
+    const double C2ND = S.ALSTR / S.VSTR * (S.RSTR / S.WMSTR * 1.0e-06);
+    const double C3RD = S.ALSTR / S.VSTR * (S.RSTR * S.RSTR / S.WMSTR / S.WMSTR * 1.0e-12);
+    double TKD = tk * S.TSTR;
+    double ELOGT = log(TKD);
+    /* forward specific rates, ckrates.f:95-101 */
+    for (int ir = 0; ir < LRX; ir += S.LREV) {
+        double ACTV = S.ALF[ir] * ELOGT - S.EXAF[ir] / TKD;
+        SPRF[ir] = S.AKF[ir] * exp(ACTV);
+    }
+    /* Gibbs functions, ckrates.f:103-115 */
+    double TKD1 = TKD / 2.0;
+    double TKD2 = TKD * TKD / 6.0;
+    double TKD3 = TKD1 * TKD2;
+    double TKD4 = F(1.2) * TKD1 * TKD3;
+    int ip = TKD > T.tpol1 ? 7 : 0;
+    double GSP[LSP];
+    for (int k = 0; k < LSP; ++k) {
+        const double *a = T.poly + k * 14 + ip;
+        double g0 = a[0] * (ELOGT - 1.0) + a[1] * TKD1 + a[2] * TKD2 + a[3] * TKD3 + a[4] * TKD4
+                    - a[5] / TKD + a[6];
+        GSP[k] = exp(g0);
+    }
+    double RUT = F(82.06) * TKD;
+    /* reverse rates, ckrates.f:116-642: k_r = AKF*k_f [/RUT|*RUT] / q */
+    for (int r = 1; r < LRX; r += 2) {
+        if (!T.rev_has[r]) continue;        /* Q1: SPRF(116),(254),(472),(502..) never set */
+        int o2 = T.rev_off[r], n = T.rev_len[r];
+        double q = GSP[T.rev_sp[o2]];
+        for (int t = 1; t < n; ++t)
+            q = T.rev_op[o2 + t] == '*' ? q * GSP[T.rev_sp[o2 + t]] : q / GSP[T.rev_sp[o2 + t]];
+        double v = S.AKF[r] * SPRF[r - 1];
+        if (T.rev_rut[r] < 0) v = v / RUT;
+        else if (T.rev_rut[r] > 0) v = v * RUT;
+        SPRF[r] = v / q;
+    }
+    /* third bodies, ckrates.f:643-731 */
+    double RHO1 = rho, RHO2 = rho * rho, RHO3 = rho * rho * rho;
+    double TBODY = y[0] / S.WM[0];
+    for (int k = 1; k < LSP; ++k) TBODY = TBODY + y[k] / S.WM[k];
+    double TB[11];
+    TB[0] = TBODY;
+    for (int g = 1; g <= 10; ++g) TB[g] = tb_value(g, y, TBODY);
+    o->tbody = TBODY;
+    /* fall-off blending, ckrates.f:740-794 */
+    if (S.NRLIND != 0) {
+        double DMOLEA = rho * S.RSTR / S.WMSTR * 1.0e-06;
+        for (int ir = 0; ir < LRX; ir += S.LREV) {
+            double DMOLE = TB[T.dmole_grp[ir]] * DMOLEA;
+            if (S.AKLOW[ir] == 0.0) continue;
+            const double *TR = S.TROE[ir];
+            if (S.AKLOW[ir] < 0.0) {            /* Tseng form (no reaction of this data uses it) */
+                double AK0M = pow(10.0, TR[0] + (TR[1] + (TR[2] + TR[3] * TKD) * TKD) * TKD) * DMOLE;
+                double AFP = AK0M / (1.0 + AK0M);
+                SPRF[ir] = AFP * SPRF[ir];
+                SPRF[ir + 1] = AFP * SPRF[ir + 1];
+                continue;
+            }
+            double ACTV = S.ALLOW[ir] * ELOGT - S.EALOW[ir] / TKD;
+            double AK0M = S.AKLOW[ir] * exp(ACTV) * DMOLE / (SPRF[ir] + 1.0e-20);
+            double RFACT;
+            if (TR[0] > 0.0) {
+                double FCLOG;
+                if (TR[1] == 0.0) FCLOG = log10(TR[0]);
+                else FCLOG = log10((1.0 - TR[0]) * exp(-(TKD / TR[1])) + TR[0] * exp(-(TKD / TR[2]))
+                                   + exp(-(TR[3] / TKD)));   /* Q2: exp(-T4/T) always added */
+                double CPLOG = log10(AK0M) - (F(0.4) + F(0.67) * FCLOG);
+                double z = CPLOG / (F(0.75) - F(1.27) * FCLOG - F(0.14) * CPLOG);
+                RFACT = pow(10.0, FCLOG / (1.0 + z * z));
+            } else if (TR[0] == 0.0) {
+                RFACT = 1.0;
+            } else {                             /* SRI form */
+                double l = log10(AK0M);
+                double XFACT = 1.0 / (1.0 + l * l);
+                RFACT = pow(-(TR[0] * exp(-(TR[1] / TKD))) + exp(-(TKD / TR[2])), XFACT);
+            }
+            double AFP = (AK0M / (1.0 + AK0M)) * RFACT;
+            SPRF[ir] = AFP * SPRF[ir];
+            SPRF[ir + 1] = AFP * SPRF[ir + 1];
+        }
+    }
+    /* rate-coefficient plane, ckrates.f:796-1333 */
+    const double CC[4] = {0, C1ST, C2ND, C3RD};
+    const double RR[4] = {0, RHO1, RHO2, RHO3};
+    for (int r = 0; r < LRX; ++r) {
+        if (!T.rc_has[r]) { o->rc[r] = 0.0; continue; }   /* slots 502..518: zero COMMON */
+        int od = T.rc_order[r];
+        double v = CC[od] * RR[od];
+        if (T.rc_tb[r] >= 0) v = v * TB[T.rc_tb[r]];
+        v = v * SPRF[r];
+        int oo = T.rc_off[r];
+        for (int t = 0; t < T.rc_len[r]; ++t) {
+            int k = T.rc_idx[oo + t];
+            if (T.rc_kind[oo + t] == FK_Y) v = v * y[k];
+            else v = v / S.WM[k];
+        }
+        o->rc[r] = v;
+    }
+    /* soot source terms, ckrates.f:1337-1352 */
+    {
+        const double PI = 3.1415927e+00, RSOOT = 1.9000e+03, SIGB = 1.38e-23, AVNO = 6.0232e+23;
+        const double CMIN = F(100.0), CAGL = F(9.0);
+        const double AKST1 = 1.000e+04, EAST1 = 2.0632e+04, AKST2 = 3.468e+03, EAST2 = 1.2077e+04;
+        const double AKST3 = 1.000e+04, ALST3 = F(0.5), EAST3 = 1.9626e+04;
+        const double AKST4 = 1.060e+02, ALST4 = F(-0.5), EAST4 = F(0.0);
+        const double AKST5 = 5.54e+00, ALST5 = F(-0.5), EAST5 = F(0.0);
+        double DPST = 0.0;
+        if (stnd >= 1.0) DPST = pow(6.0 * stmf / (PI * RSOOT * stnd), F(0.333333));
+        double ASST = PI * DPST * DPST * S.RSTR * rho * stnd;
+        double SOURNU = C1ST * RHO1 * AKST1 * exp(-(EAST1 / TKD)) / S.WM[21];
+        o->sour[0] = SOURNU + C1ST * RHO1 * ASST * AKST2 * exp(-(EAST2 / TKD)) / S.WM[21];
+        o->sour[1] = 2.0 * SOURNU * AVNO / CMIN / S.WMSTR;
+        o->sour[2] = C1ST * RHO1 * ASST * AKST3 * pow(TKD, ALST3) * exp(-(EAST3 / TKD)) / S.WM[1];
+        o->sour[3] = F(0.13) * C1ST * ASST * AKST4 * pow(TKD, ALST4) * exp(-(EAST4 / TKD)) / S.WM[4] / TBODY;
+        o->sour[4] = F(0.5) * C1ST * ASST * AKST5 * pow(TKD, ALST5) * exp(-(EAST5 / TKD)) / S.WM[3] / TBODY;
+        o->sour[5] = 2.0 * C1ST * S.RSTR * CAGL * sqrt(DPST * 6.0 * SIGB * TKD / RSOOT) * rho * rho * stnd;
+    }
+}
+
+/* n cells, SoA inputs: y[k*n + c]. Outputs rc[r*n + c], sour[m*n + c]. */
+void orc_rates(int n, const double *tk, const double *rho, const double *y, const double *stmf,
+               const double *stnd, double *rc, double *sour)
+{
+    cell_rates cr;
+    double yc[LSP];
+    for (int c = 0; c < n; ++c) {
+        for (int k = 0; k < LSP; ++k) yc[k] = y[(size_t)k * n + c];
+        rates_cell(tk[c], rho[c], yc, stmf ? stmf[c] : 0.0, stnd ? stnd[c] : 0.0, &cr);
+        if (rc) for (int r = 0; r < LRX; ++r) rc[(size_t)r * n + c] = cr.rc[r];
+        if (sour) for (int m = 0; m < 6; ++m) sour[(size_t)m * n + c] = cr.sour[m];
+    }
+}
+
+/* ------------------------------------------------------------- products */
+
+/* value of a product chain; A = current A-terms, RA = reaction rates */
+static double chain_value(int foff, int flen, const double *A, const double *RC, const double *Y,
+                          const double *Y0, const double *SOUR, const double *RA)
+{
+    double v = 0.0;
+    for (int f = 0; f < flen; ++f) {
+        int kd = T.fac_kind[foff + f], ix = T.fac_idx[foff + f];
+        double x;
+        switch (kd) {
+        case FK_NUM: x = T.fac_val[foff + f]; break;
+        case FK_A: x = A[ix]; break;
+        case FK_RC: x = RC[ix]; break;
+        case FK_Y: x = Y[ix]; break;
+        case FK_Y0: x = Y0[ix]; break;
+        case FK_SOUR: x = SOUR[ix]; break;
+        case FK_RA: x = RA[ix]; break;
+        default: x = 0.0; break;           /* FK_SRA: SRA(1..6)=0.0, solveh.f:671-676 */
+        }
+        v = f == 0 ? x : v * x;
+    }
+    return v;
+}
+
+static double sum_terms(int off, int len, const double *A, const double *RC, const double *Y,
+                        const double *Y0, const double *SOUR, const double *RA)
+{
+    double acc = 0.0;
+    for (int t = 0; t < len; ++t) {
+        int ti = off + t;
+        double v = chain_value(T.term_foff[ti], T.term_flen[ti], A, RC, Y, Y0, SOUR, RA);
+        if (t == 0) acc = T.term_sign[ti] > 0 ? v : -v;
+        else acc = T.term_sign[ti] > 0 ? acc + v : acc - v;
+    }
+    return acc;
+}
+
+/* ------------------------------------------------------------- SOLVEH rates */
+
+static void henth_cell(double tk, double *henth)
+{
+    /* solveh.f:39-57 */
+    double HCONVR = S.GASC / S.WMSTR / S.HSTR;
+    double TKD = tk * S.TSTR;
+    double TKD2 = TKD * TKD, TKD3 = TKD * TKD2, TKD4 = TKD * TKD3, TKD5 = TKD * TKD4;
+    int ip = TKD > T.tpol1 ? 7 : 0;
+    for (int k = 0; k < LSP; ++k) {
+        const double *a = T.poly + k * 14 + ip;
+        double HSSP = (a[0] * TKD + a[1] * TKD2 / 2.0 + a[2] * TKD3 / 3.0 + a[3] * TKD4 / 4.0
+                       + a[4] * TKD5 / 5.0) / S.WM[k] * HCONVR;
+        henth[k] = HSSP * S.WMSTR * S.HSTR + a[5] / S.WM[k] * S.GASC;
+    }
+}
+
+/* CKRATES followed by SOLVEH's rate part (solveh.f:116-1145) per cell.
+ * qdsp[k*n+c] = -RCONV*PRD/HFO (the reference's sign: minus omega),
+ * qdot[c] = -HRR*RCONV, henth[k*n+c] species enthalpies, and
+ * domega_dy[k*n+c] = -RCONV*W_k*L_k, the diagonal linearisation of omega_k
+ * (L_k = sum of the loss rate terms of PRD(k) with one Y_k factored out). */
+void orc_omega(int n, const double *tk, const double *rho, const double *y, const double *stmf,
+               const double *stnd, double *qdsp, double *qdot, double *henth, double *domega_dy)
+{
+    cell_rates cr;
+    double yc[LSP], RA[LRX], H[LSP], PRD[LSP];
+    const double RCONV = S.VSTR / S.WMSTR / S.ALSTR * 1.0e-06;
+    for (int c = 0; c < n; ++c) {
+        for (int k = 0; k < LSP; ++k) yc[k] = y[(size_t)k * n + c];
+        rates_cell(tk[c], rho[c], yc, stmf ? stmf[c] : 0.0, stnd ? stnd[c] : 0.0, &cr);
+        henth_cell(tk[c], H);
+        for (int r = 0; r < LRX; ++r) {     /* solveh.f:116-664 RA(r)=RC*Y*Y... */
+            if (!T.ra_has[r]) { RA[r] = 0.0; continue; }
+            double v = cr.rc[r];
+            for (int t = 0; t < T.ra_len[r]; ++t) v = v * yc[T.ra_sp[T.ra_off[r] + t]];
+            RA[r] = v;
+        }
+        for (int k = 0; k < LSP; ++k) {     /* solveh.f:677-1133 */
+            if (!T.prd_has[k]) { PRD[k] = 0.0; continue; }
+            double s = sum_terms(T.prd_off[k], T.prd_len[k], NULL, cr.rc, yc, NULL, cr.sour, RA);
+            PRD[k] = S.WM[k] * S.HFO[k] * s;
+        }
+        double HRR = 0.0;
+        for (int k = 0; k < LSP; ++k) {     /* solveh.f:1134-1140 */
+            HRR = HRR + PRD[k] * H[k] / S.HFO[k];
+            if (qdsp) qdsp[(size_t)k * n + c] = -(RCONV * PRD[k] / S.HFO[k]);
+            if (henth) henth[(size_t)k * n + c] = H[k];
+        }
+        if (qdot) qdot[c] = -(HRR * RCONV);
+        if (domega_dy) {
+            for (int k = 0; k < LSP; ++k) {
+                double L = 0.0;
+                if (T.prd_has[k]) {
+                    int o = T.prd_off[k];
+                    for (int t = 0; t < T.prd_len[k]; ++t) {
+                        int ti = o + t;
+                        if (T.term_sign[ti] > 0) continue;
+                        /* loss term -RA(r): RC(r) times the reactants but one Y_k */
+                        int fo = T.term_foff[ti];
+                        if (T.fac_kind[fo + T.term_flen[ti] - 1] != FK_RA) continue;
+                        int r = T.fac_idx[fo + T.term_flen[ti] - 1];
+                        double v = cr.rc[r];
+                        int skipped = 0;
+                        for (int q = 0; q < T.ra_len[r]; ++q) {
+                            int sp = T.ra_sp[T.ra_off[r] + q];
+                            if (sp == k && !skipped) { skipped = 1; continue; }
+                            v = v * yc[sp];
+                        }
+                        L = L + v;
+                    }
+                }
+                domega_dy[(size_t)k * n + c] = -(RCONV * S.WM[k] * L);
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------- cp, h */
+
+/* spgsolv.f:102-173: TCP, the non-dimensional mixture cp */
+void orc_cp(int n, const double *tk, const double *y, double *cp)
+{
+    for (int c = 0; c < n; ++c) {
+        double TKD = tk[c] * S.TSTR;
+        double TKD2 = TKD * TKD, TKD3 = TKD * TKD2, TKD4 = TKD * TKD3;
+        int ip = TKD > T.tpol1 ? 7 : 0;
+        double TCP = 0.0;
+        for (int k = 0; k < LSP; ++k) {
+            const double *a = T.poly + k * 14 + ip;
+            double t = (a[0] + a[1] * TKD + a[2] * TKD2 + a[3] * TKD3 + a[4] * TKD4) / S.WM[k];
+            TCP = TCP + t * y[(size_t)k * n + c];
+        }
+        cp[c] = TCP / S.WMSTR * S.GASC * S.TSTR / S.HSTR;
+    }
+}
+
+/* species enthalpies (solveh.f:39-57) and the mixture value sum_k Y_k h_k */
+void orc_enthalpy(int n, const double *tk, const double *y, double *henth, double *hmix)
+{
+    double H[LSP];
+    for (int c = 0; c < n; ++c) {
+        henth_cell(tk[c], H);
+        double s = 0.0;
+        for (int k = 0; k < LSP; ++k) {
+            if (henth) henth[(size_t)k * n + c] = H[k];
+            s = s + y[(size_t)k * n + c] * H[k];
+        }
+        if (hmix) hmix[c] = s;
+    }
+}
+
+/* ------------------------------------------------------------- transport */
+
+static double ci11t(int K, double TKDS, double TKD2, double TKD3, double TKD4, int i, int j)
+{
+    const double *c = T.ci11 + K * 5;
+    return c[0] + c[1] * TKDS + c[2] * TKD2 / S.ETLJ2[i][j] + c[3] * TKD3 / S.ETLJ3[i][j]
+           + c[4] * TKD4 / S.ETLJ4[i][j];
+}
+
+static int ci_range(double TKDS)
+{
+    int K = 0;
+    if (TKDS >= 2.0) K = 1;
+    if (TKDS > 5.0) K = 2;
+    if (TKDS > 70.0) K = 3;
+    return K;
+}
+
+/* main:821-1006 for n cells. y is clipped in place (Y<0 -> 0, N2 = 1 - sum).
+ * Outputs are the reference's non-dimensional VMU, VTC and VDFSP. nsub[c]
+ * (optional) receives the sub-mixture size LSPT. */
+void orc_props(int n, const double *tk, double *y, double *vmu, double *vtc, double *vdf,
+               int *nsub)
+{
+    const double FLMT = 1.0e-03;
+    int ISPQ[LSP], ISPQR[LSP + 1];
+    double XSP[LSP], ATC[LSP], AMU[LSP], PHIK[LSP], PHDIK[LSP], EFDIK[LSP], VDFQ[LSP];
+    static double DIF[LSP][LSP];   /* DIFSP: diagonal never assigned (static zero) */
+    for (int c = 0; c < n; ++c) {
+        double yc[LSP];
+        for (int k = 0; k < LSP; ++k) yc[k] = y[(size_t)k * n + c];
+        /* main:821-828 */
+        double TMASS = 0.0;
+        for (int k = 0; k < LSP - 1; ++k) {
+            if (yc[k] < 0.0) yc[k] = 0.0;
+            TMASS = TMASS + yc[k];
+        }
+        yc[LSP - 1] = 1.0 - TMASS;
+        for (int k = 0; k < LSP; ++k) y[(size_t)k * n + c] = yc[k];
+        /* sub-mixture, main:842-915 */
+        int IA = 0;
+        TMASS = 0.0;
+        double TMOLE = 0.0;
+        for (int k = 0; k < LSP - 1; ++k) {
+            ISPQ[k] = -1;
+            if (yc[k] < FLMT) continue;
+            ISPQ[k] = IA;
+            ISPQR[IA] = k;
+            TMASS = TMASS + yc[k];
+            XSP[IA] = yc[k] / S.WM[k];
+            TMOLE = TMOLE + XSP[IA];
+            IA += 1;
+        }
+        ISPQ[LSP - 1] = -1;                /* ISPQ(LSP) is never assigned (static 0) */
+        int LSPT = IA + 1;
+        if (LSPT >= LSP) LSPT = LSP;
+        ISPQR[LSPT - 1] = LSP - 1;
+        XSP[LSPT - 1] = (1.0 - TMASS) / S.WM[LSP - 1];
+        TMOLE = TMOLE + XSP[LSPT - 1];
+        if (nsub) nsub[c] = LSPT;
+        double TKRT = sqrt(tk[c]);
+        double TKD1 = tk[c] * S.TSTR;
+        double TKD2 = TKD1 * TKD1, TKD3 = TKD2 * TKD1, TKD4 = TKD3 * TKD1, TKD5 = TKD4 * TKD1;
+        int IPL1 = 0, IPL2 = 0;
+        if (TKD1 >= T.tpol1) { IPL1 = 7; IPL2 = 6; }
+        double TKBP = tk[c] * TKRT / S.PBACK;
+        /* main:929-955 */
+        for (int a = 0; a < LSPT; ++a) {
+            int k = ISPQR[a];
+            const double *p = T.poly + k * 14 + IPL1;
+            const double *q = T.om22 + k * 12 + IPL2;
+            double EUKEN = F(0.115) + F(0.354) * (p[0] + p[1] * TKD1 + p[2] * TKD2 + p[3] * TKD3
+                                                  + p[4] * TKD4);
+            double SIOME = T.cdia[k] * T.cdia[k] * (q[0] + q[1] * TKD1 + q[2] * TKD2 + q[3] * TKD3
+                                                   + q[4] * TKD4 + q[5] * TKD5);
+            ATC[a] = S.CONVRC * EUKEN * TKRT / S.WMIK[k][k] / SIOME;
+            AMU[a] = S.CONVRM * TKRT * S.WMIK[k][k] / SIOME;
+            for (int b = a + 1; b < LSPT; ++b) {
+                int kb = ISPQR[b];
+                double TKDS = TKD1 / S.ETLJ1[k][kb];
+                int K = ci_range(TKDS);
+                double CI = ci11t(K, TKDS, TKD2, TKD3, TKD4, k, kb);
+                DIF[a][b] = S.WMCD[k][kb] * TKBP / CI;
+                DIF[b][a] = S.WMCD[kb][k] * TKBP / CI;
+            }
+        }
+        /* main:957-979 */
+        for (int a = 0; a < LSPT; ++a) {
+            int k = ISPQR[a];
+            PHIK[a] = 0.0; PHDIK[a] = 0.0; EFDIK[a] = 0.0;
+            for (int b = 0; b < LSPT; ++b) {
+                if (b == a) continue;
+                int kb = ISPQR[b];
+                double t1 = 1.0 + sqrt(ATC[a] / ATC[b]) * S.WMIK[k][kb];
+                double t2 = 1.0 + sqrt(AMU[a] / AMU[b]) * S.WMIK[k][kb];
+                PHIK[a] = PHIK[a] + XSP[b] * (t1 * t1) / S.DWMIK[k][kb];
+                PHDIK[a] = PHDIK[a] + XSP[b] * (t2 * t2) / S.DWMIK[k][kb];
+                EFDIK[a] = EFDIK[a] + XSP[b] / DIF[a][b];
+            }
+        }
+        double VTC = 0.0, VMU = 0.0;
+        for (int a = 0; a < LSPT; ++a) {
+            VTC = VTC + ATC[a] * XSP[a] / (XSP[a] + F(1.065) * PHIK[a]);
+            VMU = VMU + AMU[a] * XSP[a] / (XSP[a] + PHDIK[a]);
+            double AA = TMOLE - XSP[a];
+            if (AA <= 1.0e-10) VDFQ[a] = S.CONVRD * DIF[a][LSPT - 1];
+            else VDFQ[a] = S.CONVRD * (TMOLE - XSP[a]) / EFDIK[a];
+        }
+        vtc[c] = VTC;
+        vmu[c] = VMU;
+        /* main:981-1003 */
+        for (int k = 0; k < LSP; ++k) {
+            double v;
+            if (ISPQ[k] < 0) {
+                double EFD = 0.0;
+                for (int b = 0; b < LSPT; ++b) {
+                    int nb = ISPQR[b];
+                    double TKDS = TKD1 / S.ETLJ1[k][nb];
+                    int K = ci_range(TKDS);
+                    double CI = ci11t(K, TKDS, TKD2, TKD3, TKD4, k, nb);
+                    EFD = EFD + XSP[b] / (S.WMCD[k][nb] * TKBP / CI);
+                }
+                v = S.CONVRD * TMOLE / EFD;
+            } else {
+                v = VDFQ[ISPQ[k]];
+            }
+            vdf[(size_t)k * n + c] = v;
+        }
+    }
+}
+
+/* ------------------------------------------------------------- SOLVESP */
+
+/* Point-implicit relaxation of species 1..51 and the two soot scalars
+ * (solvesp.f:82-2836), then the N2 closure (solvesp.f:2837-2915).
+ *
+ * Cells are independent here: the face coefficients of the reference
+ * (EA..QA, ``nbr``) enter through face_sum[k*n+c] = E+W+N+S and
+ * face_nbr[k*n+c] = P*Y(J+1)+Q*Y(J-1)+E*Y(I+1)+W*Y(I-1) evaluated on a frozen
+ * neighbour field (both may be NULL: no transport). The pass loop stops when
+ * sum|dY|/spnorm <= tol (solvesp.f:2833), over all n cells.
+ * y0: old-time mass fractions (FA..), y: current values (SA..), updated in
+ * place; rc, sour: CKRATES outputs; soot[2*n]: mass fraction, number density
+ * (updated in place; old-time values in soot0). Returns the pass count as
+ * the reference reports it in ISOR1. */
+int orc_species_update(int n, const double *rho, const double *y0, double *y, const double *rc,
+                       const double *sour, const double *soot0, double *soot,
+                       const double *face_sum, const double *face_nbr, double dt, int isor,
+                       double relx, double tol, double spnorm)
+{
+    const double SOR1 = relx, SOR2 = 1.0 - SOR1;
+    double *A = (double *)calloc(LRX + 1, sizeof(double));
+    double Y[LSP], Y0[LSP], RC[LRX], SO[6];
+    int ISORP;
+    for (ISORP = 1; ISORP <= isor; ++ISORP) {
+        double RSD = 0.0;
+        for (int c = 0; c < n; ++c) {
+            for (int k = 0; k < LSP; ++k) { Y[k] = y[(size_t)k * n + c]; Y0[k] = y0[(size_t)k * n + c]; }
+            for (int r = 0; r < LRX; ++r) RC[r] = rc[(size_t)r * n + c];
+            for (int m = 0; m < 6; ++m) SO[m] = sour[(size_t)m * n + c];
+            double RHO = rho[c];
+            double RHS1A = 0.0;
+            for (int b = 0; b < LSP - 1; ++b) {
+                /* A-term (re)computations */
+                int ro = T.blk_rec_off[b];
+                for (int t = 0; t < T.blk_rec_len[b]; ++t) {
+                    int r = T.rec_r[ro + t];
+                    A[r] = chain_value(T.rec_foff[ro + t], T.rec_flen[ro + t], A, RC, Y, Y0, SO, NULL);
+                }
+                /* Q3: a block without an RHS1A statement reuses the previous value */
+                if (T.blk_prod_has[b])
+                    RHS1A = sum_terms(T.blk_prod_off[b], T.blk_prod_len[b], A, RC, Y, Y0, SO, NULL);
+                double RHS1B = sum_terms(T.blk_extra_off[b], T.blk_extra_len[b], A, RC, Y, Y0, SO, NULL);
+                int k = b;   /* block b updates species b+1 (0-based b) */
+                double RHS1 = RHO * Y0[k] + dt * S.WM[k] * (RHS1A + RHS1B);
+                double RHS2 = 0.0;
+                if (T.blk_loss_has[b])
+                    RHS2 = -(dt * S.WM[k] * sum_terms(T.blk_loss_off[b], T.blk_loss_len[b], A, RC, Y, Y0, SO, NULL));
+                double fs = face_sum ? face_sum[(size_t)k * n + c] : 0.0;
+                double fn = face_nbr ? face_nbr[(size_t)k * n + c] : 0.0;
+                double PPP = RHO - fs;
+                double FNEW = SOR2 * Y[k] + (RHS1 - fn) * SOR1 / (PPP - RHS2);
+                RSD = RSD + fabs(Y[k] - FNEW);
+                if (FNEW < 0.0) FNEW = 0.0;
+                Y[k] = FNEW;
+                int mo = T.blk_mul_off[b];
+                for (int t = 0; t < T.blk_mul_len[b]; ++t) A[T.mul_r[mo + t]] = FNEW * A[T.mul_r[mo + t]];
+            }
+            /* soot mass fraction, solvesp.f:2807-2820 (molar mass of C) */
+            {
+                double RHS1 = RHO * soot0[c] + dt * (F(0.012011) / S.WMSTR) *
+                              (2.0 * SO[0] * Y[21] - SO[2] * Y[1] - SO[3] * Y[4] - SO[4] * Y[3]);
+                double PPP = RHO - 0.0;
+                double FNEW = SOR2 * soot[c] + RHS1 * SOR1 / (PPP - 0.0);
+                RSD = RSD + fabs(soot[c] - FNEW);
+                if (FNEW < 0.0) FNEW = 0.0;
+                soot[c] = FNEW;
+            }
+            /* soot number density, solvesp.f:2822-2832 */
+            {
+                double RHS1 = RHO * soot0[n + c] + dt * SO[1] * Y[21];
+                double RHS2 = -(dt * SO[5]);
+                double PPP = RHO - 0.0;
+                double FNEW = SOR2 * soot[n + c] + RHS1 * SOR1 / (PPP - RHS2);
+                if (FNEW < 0.0) FNEW = 0.0;
+                soot[n + c] = FNEW;
+            }
+            for (int k = 0; k < LSP - 1; ++k) y[(size_t)k * n + c] = Y[k];
+        }
+        if (RSD / spnorm <= tol) break;
+    }
+    /* solvesp.f:2834-2838: the reference reports ISORP (ISOR1+1 if not converged) */
+    int passes = ISORP;
+    /* N2 closure and renormalisation, solvesp.f:2839-2915 (Q5: only if sum > 1) */
+    for (int c = 0; c < n; ++c) {
+        double FTOT = y[c];
+        for (int k = 1; k < LSP - 1; ++k) FTOT = FTOT + y[(size_t)k * n + c];
+        FTOT = FTOT + soot[c];
+        double N2 = 1.0 - FTOT;
+        if (FTOT > 1.0) {
+            for (int k = 0; k < LSP - 1; ++k) y[(size_t)k * n + c] = y[(size_t)k * n + c] / FTOT;
+            soot[c] = soot[c] / FTOT;
+            N2 = 0.0;
+        }
+        y[(size_t)(LSP - 1) * n + c] = N2;
+    }
+    free(A);
+    return passes;
+}
+
+/* ------------------------------------------------------------- T from h */
+
+/* solveh.f:1170-1234: temperature from the non-dimensional sensible
+ * enthalpy ht (FPZ) and the mass fractions; tk holds the guess on entry. */
+void orc_temperature(int n, double *tk, const double *y, const double *ht)
+{
+    const double TKDMIN = S.TSTR - 1.0;
+    for (int c = 0; c < n; ++c) {
+        double ENTH = (ht[c] - F(0.5) * 0.0) * S.HSTR;
+        for (int k = 0; k < LSP; ++k) ENTH = ENTH + y[(size_t)k * n + c] * S.HFO[k] * S.HSTR;
+        int IPL = 0;
+        double TPOLY = T.tpol1;
+        double TKD = tk[c] * S.TSTR;
+        double A1, A2, A3, A4, A5, A6;
+        for (;;) {
+            if (TKD > TPOLY) TKD = TPOLY / 2.0;
+            A1 = A2 = A3 = A4 = A5 = A6 = 0.0;
+            for (int k = 0; k < LSP; ++k) {
+                const double *a = T.poly + k * 14 + IPL;
+                double yk = y[(size_t)k * n + c];
+                A1 = A1 + a[0] * yk / S.WM[k];
+                A2 = A2 + a[1] * yk / S.WM[k] / 2.0;
+                A3 = A3 + a[2] * yk / S.WM[k] / 3.0;
+                A4 = A4 + a[3] * yk / S.WM[k] / 4.0;
+                A5 = A5 + a[4] * yk / S.WM[k] / 5.0;
+                A6 = A6 + a[5] * yk / S.WM[k];
+            }
+            double FUNT = ((A1 + (A2 + (A3 + (A4 + A5 * TPOLY) * TPOLY) * TPOLY) * TPOLY) * TPOLY + A6)
+                          * S.GASC / S.WMSTR - ENTH;
+            if (FUNT >= 1.0e-07) break;
+            if (IPL >= 7) break;
+            IPL = 7;
+            if (TKD <= TPOLY) TKD = T.tpol2 / 2.0;
+            TPOLY = T.tpol2;
+        }
+        for (int it = 1; it <= 100; ++it) {
+            double DTKD = ((A1 + (A2 + (A3 + (A4 + A5 * TKD) * TKD) * TKD) * TKD) * TKD + A6
+                           - ENTH * S.WMSTR / S.GASC)
+                          / (A1 + (2.0 * A2 + (3.0 * A3 + (4.0 * A4 + 5.0 * A5 * TKD) * TKD) * TKD) * TKD);
+            if (fabs(DTKD) <= F(0.001)) break;
+            TKD = TKD - DTKD;
+        }
+        if (TKD > T.tpol2) TKD = T.tpol2;
+        if (TKD < TKDMIN) TKD = TKDMIN;
+        tk[c] = TKD / S.TSTR;
+    }
+}
