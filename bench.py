@@ -1,0 +1,356 @@
+"""Benchmark: chem+property cell-updates/s of UNICORN's species sweep on B200.
+
+One step = one species sweep over the 601x301 (180,901-cell) heptane field
+(fuel=11, T peak 2300 K, seed 0): Y clip + mixture-averaged transport, cp and
+h, the 544 rate coefficients, omega_k and d(omega_k)/dY_k, then the
+point-implicit update of SOLVESP with the reference's input-card settings
+(up to 100 passes, relaxation 0.99, tolerance 1e-8) at dt = 1e-5 s.
+A cell-update = one cell through one such sweep.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+``value`` is device-resident throughput (fields already on the GPU);
+``e2e`` is the same sweep through the C ABI with the step's inputs copied
+from pinned host memory and its outputs copied back, inside the timed
+region. ``--impl reference`` times the reference's own routines (translated
+to C, oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "chem+property cell-updates/s: FP64 vs mixed vs MLP+fallback at stated ω error"
+UNIT = "cell-updates/s"
+DT = 1e-3            # non-dimensional: 1e-5 s / TMSTR (0.01 s)
+ISOR, RELX, TOL = 100, 0.99, 1e-8     # docs/input.uni:25-27
+NZ, NR, FUEL, TPEAK = 601, 301, 11, 2300.0
+
+
+def workload_config(n_gpus, extra=None):
+    c = {"workload": "C2: 601x301 heptane jet field (fuel=11, T_peak 2300 K, seed 0), one species sweep per step "
+                     "(props, cp/h, rates, omega, domega/dY, point-implicit update isor=100 relx=0.99 tol=1e-8, dt=1e-5 s)",
+         "cells": NZ * NR, "precision": "fp64", "l2": "working set > L2 (RC plane 787 MB written and read every step)",
+         "parallelism": f"cell-sharded x{n_gpus} (independent fields per rank)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index: int):
+        self.index, self.samples, self._stop = index, [], threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        q = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+            "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            for nm, v in zip(names, s[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- our arm
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline_port(f, scales_src):
+    """The oracle (a faithful FP64 C restatement) on one host core, bounded sample."""
+    from oracle.oracle import Oracle
+    from unicorn_b200.fields import nondimensional
+    o = Oracle()
+    ns = 1024
+    tk, rho = nondimensional(f, o.scales, o.wm)
+    tk, rho, y = tk[:ns].copy(), rho[:ns].copy(), np.ascontiguousarray(f.y[:, :ns])
+    t0 = time.perf_counter()
+    yc, mu, lam, dk, _ = o.props(tk, y)
+    cp = o.cp(tk, yc)
+    h = o.enthalpy(tk, yc)
+    q = o.omega(tk, rho, yc)
+    rc, sour = o.rates(tk, rho, yc)
+    yn, s, passes = o.species_update(rho, yc, rc, sour, DT, isor=ISOR, relx=RELX, tol=TOL)
+    dt = time.perf_counter() - t0
+    return {"value": ns / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"first {ns} cells of the C2 field, one full sweep (oracle/unichem_oracle.c, -O2, 1 thread; "
+                      f"{passes} update passes), {dt:.2f} s"}
+
+
+def run_ours(args, rank, world, dev):
+    import torch
+    from unicorn_b200 import unichem
+    from unicorn_b200.fields import jet_field, nondimensional
+    f = jet_field(NZ, NR, fuel=FUEL, t_peak=TPEAK, seed=rank)
+    n = f.n
+    u = unichem.UniChem(n, device=dev)
+    tk, rho = nondimensional(f, u.scales, u.wm)
+    view = unichem_view(u)
+    ext = torch.cuda.ExternalStream(view["stream"], device=dev)
+    # pinned host buffers for the end-to-end path
+    pin = lambda *s: torch.empty(s, dtype=torch.float64, pin_memory=True).numpy()
+    h_tk, h_rho, h_y = pin(n), pin(n), pin(52, n)
+    h_tk[:], h_rho[:], h_y[:] = tk, rho, f.y
+    outs = dict(qdsp=pin(52, n), qdot=pin(n), domega_dy=pin(52, n), vmu=pin(n), vtc=pin(n), vdf=pin(52, n),
+                cp=pin(n), h=pin(n))
+    h_yout = pin(52, n)
+
+    def reset():
+        u.upload(h_tk, h_rho, h_y)
+
+    def step_device():
+        return u.sweep(DT, isor=ISOR, relx=RELX, tol=TOL)
+
+    passes_seen = []
+    reset()
+    for _ in range(args.warmup):
+        passes_seen.append(step_device())
+    # ---------------- device-resident timing
+    reset()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    u.profile(True)
+    with torch.cuda.stream(ext):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(dev if world == 1 else dev) as clk:
+            e0.record(ext)
+            for _ in range(args.steps):
+                passes_seen.append(step_device())
+            e1.record(ext)
+            torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    kt = u.profile_read()
+    u.profile(False)
+    ms = max_over_ranks(ms, world)
+    # ---------------- end-to-end through the C ABI (host buffers)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        u.upload(h_tk, h_rho, h_y)
+        u.sweep(DT, isor=ISOR, relx=RELX, tol=TOL)
+        u.download_outputs(outs)
+        u.lib.uc_download_fields(u._h, None, None, unichem._p(h_yout), None, None)
+    u.sync()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) * 1e3, world) / 1e3
+    h2d = (2 + 52) * 8 * n
+    d2h = (52 * 4 + 5) * 8 * n
+    res = {"ms_per_step": ms / args.steps, "value": world * n * args.steps / (ms / 1e3),
+           "e2e": {"value": world * n * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h},
+           "kernel_ms": kt, "passes": passes_seen, "clocks": clk.summary(), "n": n,
+           "gpu_launches": sum(c for _, c in kt.values())}
+    u.close()
+    return res, f
+
+
+def unichem_view(u):
+    import ctypes
+
+    class View(ctypes.Structure):
+        _fields_ = [(k, ctypes.c_void_p) for k in ("tk", "rho", "fsp", "fsp_old", "stmf", "stnd", "rc", "qdsp", "qdot",
+                                                    "domega_dy", "vmu", "vtc", "vdf", "cp", "h")] + \
+                   [("n", ctypes.c_int), ("npad", ctypes.c_int), ("stream", ctypes.c_void_p)]
+    v = View()
+    u.lib.uc_device_view_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(View)]
+    u._ck(u.lib.uc_device_view_get(u._h, ctypes.byref(v)))
+    return {"stream": v.stream or 0, "npad": v.npad}
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def roofline(res, n, steps):
+    """Dominant kernel of the step and its achieved rate against the measured HBM copy bandwidth."""
+    kt = res["kernel_ms"]
+    name = max(kt, key=lambda k: kt[k][0])
+    ms, cnt = kt[name]
+    hbm, src = peaks()
+    npad = (n + 31) // 32 * 32
+    passes = sum(res["passes"][-steps:]) / max(1, steps)
+    # algorithmic bytes per launch (per-cell figures x cells)
+    if name == "update":
+        per_cell = passes * (544 + 52 + 52 + 6 + 2 + 2) * 8 + (52 + 2) * 8
+        unit_note = f"per cell and launch: {passes:.1f} passes x (RC 544 + Y 52 in + 52 out + SOUR 6 + soot 4) x 8 B"
+    elif name == "chem":
+        per_cell = (52 + 4) * 8 + (544 + 52 + 52 + 1 + 6) * 8
+        unit_note = "per cell: read T, rho, soot, Y (56 x 8 B); write RC 544, QDSP 52, dw/dY 52, QDOT, SOUR 6"
+    else:
+        per_cell = (54 + 54) * 8
+        unit_note = "per cell: 54 inputs + 54 outputs x 8 B"
+    bytes_per_launch = per_cell * n
+    achieved = bytes_per_launch / (ms / cnt / 1e3) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "peak_source": src,
+            "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None, "bytes_per_launch": bytes_per_launch,
+            "avg_launch_ms": ms / cnt, "bytes_rule": unit_note}
+
+
+def main_ours(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    res, f = run_ours(args, rank, world, local)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(f, None)
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(res["value"], 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(res["ms_per_step"], 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded C2 generator; the reference ships no benchmark data)",
+                "config": workload_config(world, {"update_passes_per_step": res["passes"][-args.steps:]}),
+                "e2e": res["e2e"], "gpu_launches": res["gpu_launches"] * world, "clocks": res["clocks"],
+                "roofline": roofline(res, res["n"], args.steps),
+                "kernel_ms": {k: round(v[0], 3) for k, v in res["kernel_ms"].items()}}
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- reference arm
+def _ref_worker(args_tuple):
+    """One host process: the reference's own routines on a chunk of cells."""
+    tk, rho, y, isor = args_tuple
+    from oracle.ref import RefUnicorn
+    r = _ref_worker.r if hasattr(_ref_worker, "r") else None
+    if r is None:
+        r = _ref_worker.r = RefUnicorn()
+    t0 = time.perf_counter()
+    yc, mu, lam, vdf = r.props(tk, y)
+    cp = r.cp(tk, yc)
+    q = r.omega(tk, rho, yc)
+    yn, s1, s2, passes = r.species_update(tk, rho, yc, DT, isor=isor, relx=RELX, tol=TOL)
+    return len(tk), time.perf_counter() - t0, passes
+
+
+def main_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import ref as R
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference routines translated to C) "
+                          "is not built: run python -c 'import __graft_entry__ as g; g.build()' where the reference "
+                          "checkout exists"}))
+        return
+    import multiprocessing as mp
+    from unicorn_b200.fields import jet_field, nondimensional
+    r0 = R.RefUnicorn()
+    f = jet_field(NZ, NR, fuel=FUEL, t_peak=TPEAK, seed=0)
+    tk, rho = nondimensional(f, r0.scales, r0.wm)
+    chunk = r0.chunk
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        def one_step(step):
+            jobs = []
+            for w in range(cores):
+                a = ((step * cores + w) * chunk) % (f.n - chunk)
+                jobs.append((tk[a:a + chunk].copy(), rho[a:a + chunk].copy(),
+                             np.ascontiguousarray(f.y[:, a:a + chunk]), ISOR))
+            t0 = time.perf_counter()
+            out = pool.map(_ref_worker, jobs)
+            return sum(o[0] for o in out), time.perf_counter() - t0, [o[2] for o in out]
+        for w in range(args.warmup):
+            one_step(w)
+        cells, secs, passes = 0, 0.0, []
+        for s in range(args.steps):
+            c, t, p = one_step(args.warmup + s)
+            cells += c
+            secs += t
+            passes += p
+    v = cells / secs
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(secs / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded C2 generator)",
+        "config": workload_config(1, {"update_passes_per_chunk": passes[:8]}),
+        "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{cores} chunks of {chunk} cells of the C2 field per step, one process per core, "
+                                   "each running the reference's PROPS/CKRATES/SOLVESP/SOLVEH-rate code "
+                                   "(translated from its Fortran, gcc -O2)"},
+        "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        main_reference(args)
+    else:
+        main_ours(args)
+
+
+if __name__ == "__main__":
+    main()

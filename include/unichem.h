@@ -1,0 +1,169 @@
+/*
+ * unichem: B200 (sm_100a) implementation of UNICORN's per-cell chemistry and
+ * property hot path, behind a C ABI that a Fortran host binds with
+ * ISO_C_BINDING (see INTEGRATION.md for the interface module).
+ *
+ * Data layout: the host's COMMON arrays as they are. A field of n cells is
+ * passed as Fortran arrays over the (J,I) grid flattened column-major, i.e.
+ * cell c = (I-1)*LJ + (J-1); species fields are FSP(LJ,LI,LSP), which is
+ * [52][n] in C terms. All quantities are the reference's non-dimensional
+ * ones (TK = T/TSTR, RHO = rho/RSTR, ...; the scales follow from uc_inputs).
+ *
+ * Fields stay resident on the device between calls: uc_upload_fields copies
+ * host arrays in, the compute calls work on the device copies, and results
+ * are copied out only when a host pointer is given. The library never keeps
+ * a host pointer after a call returns.
+ *
+ * Every call returns 0 on success or a negative UC_E* code; uc_last_error()
+ * gives the message. Calls on one context are not re-entrant; use one context
+ * per host thread (each context owns one CUDA stream).
+ */
+#ifndef UNICHEM_H
+#define UNICHEM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UC_LSP 52   /* species, src/unicornd-mild-sd-5.f:3 (LSP) */
+#define UC_LRX 544  /* reaction slots, src/unicornd-mild-sd-5.f:3 (LRX) */
+
+/* precision of uc_rates / uc_omega */
+#define UC_FP64 0   /* all-FP64, the drop-in form */
+#define UC_MIXED 1  /* FP32 exponentials, power laws and sums; FP64 Kc and update */
+
+/* error codes */
+#define UC_OK 0
+#define UC_E_ARG -1        /* invalid argument (null pointer, size out of range) */
+#define UC_E_CUDA -2       /* CUDA runtime error (message in uc_last_error) */
+#define UC_E_STATE -3      /* call order: e.g. update before fields were uploaded */
+#define UC_E_TIMEOUT -4    /* a device-side bounded wait gave up */
+#define UC_E_NOCONV -5     /* a bounded iteration did not converge (reported, not fatal) */
+#define UC_E_NOMEM -6      /* device allocation failed */
+
+typedef struct uc_ctx uc_ctx;
+
+/* Input-card values the reference reads from cfg/input.uni
+ * (src/unicornd-mild-sd-5.f:154-155; sample values docs/input.uni:4-5). */
+typedef struct {
+    double rtin, rtot;   /* inner/outer radius [m]: ALSTR = RTOT - RTIN */
+    double vref;         /* reference velocity [m/s] */
+    double tref;         /* reference temperature [K] */
+    double pref;         /* reference pressure [Pa] */
+    double rref;         /* density card value (recomputed from the gas law, as the reference does) */
+    double fo2in;        /* O2 mass fraction of the air stream */
+} uc_inputs;
+
+/* Reference scales after set-up (/CB06/ of the reference, main:421-459). */
+typedef struct {
+    double alstr, vstr, rstr, pstr, tstr, tmstr, amstr, acstr, dstr, hstr, cpstr, akstr, epstr,
+           wmstr, gasc, beta1, beta2, beta3, beta4, rei, pback, hconv, convrc, convrm, convrd;
+} uc_scales;
+
+/* Set-up: replaces the reference's table preparation (main:327-483) and
+ * allocates device storage for n cells on CUDA device `device`.
+ * Replaces: the start-up section of PROGRAM UNICORN, src/unicornd-mild-sd-5.f:327-483. */
+int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out);
+
+/* Scales and non-dimensional molar masses WM(52), formation enthalpies HFO(52). */
+int uc_get_scales(const uc_ctx *ctx, uc_scales *sc, double *wm, double *hfo);
+
+/* Copy fields to the device. tk[n], rho[n], fsp[52*n] required; stmf, stnd
+ * (soot mass fraction and number density) may be NULL (= 0). The uploaded
+ * mass fractions also become the "old time level" (FA.. of SOLVESP).
+ * Replaces: the COMMON /CB04/ and /SOOT/ state read by CKRATES/SOLVESP. */
+int uc_upload_fields(uc_ctx *ctx, const double *tk, const double *rho, const double *fsp,
+                     const double *stmf, const double *stnd);
+
+/* Copy the device-resident state back (any pointer may be NULL). */
+int uc_download_fields(uc_ctx *ctx, double *tk, double *rho, double *fsp, double *stmf,
+                       double *stnd);
+
+/* Rate coefficients of all 544 slots, kept on the device for uc_species_update.
+ * Replaces: CALL CKRATES, src/lib/spgsolv.f:1293 (src/lib/ckrates.f). If rc is
+ * not NULL the RC plane RC(n,544) ([544][n]) is also copied to the host. */
+int uc_rates(uc_ctx *ctx, int precision, double *rc);
+
+/* Species source terms from the device-resident state: qdsp[52*n] is the
+ * reference's QDSP (= -omega_k), qdot[n] its QDOT, domega_dy[52*n] the
+ * diagonal linearisation d(omega_k)/dY_k = -RCONV*W_k*L_k (same units as
+ * omega). NULL outputs stay on the device.
+ * Replaces: the rate part of CALL SOLVEH, src/lib/solveh.f:116-1145. */
+int uc_omega(uc_ctx *ctx, int precision, double *qdsp, double *qdot, double *domega_dy);
+
+/* Y clip and N2 closure (applied to the device state, as main:821-828 does)
+ * and mixture-averaged transport: vmu[n], vtc[n], vdf[52*n].
+ * Replaces: the inline property block of PROGRAM UNICORN, src/unicornd-mild-sd-5.f:821-1006. */
+int uc_props(uc_ctx *ctx, double *vmu, double *vtc, double *vdf);
+
+/* Mixture cp (the reference's TCP, non-dimensional) and mixture enthalpy
+ * h = sum_k Y_k h_k with h_k the reference's HENTH.
+ * Replaces: src/lib/spgsolv.f:102-173 (TCP) and src/lib/solveh.f:39-57 (HENTH). */
+int uc_cp_h(uc_ctx *ctx, double *cp, double *h);
+
+/* Point-implicit species update of species 1..51 and the two soot scalars,
+ * up to isor passes until sum|dY|/spnorm <= tol (spnorm <= 0 means
+ * 51*n), then the N2 closure. Uses the RC plane of the last uc_rates call.
+ * face_sum[51*n] (E+W+N+S) and face_nbr[51*n] (sum of coefficient times the
+ * neighbour value) are the frozen transport terms; NULL means none. passes
+ * receives the count the reference reports in ISOR1.
+ * Replaces: CALL SOLVESP(ISOR1,RELXSP,TOLRSP,SPNORM), src/lib/spgsolv.f:1295. */
+int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, double tol, double spnorm,
+                      const double *face_sum, const double *face_nbr, int *passes);
+
+/* Temperature from the non-dimensional sensible enthalpy ht[n] (FPZ) by
+ * Newton's method; updates the device temperature (initial guess = current).
+ * Replaces: src/lib/solveh.f:1170-1234. */
+int uc_temperature_from_h(uc_ctx *ctx, const double *ht);
+
+/* One species sweep on the device-resident state, in the order of the
+ * reference's time step: Y clip + transport properties (main:821-1006), cp
+ * and h, rate coefficients with omega and d(omega)/dY at the start-of-step
+ * state (CKRATES + SOLVEH rates), then the point-implicit update (SOLVESP)
+ * with the arguments of uc_species_update. Outputs stay on the device
+ * (uc_device_view_get / the download calls).
+ * Replaces: CALL SPGSOLV's chemistry part (src/lib/spgsolv.f:102-176,1291-1298)
+ * preceded by the property block of main:821-1006. */
+int uc_sweep(uc_ctx *ctx, int precision, double dt, int isor, double relx, double tol, double spnorm,
+             const double *face_sum, const double *face_nbr, int *passes);
+
+/* Outputs of the last uc_sweep/uc_omega/uc_props/uc_cp_h to the host (NULL = skip). */
+int uc_download_outputs(uc_ctx *ctx, double *qdsp, double *qdot, double *domega_dy, double *vmu,
+                        double *vtc, double *vdf, double *cp, double *h);
+
+/* Kernel timing with CUDA events on the context's stream (tracing).
+ * uc_profile(ctx, 1) starts recording every launch; uc_profile_read
+ * synchronises and returns, per kernel kind (UC_K_*), the summed device time
+ * in ms and the launch count since the last read. */
+#define UC_K_CHEM 0
+#define UC_K_UPDATE 1
+#define UC_K_PROPS 2
+#define UC_K_CPH 3
+#define UC_K_TEMP 4
+#define UC_K_COUNT 5
+int uc_profile(uc_ctx *ctx, int on);
+int uc_profile_read(uc_ctx *ctx, double *ms, int *launches);
+
+/* Synchronise the context's stream. */
+int uc_sync(uc_ctx *ctx);
+
+/* Message of the last error on this context (static storage, valid until the next call). */
+const char *uc_last_error(const uc_ctx *ctx);
+
+/* Release all device memory of the context. */
+void uc_destroy(uc_ctx *ctx);
+
+/* Device pointers of the resident state, for callers that keep their own
+ * device data (all [k][n] SoA, FP64). */
+typedef struct {
+    double *tk, *rho, *fsp, *fsp_old, *stmf, *stnd, *rc, *qdsp, *qdot, *domega_dy, *vmu, *vtc,
+           *vdf, *cp, *h;
+    int n, npad;
+    void *stream;   /* cudaStream_t */
+} uc_device_view;
+int uc_device_view_get(uc_ctx *ctx, uc_device_view *v);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

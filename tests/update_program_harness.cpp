@@ -1,0 +1,39 @@
+// Test-only harness: runs the generated species-update program
+// (unicorn_b200/csrc/generated/update_program.cuh) on the host, so that the
+// symbolic resolution of the reference's A-terms can be checked against the
+// oracle without a GPU. Not part of the product.
+#include <cmath>
+#include <cstring>
+#define LSP 52
+#define LRX 544
+
+extern "C" int harness_update(int n, const double *rho_a, const double *y0_a, double *y_a,
+                              const double *rc_a, const double *sour_a, const double *wm,
+                              double dt, int isor, double relx, double tol, double spnorm)
+{
+    const double sor1 = relx, sor2 = 1.0 - relx;
+    double yo[LSP], yn[LSP], y0[LSP], sour[6];
+    int pass;
+    for (pass = 1; pass <= isor; ++pass) {
+        double rsd = 0.0;
+        for (int c = 0; c < n; ++c) {
+            for (int k = 0; k < LSP; ++k) { yo[k] = y_a[k * n + c]; y0[k] = y0_a[k * n + c]; yn[k] = 0.0; }
+            for (int m = 0; m < 6; ++m) sour[m] = sour_a[m * n + c];
+            const double rho = rho_a[c];
+#define RC(r) rc_a[(r) * n + c]
+#define YO(k) yo[k]
+#define YN(k) yn[k]
+#define Y0(k) y0[k]
+#define SOUR(m) sour[m]
+#define WM(k) wm[k]
+#define FACE_SUM(k) 0.0
+#define FACE_NBR(k) 0.0
+#define UC_UPDATE_TAIL(k) do { if (fnew < 0.0) fnew = 0.0; yn[k] = fnew; } while (0)
+#include "../unicorn_b200/csrc/generated/update_program.cuh"
+            UC_UPDATE_PROGRAM();
+            for (int k = 0; k < LSP - 1; ++k) y_a[k * n + c] = yn[k];
+        }
+        if (rsd / spnorm <= tol) break;
+    }
+    return pass;
+}

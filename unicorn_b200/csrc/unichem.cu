@@ -1,0 +1,684 @@
+// unichem: host side of the C ABI (include/unichem.h) and kernel launches.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/unichem.h"
+#include "chem_kernel.cuh"
+#include "props_kernel.cuh"
+#include "update_kernel.cuh"
+
+using namespace uc;
+
+#define F32(x) ((double)(float)(x))
+
+struct uc_ctx {
+    int device = 0, n = 0, npad = 0, ntile = 0, nsm = 0;
+    cudaStream_t stream = nullptr;
+    uc_scales sc{};
+    DevParams *hP = nullptr;          // host copy
+    DevParams *dP = nullptr;
+    PairTab *dTab = nullptr;
+    double *tk = nullptr, *rho = nullptr, *y = nullptr, *y0 = nullptr, *soot = nullptr, *soot0 = nullptr;
+    double *rc = nullptr, *sour = nullptr;
+    double *qdsp = nullptr, *qdot = nullptr, *dwdy = nullptr;
+    double *vmu = nullptr, *vtc = nullptr, *vdf = nullptr, *cp = nullptr, *h = nullptr;
+    double *face_sum = nullptr, *face_nbr = nullptr, *ht = nullptr, *partial = nullptr;
+    int *status = nullptr, *passes = nullptr;
+    bool have_fields = false, have_rc = false;
+    int upd_grid = 0;
+    // tracing: CUDA event pairs around launches
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, int>> ev_used;   // (kind, index of the start event)
+    char err[512] = {0};
+};
+
+static void prof_begin(uc_ctx *c, int kind, int &slot)
+{
+    slot = -1;
+    if (!c->prof) return;
+    const int i = (int)c->ev_used.size() * 2;
+    while ((int)c->ev_pool.size() < i + 2) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        c->ev_pool.push_back(e);
+    }
+    cudaEventRecord(c->ev_pool[i], c->stream);
+    c->ev_used.push_back({kind, i});
+    slot = i;
+}
+
+static void prof_end(uc_ctx *c, int slot)
+{
+    if (slot >= 0) cudaEventRecord(c->ev_pool[slot + 1], c->stream);
+}
+
+static int set_err(uc_ctx *c, int code, const char *fmt, ...)
+{
+    if (c) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(c->err, sizeof(c->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return set_err(ctx, UC_E_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                           __FILE__, __LINE__);                                                  \
+    } while (0)
+
+// ------------------------------------------------------------------ set-up
+
+// Tables and scales of src/unicornd-mild-sd-5.f:327-483 (all reactions on,
+// IRSW=1), written for the device parameter block. Literal constants keep
+// the reference's single-precision kind where it has one.
+static void build_params(const uc_inputs &in, DevParams &P, std::vector<PairTab> &tab, uc_scales &sc)
+{
+    const double RUCAL = F32(1.9872), GASC = F32(8.3144);
+    double AKF[LRX], ALF[LRX], EXAF[LRX], AKLOW[LRX], ALLOW[LRX], EALOW[LRX], TROE[LRX][4];
+    for (int r = 0; r < LRX; ++r) {
+        AKF[r] = uc_raw_akf[r]; ALF[r] = uc_raw_alf[r]; EXAF[r] = uc_raw_exaf[r];
+        AKLOW[r] = uc_raw_aklow[r]; ALLOW[r] = uc_raw_allow[r]; EALOW[r] = uc_raw_ealow[r];
+        for (int c = 0; c < 4; ++c) TROE[r][c] = uc_raw_troe[r * 4 + c];
+    }
+    for (int i = 0; i < LRX; i += 2) {   // main:364-413
+        EXAF[i] = EXAF[i] / RUCAL;
+        if (AKF[i] < 0) {
+            AKF[i] = -AKF[i];
+            EALOW[i] = EALOW[i] / RUCAL;
+        } else {
+            EALOW[i] = AKLOW[i] = ALLOW[i] = 0.0;
+            for (int c = 0; c < 4; ++c) TROE[i][c] = 0.0;
+        }
+        AKF[i + 1] = 1.0;
+        EXAF[i + 1] = ALF[i + 1] = EALOW[i + 1] = AKLOW[i + 1] = ALLOW[i + 1] = 0.0;
+        for (int c = 0; c < 4; ++c) TROE[i + 1][c] = 0.0;
+    }
+    // main:421-459
+    const double WMREF = 1.0 / (in.fo2in / uc_wsp[1] + (1.0 - in.fo2in) / uc_wsp[LSP - 1]) / 1000.0;
+    const double AMREF = 5.69428e-07 * pow(in.tref, F32(0.62245));
+    const double ACREF = 2.78763e-04 * pow(in.tref, F32(0.796783));
+    const double DREF = 1.2e-04;
+    const double RREF = in.pref / (GASC / WMREF) / in.tref;
+    sc.gasc = GASC;
+    sc.alstr = in.rtot - in.rtin;
+    sc.vstr = in.vref;
+    sc.rstr = RREF;
+    sc.pstr = RREF * in.vref * in.vref;
+    sc.pback = in.pref / sc.pstr;
+    sc.tstr = in.tref;
+    sc.hstr = in.vref * in.vref;
+    sc.akstr = in.vref * in.vref;
+    sc.epstr = in.vref * in.vref * in.vref / sc.alstr;
+    sc.cpstr = in.vref * in.vref / in.tref;
+    sc.acstr = ACREF;
+    sc.tmstr = sc.alstr / in.vref;
+    sc.amstr = AMREF;
+    sc.dstr = DREF;
+    sc.wmstr = WMREF;
+    sc.rei = AMREF / RREF / in.vref / sc.alstr;
+    sc.beta1 = GASC * sc.rstr * sc.tstr / sc.pstr / sc.wmstr;
+    sc.beta2 = sc.tstr * sc.acstr / sc.amstr / sc.vstr / sc.vstr;
+    sc.beta3 = sc.rstr * sc.dstr / sc.amstr;
+    sc.beta4 = 0.0;
+    sc.hconv = GASC / sc.wmstr / sc.hstr;
+    sc.convrc = F32(418.68) * 1.9891e-04 * sqrt(sc.tstr / 1000.0 / sc.wmstr) / sc.acstr;
+    sc.convrm = F32(0.1) * 2.6693e-05 * sqrt(1000.0 * sc.wmstr * sc.tstr) / sc.amstr;
+    sc.convrd = F32(0.02628) * sc.tstr * sqrt(sc.tstr) / sc.pstr / sqrt(sc.wmstr * 1000.0) / sc.dstr;
+
+    memset(&P, 0, sizeof(P));
+    P.TSTR = sc.tstr; P.RSTR = sc.rstr; P.WMSTR = sc.wmstr; P.ALSTR = sc.alstr; P.VSTR = sc.vstr;
+    P.HSTR = sc.hstr; P.GASC = GASC; P.PBACK = sc.pback;
+    P.CONVRC = sc.convrc; P.CONVRM = sc.convrm; P.CONVRD = sc.convrd;
+    // ckrates.f:87-89, solveh.f:35-38
+    P.C1ST = sc.alstr / sc.vstr;
+    P.C2ND = sc.alstr / sc.vstr * (sc.rstr / sc.wmstr * 1.0e-06);
+    P.C3RD = sc.alstr / sc.vstr * (sc.rstr * sc.rstr / sc.wmstr / sc.wmstr * 1.0e-12);
+    P.RCONV = sc.vstr / sc.wmstr / sc.alstr * 1.0e-06;
+    P.HCONVR = GASC / sc.wmstr / sc.hstr;
+    P.TKDMIN = sc.tstr - 1.0;
+    P.RSTR_WMSTR = sc.rstr / sc.wmstr;
+    for (int k = 0; k < LSP; ++k) {   // main:461-464
+        P.WM[k] = uc_wsp[k] / 1000.0 / sc.wmstr;
+        P.HFO[k] = sc.hconv * uc_poly[k * 14 + 5] / P.WM[k];
+        P.cdia[k] = uc_cdia[k];
+    }
+    memcpy(P.poly, uc_poly, sizeof(P.poly));
+    memcpy(P.om22, uc_om22, sizeof(P.om22));
+    memcpy(P.ci11, uc_ci11, sizeof(P.ci11));
+    for (int i = 0; i < LSP; ++i)       // main:471-483
+        for (int j = 0; j < LSP; ++j) {
+            const int ij = i * LSP + j;
+            P.WMIK[ij] = (i == j) ? sqrt(P.WM[i]) : pow(P.WM[i] / P.WM[j], F32(0.25));
+            P.DWMIK[ij] = F32(2.828427125) * sqrt(1.0 + P.WM[i] / P.WM[j]);
+            const double ECDIA = F32(0.5) * (uc_cdia[i] + uc_cdia[j]);
+            P.WMCD[ij] = sqrt((P.WM[i] + P.WM[j]) / 2.0 / P.WM[i] / P.WM[j]) / ECDIA / ECDIA;
+            P.ETLJ1[ij] = sqrt(uc_tlj[i] * uc_tlj[j]);
+            P.ETLJ2[ij] = P.ETLJ1[ij] * P.ETLJ1[ij];
+            P.ETLJ3[ij] = P.ETLJ2[ij] * P.ETLJ1[ij];
+            P.ETLJ4[ij] = P.ETLJ3[ij] * P.ETLJ1[ij];
+        }
+    for (int g = 0; g < 11; ++g) { P.tb_off[g] = uc_tb_off[g]; P.tb_len[g] = uc_tb_len[g]; }
+    const int ntb = (int)(sizeof(uc_tb_sp) / sizeof(uc_tb_sp[0]));
+    for (int t = 0; t < ntb; ++t) {
+        P.tb_sp[t] = uc_tb_sp[t]; P.tb_sign[t] = uc_tb_sign[t];
+        P.tb_hascoef[t] = uc_tb_hascoef[t]; P.tb_coef[t] = uc_tb_coef[t];
+    }
+    for (int k = 0; k < LSP; ++k) {
+        P.prd_off[k] = uc_prd_off[k]; P.prd_len[k] = uc_prd_len[k];
+        P.loss_off[k] = uc_loss_off[k]; P.loss_len[k] = uc_loss_len[k];
+    }
+    memcpy(P.prd_term, uc_prd_term, sizeof(P.prd_term));
+    memcpy(P.prd_coef, uc_prd_coef, sizeof(P.prd_coef));
+    memcpy(P.loss_term, uc_loss_term, sizeof(P.loss_term));
+    memcpy(P.ra_len, uc_ra_len, sizeof(P.ra_len));
+    memcpy(P.ra_sp, uc_ra_sp, sizeof(P.ra_sp));
+
+    // reaction-pair table
+    tab.assign(NPAIR, PairTab{});
+    std::vector<double> pcost(NPAIR);
+    for (int p = 0; p < NPAIR; ++p) {
+        PairTab &T = tab[p];
+        memset(&T, 0, sizeof(T));
+        const int r0 = 2 * p, r1 = 2 * p + 1;
+        T.akf = AKF[r0]; T.alf = ALF[r0]; T.exaf = EXAF[r0]; T.akf_r = AKF[r1];
+        T.aklow = AKLOW[r0]; T.allow = ALLOW[r0]; T.ealow = EALOW[r0];
+        for (int c = 0; c < 4; ++c) T.troe[c] = TROE[r0][c];
+        T.has_rev = uc_rev_has[r1];
+        T.rut = uc_rev_rut[r1];
+        T.qlen = uc_rev_len[r1];
+        for (int t = 0; t < T.qlen; ++t) { T.qsp[t] = uc_rev_sp[r1 * UC_QMAX + t]; T.qdiv[t] = uc_rev_div[r1 * UC_QMAX + t]; }
+        T.dmole = uc_dmole_grp[r0];
+        T.rc_order0 = uc_rc_order[r0]; T.rc_order1 = uc_rc_order[r1];
+        T.rc_tb0 = uc_rc_tb[r0]; T.rc_tb1 = uc_rc_tb[r1];
+        T.rc_len0 = uc_rc_len[r0]; T.rc_len1 = uc_rc_len[r1];
+        for (int t = 0; t < 4; ++t) {
+            if (t < T.rc_len0) { T.rc_kind0[t] = uc_rc_kind[r0 * UC_PMAX + t]; T.rc_idx0[t] = uc_rc_idx[r0 * UC_PMAX + t]; }
+            if (t < T.rc_len1) { T.rc_kind1[t] = uc_rc_kind[r1 * UC_PMAX + t]; T.rc_idx1[t] = uc_rc_idx[r1 * UC_PMAX + t]; }
+        }
+        pcost[p] = 3.0 + (T.has_rev ? 1.0 + 0.5 * T.qlen : 0.0) + (T.aklow != 0.0 ? 6.0 : 0.0);
+    }
+    // balance pairs and species over the warps (longest first onto the least loaded warp)
+    auto balance = [](const std::vector<double> &cost, int nw, int cap, std::vector<std::vector<int>> &out) {
+        std::vector<int> idx(cost.size());
+        for (size_t i = 0; i < idx.size(); ++i) idx[i] = (int)i;
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+        std::vector<double> load(nw, 0.0);
+        out.assign(nw, {});
+        for (int i : idx) {
+            int best = -1;
+            for (int w = 0; w < nw; ++w)
+                if ((int)out[w].size() < cap && (best < 0 || load[w] < load[best])) best = w;
+            out[best].push_back(i);
+            load[best] += cost[i];
+        }
+        for (auto &v : out) std::sort(v.begin(), v.end());
+    };
+    std::vector<std::vector<int>> pw, sw;
+    balance(pcost, CHEM_WARPS, 24, pw);
+    for (int w = 0; w < CHEM_WARPS; ++w) {
+        P.npair_of_warp[w] = (int8_t)pw[w].size();
+        for (size_t i = 0; i < pw[w].size(); ++i) P.pair_of_warp[w][i] = (int16_t)pw[w][i];
+    }
+    std::vector<double> scost(LSP);
+    for (int k = 0; k < LSP; ++k) scost[k] = 8.0 + 2.0 * uc_prd_len[k] + 2.5 * uc_loss_len[k];
+    balance(scost, CHEM_WARPS, MAX_SPEC_PER_WARP, sw);
+    for (int w = 0; w < CHEM_WARPS; ++w) {
+        P.nspec_of_warp[w] = (int8_t)sw[w].size();
+        for (size_t i = 0; i < sw[w].size(); ++i) P.spec_of_warp[w][i] = (int8_t)sw[w][i];
+    }
+}
+
+// ------------------------------------------------------------------ helpers
+
+static void free_ctx(uc_ctx *c)
+{
+    if (!c) return;
+    double **bufs[] = {&c->tk, &c->rho, &c->y, &c->y0, &c->soot, &c->soot0, &c->rc, &c->sour, &c->qdsp,
+                       &c->qdot, &c->dwdy, &c->vmu, &c->vtc, &c->vdf, &c->cp, &c->h, &c->face_sum,
+                       &c->face_nbr, &c->ht, &c->partial};
+    for (auto b : bufs)
+        if (*b) { cudaFree(*b); *b = nullptr; }
+    if (c->dP) cudaFree(c->dP);
+    if (c->dTab) cudaFree(c->dTab);
+    if (c->status) cudaFree(c->status);
+    if (c->passes) cudaFree(c->passes);
+    for (auto e : c->ev_pool) cudaEventDestroy(e);
+    c->ev_pool.clear();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c->hP;
+}
+
+static int dalloc(uc_ctx *ctx, double **p, size_t count)
+{
+    if (*p) return UC_OK;
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(double));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return set_err(ctx, UC_E_NOMEM, "cudaMalloc of %zu doubles failed: %s", count, cudaGetErrorString(e));
+    }
+    return UC_OK;
+}
+
+// copies of the last real cell into the padding cells of a [rows][npad] array
+__global__ void pad_rows_kernel(double *a, int rows, int n, int npad)
+{
+    const int pad = npad - n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows * pad; i += gridDim.x * blockDim.x) {
+        const int r = i / pad, c = n + i % pad;
+        a[(size_t)r * npad + c] = a[(size_t)r * npad + n - 1];
+    }
+}
+
+static int upload_rows(uc_ctx *ctx, double *dst, const double *src, int rows)
+{
+    if (src) {
+        CK(cudaMemcpy2DAsync(dst, (size_t)ctx->npad * sizeof(double), src, (size_t)ctx->n * sizeof(double),
+                             (size_t)ctx->n * sizeof(double), rows, cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+        CK(cudaMemsetAsync(dst, 0, (size_t)rows * ctx->npad * sizeof(double), ctx->stream));
+    }
+    if (ctx->npad > ctx->n) {
+        pad_rows_kernel<<<64, 256, 0, ctx->stream>>>(dst, rows, ctx->n, ctx->npad);
+        CK(cudaGetLastError());
+    }
+    return UC_OK;
+}
+
+static int download_rows(uc_ctx *ctx, double *dst, const double *src, int rows)
+{
+    if (!dst) return UC_OK;
+    CK(cudaMemcpy2DAsync(dst, (size_t)ctx->n * sizeof(double), src, (size_t)ctx->npad * sizeof(double),
+                         (size_t)ctx->n * sizeof(double), rows, cudaMemcpyDeviceToHost, ctx->stream));
+    return UC_OK;
+}
+
+static int check_status(uc_ctx *ctx)
+{
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, ctx->status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (st == ST_TMA_TIMEOUT) {
+        CK(cudaMemsetAsync(ctx->status, 0, sizeof(int), ctx->stream));
+        return set_err(ctx, UC_E_TIMEOUT, "table staging (bulk copy) timed out on the device");
+    }
+    if (st == ST_NEWTON_NOCONV) {
+        CK(cudaMemsetAsync(ctx->status, 0, sizeof(int), ctx->stream));
+        return set_err(ctx, UC_E_NOCONV, "temperature Newton iteration did not converge in 100 steps for some cell");
+    }
+    return UC_OK;
+}
+
+#define RET_IF(x)                 \
+    do {                          \
+        int r_ = (x);             \
+        if (r_ != UC_OK) return r_; \
+    } while (0)
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
+{
+    if (!out) return UC_E_ARG;
+    *out = nullptr;
+    if (!in || ncell <= 0) return UC_E_ARG;
+    if (!(in->rtot > in->rtin) || !(in->vref > 0) || !(in->tref > 0) || !(in->pref > 0) ||
+        !(in->fo2in >= 0 && in->fo2in <= 1))
+        return UC_E_ARG;
+    uc_ctx *ctx = new (std::nothrow) uc_ctx();
+    if (!ctx) return UC_E_NOMEM;
+    int rc = UC_OK;
+    do {
+        cudaError_t e = cudaSetDevice(device);
+        if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e)); break; }
+        ctx->device = device;
+        cudaDeviceProp prop;
+        cudaGetDeviceProperties(&prop, device);
+        ctx->nsm = prop.multiProcessorCount;
+        e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "stream: %s", cudaGetErrorString(e)); break; }
+        ctx->n = ncell;
+        ctx->ntile = (ncell + TILE - 1) / TILE;
+        ctx->npad = ctx->ntile * TILE;
+        ctx->hP = new (std::nothrow) DevParams();
+        if (!ctx->hP) { rc = UC_E_NOMEM; break; }
+        std::vector<PairTab> tab;
+        build_params(*in, *ctx->hP, tab, ctx->sc);
+        if (cudaMalloc((void **)&ctx->dP, sizeof(DevParams)) != cudaSuccess ||
+            cudaMalloc((void **)&ctx->dTab, PAIRTAB_BYTES) != cudaSuccess ||
+            cudaMalloc((void **)&ctx->status, sizeof(int)) != cudaSuccess ||
+            cudaMalloc((void **)&ctx->passes, sizeof(int)) != cudaSuccess) {
+            rc = set_err(ctx, UC_E_NOMEM, "device allocation of the parameter block failed");
+            break;
+        }
+        cudaMemcpy(ctx->dP, ctx->hP, sizeof(DevParams), cudaMemcpyHostToDevice);
+        cudaMemcpy(ctx->dTab, tab.data(), PAIRTAB_BYTES, cudaMemcpyHostToDevice);
+        cudaMemset(ctx->status, 0, sizeof(int));
+        const size_t np = ctx->npad;
+        if ((rc = dalloc(ctx, &ctx->tk, np)) || (rc = dalloc(ctx, &ctx->rho, np)) ||
+            (rc = dalloc(ctx, &ctx->y, LSP * np)) || (rc = dalloc(ctx, &ctx->y0, LSP * np)) ||
+            (rc = dalloc(ctx, &ctx->soot, 2 * np)) || (rc = dalloc(ctx, &ctx->soot0, 2 * np)) ||
+            (rc = dalloc(ctx, &ctx->sour, 6 * np)))
+            break;
+        e = cudaFuncSetAttribute(chem_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CHEM_SMEM);
+        if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "smem attribute: %s", cudaGetErrorString(e)); break; }
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update_fp64_kernel, UPD_THREADS, 0);
+        if (per_sm < 1) per_sm = 1;
+        ctx->upd_grid = std::min(per_sm * ctx->nsm, std::max(1, (ctx->ntile + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32)));
+        if ((rc = dalloc(ctx, &ctx->partial, 2 * (size_t)per_sm * ctx->nsm))) break;
+        e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "init: %s", cudaGetErrorString(e)); break; }
+    } while (0);
+    if (rc != UC_OK) {
+        fprintf(stderr, "uc_init: %s\n", ctx->err);
+        free_ctx(ctx);
+        delete ctx;
+        return rc;
+    }
+    *out = ctx;
+    return UC_OK;
+}
+
+extern "C" int uc_get_scales(const uc_ctx *ctx, uc_scales *sc, double *wm, double *hfo)
+{
+    if (!ctx) return UC_E_ARG;
+    if (sc) *sc = ctx->sc;
+    if (wm) memcpy(wm, ctx->hP->WM, sizeof(double) * LSP);
+    if (hfo) memcpy(hfo, ctx->hP->HFO, sizeof(double) * LSP);
+    return UC_OK;
+}
+
+extern "C" int uc_upload_fields(uc_ctx *ctx, const double *tk, const double *rho, const double *fsp,
+                                const double *stmf, const double *stnd)
+{
+    if (!ctx || !tk || !rho || !fsp) return set_err(ctx, UC_E_ARG, "uc_upload_fields: tk, rho and fsp are required");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(upload_rows(ctx, ctx->tk, tk, 1));
+    RET_IF(upload_rows(ctx, ctx->rho, rho, 1));
+    RET_IF(upload_rows(ctx, ctx->y, fsp, LSP));
+    RET_IF(upload_rows(ctx, ctx->soot, stmf, 1));
+    RET_IF(upload_rows(ctx, ctx->soot + ctx->npad, stnd, 1));
+    CK(cudaMemcpyAsync(ctx->y0, ctx->y, (size_t)LSP * ctx->npad * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->soot0, ctx->soot, 2 * (size_t)ctx->npad * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->have_fields = true;
+    ctx->have_rc = false;
+    return UC_OK;
+}
+
+extern "C" int uc_download_fields(uc_ctx *ctx, double *tk, double *rho, double *fsp, double *stmf, double *stnd)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "no fields uploaded");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(download_rows(ctx, tk, ctx->tk, 1));
+    RET_IF(download_rows(ctx, rho, ctx->rho, 1));
+    RET_IF(download_rows(ctx, fsp, ctx->y, LSP));
+    RET_IF(download_rows(ctx, stmf, ctx->soot, 1));
+    RET_IF(download_rows(ctx, stnd, ctx->soot + ctx->npad, 1));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return UC_OK;
+}
+
+static int launch_chem(uc_ctx *ctx, int precision, bool want_rc, bool want_omega)
+{
+    if (precision != UC_FP64 && precision != UC_MIXED) return set_err(ctx, UC_E_ARG, "unknown precision %d", precision);
+    if (precision == UC_MIXED) return set_err(ctx, UC_E_ARG, "precision UC_MIXED is not built in this library version");
+    if (want_rc) RET_IF(dalloc(ctx, &ctx->rc, (size_t)LRX * ctx->npad));
+    if (want_omega) {
+        RET_IF(dalloc(ctx, &ctx->qdsp, (size_t)LSP * ctx->npad));
+        RET_IF(dalloc(ctx, &ctx->qdot, ctx->npad));
+        RET_IF(dalloc(ctx, &ctx->dwdy, (size_t)LSP * ctx->npad));
+    }
+    ChemArgs a{};
+    a.P = ctx->dP;
+    a.tab = ctx->dTab;
+    a.tk = ctx->tk; a.rho = ctx->rho; a.y = ctx->y; a.stmf = ctx->soot; a.stnd = ctx->soot + ctx->npad;
+    a.rc = want_rc ? ctx->rc : nullptr;
+    a.sour = ctx->sour;
+    a.qdsp = want_omega ? ctx->qdsp : nullptr;
+    a.qdot = want_omega ? ctx->qdot : nullptr;
+    a.dwdy = want_omega ? ctx->dwdy : nullptr;
+    a.n = ctx->n; a.npad = ctx->npad; a.ntile = ctx->ntile;
+    a.status = ctx->status;
+    const int grid = std::min(ctx->ntile, ctx->nsm);
+    int slot;
+    prof_begin(ctx, UC_K_CHEM, slot);
+    chem_fp64_kernel<<<grid, CHEM_THREADS, CHEM_SMEM, ctx->stream>>>(a);
+    prof_end(ctx, slot);
+    CK(cudaGetLastError());
+    return UC_OK;
+}
+
+extern "C" int uc_rates(uc_ctx *ctx, int precision, double *rc)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "uc_rates before uc_upload_fields");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(launch_chem(ctx, precision, true, false));
+    ctx->have_rc = true;
+    if (rc) {
+        RET_IF(download_rows(ctx, rc, ctx->rc, LRX));
+        CK(cudaStreamSynchronize(ctx->stream));
+        RET_IF(check_status(ctx));
+    }
+    return UC_OK;
+}
+
+extern "C" int uc_omega(uc_ctx *ctx, int precision, double *qdsp, double *qdot, double *domega_dy)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "uc_omega before uc_upload_fields");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(launch_chem(ctx, precision, false, true));
+    if (qdsp || qdot || domega_dy) {
+        RET_IF(download_rows(ctx, qdsp, ctx->qdsp, LSP));
+        RET_IF(download_rows(ctx, qdot, ctx->qdot, 1));
+        RET_IF(download_rows(ctx, domega_dy, ctx->dwdy, LSP));
+        RET_IF(check_status(ctx));
+    }
+    return UC_OK;
+}
+
+extern "C" int uc_props(uc_ctx *ctx, double *vmu, double *vtc, double *vdf)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "uc_props before uc_upload_fields");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(dalloc(ctx, &ctx->vmu, ctx->npad));
+    RET_IF(dalloc(ctx, &ctx->vtc, ctx->npad));
+    RET_IF(dalloc(ctx, &ctx->vdf, (size_t)LSP * ctx->npad));
+    PropArgs a{ctx->dP, ctx->tk, ctx->y, ctx->vmu, ctx->vtc, ctx->vdf, ctx->n, ctx->npad};
+    const int grid = std::min((ctx->n + 127) / 128, ctx->nsm * 16);
+    int slot;
+    prof_begin(ctx, UC_K_PROPS, slot);
+    props_fp64_kernel<<<grid, 128, 0, ctx->stream>>>(a);
+    prof_end(ctx, slot);
+    CK(cudaGetLastError());
+    if (vmu || vtc || vdf) {
+        RET_IF(download_rows(ctx, vmu, ctx->vmu, 1));
+        RET_IF(download_rows(ctx, vtc, ctx->vtc, 1));
+        RET_IF(download_rows(ctx, vdf, ctx->vdf, LSP));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return UC_OK;
+}
+
+extern "C" int uc_cp_h(uc_ctx *ctx, double *cp, double *h)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "uc_cp_h before uc_upload_fields");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(dalloc(ctx, &ctx->cp, ctx->npad));
+    RET_IF(dalloc(ctx, &ctx->h, ctx->npad));
+    CpHArgs a{ctx->dP, ctx->tk, ctx->y, ctx->cp, ctx->h, ctx->n, ctx->npad};
+    const int grid = std::min((ctx->n + 255) / 256, ctx->nsm * 8);
+    int slot;
+    prof_begin(ctx, UC_K_CPH, slot);
+    cp_h_fp64_kernel<<<grid, 256, 0, ctx->stream>>>(a);
+    prof_end(ctx, slot);
+    CK(cudaGetLastError());
+    if (cp || h) {
+        RET_IF(download_rows(ctx, cp, ctx->cp, 1));
+        RET_IF(download_rows(ctx, h, ctx->h, 1));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return UC_OK;
+}
+
+extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, double tol, double spnorm,
+                                 const double *face_sum, const double *face_nbr, int *passes)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->have_rc) return set_err(ctx, UC_E_STATE, "uc_species_update needs the RC plane of uc_rates");
+    if (isor < 1 || !(relx > 0.0) || !(dt >= 0.0)) return set_err(ctx, UC_E_ARG, "invalid isor/relx/dt");
+    CK(cudaSetDevice(ctx->device));
+    // old time level = state at the start of the update (SPGSOLV copies FSP -> SA, src/lib/spgsolv.f:177-231)
+    CK(cudaMemcpyAsync(ctx->y0, ctx->y, (size_t)LSP * ctx->npad * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->soot0, ctx->soot, 2 * (size_t)ctx->npad * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    const double *fs = nullptr, *fn = nullptr;
+    if (face_sum) {
+        RET_IF(dalloc(ctx, &ctx->face_sum, (size_t)(LSP - 1) * ctx->npad));
+        RET_IF(upload_rows(ctx, ctx->face_sum, face_sum, LSP - 1));
+        fs = ctx->face_sum;
+    }
+    if (face_nbr) {
+        RET_IF(dalloc(ctx, &ctx->face_nbr, (size_t)(LSP - 1) * ctx->npad));
+        RET_IF(upload_rows(ctx, ctx->face_nbr, face_nbr, LSP - 1));
+        fn = ctx->face_nbr;
+    }
+    UpdArgs a{};
+    a.P = ctx->dP; a.rc = ctx->rc; a.sour = ctx->sour; a.rho = ctx->rho; a.y0 = ctx->y0; a.soot0 = ctx->soot0;
+    a.face_sum = fs; a.face_nbr = fn; a.y = ctx->y; a.soot = ctx->soot; a.partial = ctx->partial;
+    a.passes = ctx->passes;
+    a.dt = dt; a.sor1 = relx; a.tol = tol; a.spnorm = spnorm > 0.0 ? spnorm : (double)ctx->n * (LSP - 1);
+    a.isor = isor; a.n = ctx->n; a.npad = ctx->npad; a.ntile = ctx->ntile;
+    void *args[] = {&a};
+    int slot;
+    prof_begin(ctx, UC_K_UPDATE, slot);
+    CK(cudaLaunchCooperativeKernel((void *)update_fp64_kernel, dim3(ctx->upd_grid), dim3(UPD_THREADS), args, 0,
+                                   ctx->stream));
+    prof_end(ctx, slot);
+    if (passes) {
+        CK(cudaMemcpyAsync(passes, ctx->passes, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    ctx->have_rc = false;   // the RC plane belongs to the state before the update
+    return UC_OK;
+}
+
+extern "C" int uc_temperature_from_h(uc_ctx *ctx, const double *ht)
+{
+    if (!ctx || !ht) return set_err(ctx, UC_E_ARG, "uc_temperature_from_h: ht is required");
+    if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "no fields uploaded");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(dalloc(ctx, &ctx->ht, ctx->npad));
+    RET_IF(upload_rows(ctx, ctx->ht, ht, 1));
+    TempArgs a{ctx->dP, ctx->y, ctx->ht, ctx->tk, ctx->status, ctx->n, ctx->npad};
+    const int grid = std::min((ctx->n + 127) / 128, ctx->nsm * 16);
+    int slot;
+    prof_begin(ctx, UC_K_TEMP, slot);
+    temperature_fp64_kernel<<<grid, 128, 0, ctx->stream>>>(a);
+    prof_end(ctx, slot);
+    CK(cudaGetLastError());
+    ctx->have_rc = false;
+    return check_status(ctx);
+}
+
+extern "C" int uc_sweep(uc_ctx *ctx, int precision, double dt, int isor, double relx, double tol, double spnorm,
+                        const double *face_sum, const double *face_nbr, int *passes)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "uc_sweep before uc_upload_fields");
+    RET_IF(uc_props(ctx, nullptr, nullptr, nullptr));
+    RET_IF(uc_cp_h(ctx, nullptr, nullptr));
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(launch_chem(ctx, precision, true, true));
+    ctx->have_rc = true;
+    return uc_species_update(ctx, dt, isor, relx, tol, spnorm, face_sum, face_nbr, passes);
+}
+
+extern "C" int uc_download_outputs(uc_ctx *ctx, double *qdsp, double *qdot, double *domega_dy, double *vmu,
+                                   double *vtc, double *vdf, double *cp, double *h)
+{
+    if (!ctx) return UC_E_ARG;
+    CK(cudaSetDevice(ctx->device));
+    struct { double *dst; double *src; int rows; const char *name; } o[] = {
+        {qdsp, ctx->qdsp, LSP, "qdsp"}, {qdot, ctx->qdot, 1, "qdot"}, {domega_dy, ctx->dwdy, LSP, "domega_dy"},
+        {vmu, ctx->vmu, 1, "vmu"}, {vtc, ctx->vtc, 1, "vtc"}, {vdf, ctx->vdf, LSP, "vdf"},
+        {cp, ctx->cp, 1, "cp"}, {h, ctx->h, 1, "h"}};
+    for (auto &x : o) {
+        if (!x.dst) continue;
+        if (!x.src) return set_err(ctx, UC_E_STATE, "%s has not been computed yet", x.name);
+        RET_IF(download_rows(ctx, x.dst, x.src, x.rows));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_status(ctx);
+}
+
+extern "C" int uc_profile(uc_ctx *ctx, int on)
+{
+    if (!ctx) return UC_E_ARG;
+    ctx->prof = on != 0;
+    ctx->ev_used.clear();
+    return UC_OK;
+}
+
+extern "C" int uc_profile_read(uc_ctx *ctx, double *ms, int *launches)
+{
+    if (!ctx || !ms || !launches) return UC_E_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < UC_K_COUNT; ++k) { ms[k] = 0.0; launches[k] = 0; }
+    for (auto &u : ctx->ev_used) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, ctx->ev_pool[u.second], ctx->ev_pool[u.second + 1]));
+        ms[u.first] += t;
+        launches[u.first] += 1;
+    }
+    ctx->ev_used.clear();
+    return UC_OK;
+}
+
+extern "C" int uc_sync(uc_ctx *ctx)
+{
+    if (!ctx) return UC_E_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_status(ctx);
+}
+
+extern "C" const char *uc_last_error(const uc_ctx *ctx)
+{
+    return ctx ? ctx->err : "null context";
+}
+
+extern "C" void uc_destroy(uc_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_ctx(ctx);
+    delete ctx;
+}
+
+extern "C" int uc_device_view_get(uc_ctx *ctx, uc_device_view *v)
+{
+    if (!ctx || !v) return UC_E_ARG;
+    v->tk = ctx->tk; v->rho = ctx->rho; v->fsp = ctx->y; v->fsp_old = ctx->y0;
+    v->stmf = ctx->soot; v->stnd = ctx->soot + ctx->npad;
+    v->rc = ctx->rc; v->qdsp = ctx->qdsp; v->qdot = ctx->qdot; v->domega_dy = ctx->dwdy;
+    v->vmu = ctx->vmu; v->vtc = ctx->vtc; v->vdf = ctx->vdf; v->cp = ctx->cp; v->h = ctx->h;
+    v->n = ctx->n; v->npad = ctx->npad;
+    v->stream = (void *)ctx->stream;
+    return UC_OK;
+}

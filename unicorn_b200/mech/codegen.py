@@ -1,0 +1,326 @@
+"""Generate the device-side mechanism tables and the species-update program.
+
+Build-time tool: reads ``sandiego52.json`` (written by ``extract.py``) and
+writes ``unicorn_b200/csrc/generated/mech_tables.h`` and
+``unicorn_b200/csrc/generated/update_program.cuh``.
+
+The species update of the reference (``src/lib/solvesp.f:85-2806``) keeps
+544 scalar "A-terms" per cell that are recomputed with one species factored
+out, multiplied by the freshly updated mass fraction, and reused by later
+species. On a GPU, 544 doubles per cell do not fit on chip, so the generator
+executes that statement sequence symbolically: every A-term becomes an
+expression tree over three kinds of leaves, RC(r), Y_j as it was at the
+start of the pass (``yo``) and Y_j after its own update in this pass
+(``yn``). Each production and loss term of each species is then emitted as
+that tree, with the reference's operand order, so the device code needs only
+RC, the old and the new Y of the cell.
+"""
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+LSP, LRX = 52, 544
+HERE = Path(__file__).resolve().parent
+MECH = HERE / "sandiego52.json"
+GEN = HERE.parent / "csrc" / "generated"
+
+
+# ------------------------------------------------------------------ symbolic update
+
+class Leaf:
+    __slots__ = ("kind", "idx", "val")
+
+    def __init__(self, kind, idx=0, val=0.0):
+        self.kind, self.idx, self.val = kind, idx, val
+
+    def c(self, ctx) -> str:
+        if self.kind == "RC":
+            return ctx.rc(self.idx)
+        if self.kind == "yo":
+            return f"YO({self.idx})"
+        if self.kind == "yn":
+            return f"YN({self.idx})"
+        if self.kind == "y0":
+            return f"Y0({self.idx})"
+        if self.kind == "SOUR":
+            return f"SOUR({self.idx})"
+        if self.kind == "num":
+            return repr(float(self.val))
+        raise ValueError(self.kind)
+
+
+class Mul:
+    __slots__ = ("a", "b")
+
+    def __init__(self, a, b):
+        self.a, self.b = a, b
+
+    def c(self, ctx) -> str:
+        return f"({self.a.c(ctx)} * {self.b.c(ctx)})"
+
+
+def leaves(e, out):
+    if isinstance(e, Mul):
+        leaves(e.a, out)
+        leaves(e.b, out)
+    else:
+        out.append(e)
+    return out
+
+
+def resolve_update(mech: dict) -> list[dict]:
+    """Symbolic execution of the per-cell update program.
+
+    Returns one dict per species block k (0-based) with expression trees for
+    the production sum (list of (sign, tree) or None = reuse the previous
+    block's value), the extra sum, and the loss sum (None = 0)."""
+    A: dict[int, object] = {}
+    updated: set[int] = set()
+
+    def yleaf(k0):
+        return Leaf("yn" if k0 in updated else "yo", k0)
+
+    def chain_tree(factors):
+        t = None
+        for f in factors:
+            kind = f[0]
+            if kind == "num":
+                x = Leaf("num", val=f[1])
+            elif kind == "Y":
+                x = yleaf(f[1] - 1)
+            elif kind == "Y0":
+                x = Leaf("y0", f[1] - 1)
+            elif kind == "RC":
+                x = Leaf("RC", f[1] - 1)
+            elif kind == "SOUR":
+                x = Leaf("SOUR", f[1] - 1)
+            elif kind == "A":
+                x = A[f[1]]
+            else:
+                raise ValueError(kind)
+            t = x if t is None else Mul(t, x)
+        return t
+
+    out = []
+    for b in mech["update"]["blocks"]:
+        k0 = b["species"] - 1
+        for r, fac in b["recompute"]:
+            A[r] = chain_tree(fac)
+        blk = {"species": k0}
+        blk["prod"] = None if b["prod"] is None else [(s, chain_tree(f)) for s, f in b["prod"]]
+        blk["extra"] = [(s, chain_tree(f)) for s, f in b["extra"]]
+        blk["loss"] = None if b["loss"] is None else [(s, chain_tree(f)) for s, f in b["loss"]]
+        out.append(blk)
+        updated.add(k0)
+        for r in b["multiply"]:
+            A[r] = Mul(Leaf("yn", k0), A[r])
+    return out
+
+
+def emit_sum(terms, ctx, acc: str) -> list[str]:
+    lines = []
+    for i, (s, t) in enumerate(terms):
+        v = t.c(ctx)
+        if i == 0:
+            lines.append(f"{acc} = {'' if s > 0 else '-'}{v};")
+        else:
+            lines.append(f"{acc} = {acc} {'+' if s > 0 else '-'} {v};")
+    return lines
+
+
+class _Ctx:
+    def rc(self, r0: int) -> str:
+        return f"RC({r0})"
+
+
+def gen_update_program(mech: dict) -> str:
+    blocks = resolve_update(mech)
+    ctx = _Ctx()
+    L = ["// Generated by unicorn_b200/mech/codegen.py from the update program of",
+         "// src/lib/solvesp.f:85-2806 (one block per species, in the reference's order).",
+         "// Requires accessor macros RC(r) (0-based reaction slot), YO(k) (Y at the",
+         "// start of the pass), YN(k) (Y after its own update), Y0(k) (old time level),",
+         "// SOUR(m), WM(k), FACE_SUM(k), FACE_NBR(k); scalars rho, dt, sor1, sor2, rsd;",
+         "// and UC_UPDATE_TAIL(k), which clips fnew and stores it as YN(k).",
+         "#pragma once",
+         "#define UC_UPDATE_PROGRAM() do { \\",
+         "    double prod = 0.0, extra, loss, rhs1, rhs2, ppp, fnew; \\"]
+    nterms = 0
+    for b in blocks:
+        k = b["species"]
+        body = []
+        if b["prod"] is not None:
+            body += emit_sum(b["prod"], ctx, "prod")
+            nterms += len(b["prod"])
+        body += emit_sum(b["extra"], ctx, "extra")
+        nterms += len(b["extra"])
+        body.append(f"rhs1 = rho * Y0({k}) + dt * WM({k}) * (prod + extra);")
+        if b["loss"] is None:
+            body.append("rhs2 = 0.0;")
+        else:
+            body += emit_sum(b["loss"], ctx, "loss")
+            nterms += len(b["loss"])
+            body.append(f"rhs2 = -(dt * WM({k}) * loss);")
+        body.append(f"ppp = rho - FACE_SUM({k});")
+        body.append(f"fnew = sor2 * YO({k}) + (rhs1 - FACE_NBR({k})) * sor1 / (ppp - rhs2);")
+        body.append(f"rsd += fabs(YO({k}) - fnew);")
+        body.append(f"UC_UPDATE_TAIL({k});")
+        L.append(f"    /* species {k + 1} */ \\")
+        L.extend("    " + x + " \\" for x in body)
+    L.append("} while (0)")
+    L.insert(6, f"// {nterms} production/extra/loss terms per cell and pass")
+    return "\n".join(L) + "\n"
+
+
+# ------------------------------------------------------------------ tables
+
+def fmt(v: float) -> str:
+    return repr(float(v)) if v == v else "0.0"
+
+
+def arr(name, ctype, vals, per_line=8) -> str:
+    vals = list(vals)
+    rows = []
+    for i in range(0, len(vals), per_line):
+        rows.append("    " + ", ".join(vals[i:i + per_line]))
+    return f"static const {ctype} {name}[{len(vals)}] = {{\n" + ",\n".join(rows) + "\n};\n"
+
+
+def gen_tables(mech: dict) -> str:
+    R = mech["reactions"]
+    out = ["// Generated by unicorn_b200/mech/codegen.py from sandiego52.json (the",
+           "// San Diego mechanism as UNICORN encodes it: src/lib/DATA.f, src/lib/ckrates.f,",
+           "// src/lib/solveh.f, src/unicornd-mild-sd-5.f:76-113). Do not edit.",
+           "#pragma once", "#include <stdint.h>",
+           f"#define UC_LSP {LSP}", f"#define UC_LRX {LRX}", f"#define UC_NPAIR {LRX // 2}",
+           f"#define UC_TPOL1 {fmt(mech['tpol'][0])}", f"#define UC_TPOL2 {fmt(mech['tpol'][1])}"]
+    out.append(arr("uc_wsp", "double", map(fmt, mech["wsp"])))
+    out.append(arr("uc_cdia", "double", map(fmt, mech["cdia"])))
+    out.append(arr("uc_tlj", "double", map(fmt, mech["tlj"])))
+    out.append(arr("uc_poly", "double", (fmt(v) for row in mech["poly"] for v in row)))
+    out.append(arr("uc_om22", "double", (fmt(v) for row in mech["omega22"] for v in row)))
+    out.append(arr("uc_ci11", "double", (fmt(v) for row in mech["ci11"] for v in row)))
+    for k in ("akf", "alf", "exaf", "aklow", "allow", "ealow"):
+        out.append(arr(f"uc_raw_{k}", "double", (fmt(x[k]) for x in R)))
+    out.append(arr("uc_raw_troe", "double", (fmt(v) for x in R for v in x["troe"])))
+    # reverse formulas: per even slot (0-based odd index r0), rut and q chain (<= 6 factors)
+    QMAX = max(len(v["q"]) for v in mech["reverse"].values())
+    rev_has, rev_rut, rev_len = [0] * LRX, [0] * LRX, [0] * LRX
+    rev_sp = [0] * (LRX * QMAX)
+    rev_div = [0] * (LRX * QMAX)
+    for key, rv in mech["reverse"].items():
+        r0 = int(key) - 1
+        rev_has[r0], rev_rut[r0], rev_len[r0] = 1, rv["rut"], len(rv["q"])
+        for t, (op, sp) in enumerate(rv["q"]):
+            rev_sp[r0 * QMAX + t] = sp - 1
+            rev_div[r0 * QMAX + t] = 1 if op == "/" else 0
+    out.append(f"#define UC_QMAX {QMAX}")
+    out.append(arr("uc_rev_has", "int8_t", map(str, rev_has), 32))
+    out.append(arr("uc_rev_rut", "int8_t", map(str, rev_rut), 32))
+    out.append(arr("uc_rev_len", "int8_t", map(str, rev_len), 32))
+    out.append(arr("uc_rev_sp", "int8_t", map(str, rev_sp), 32))
+    out.append(arr("uc_rev_div", "int8_t", map(str, rev_div), 32))
+    # third-body groups 1..10: TBODY + sum sign*coef*Y/W
+    tbn = [0] * 11
+    tbo = [0] * 11
+    tsp, tsg, tco, thc = [], [], [], []
+    for g in range(1, 11):
+        terms = mech["tb"][f"TB{g:03d}"][1:]
+        tbo[g], tbn[g] = len(tsp), len(terms)
+        for s, k, c in terms:
+            tsp.append(k - 1)
+            tsg.append(s)
+            tco.append(0.0 if c is None else c)
+            thc.append(0 if c is None else 1)
+    out.append(arr("uc_tb_off", "int16_t", map(str, tbo), 16))
+    out.append(arr("uc_tb_len", "int16_t", map(str, tbn), 16))
+    out.append(arr("uc_tb_sp", "int8_t", map(str, tsp), 32))
+    out.append(arr("uc_tb_sign", "int8_t", map(str, tsg), 32))
+    out.append(arr("uc_tb_coef", "double", map(fmt, tco)))
+    out.append(arr("uc_tb_hascoef", "int8_t", map(str, thc), 32))
+    dm = [0] * LRX
+    for key, g in mech["dmole"].items():
+        dm[int(key) - 1] = int(g[2:])
+    out.append(arr("uc_dmole_grp", "int8_t", map(str, dm), 32))
+    # RC assembly: order (0 = never written), tb (-1 none, 0 TBODY, g), post ops <= 4
+    PMAX = max(len(v["post"]) for v in mech["rc"].values())
+    rc_order, rc_tb, rc_len = [0] * LRX, [-1] * LRX, [0] * LRX
+    rc_kind = [0] * (LRX * PMAX)
+    rc_idx = [0] * (LRX * PMAX)
+    for key, rc in mech["rc"].items():
+        r0 = int(key) - 1
+        rc_order[r0] = rc["order"]
+        rc_tb[r0] = -1 if rc["tb"] is None else (0 if rc["tb"] == "TBODY" else int(rc["tb"][2:]))
+        rc_len[r0] = len(rc["post"])
+        for t, (op, kind, idx) in enumerate(rc["post"]):
+            rc_kind[r0 * PMAX + t] = 1 if kind == "Y" else 0   # 1: *Y_idx, 0: /W_idx
+            rc_idx[r0 * PMAX + t] = idx - 1
+    out.append(f"#define UC_PMAX {PMAX}")
+    out.append(arr("uc_rc_order", "int8_t", map(str, rc_order), 32))
+    out.append(arr("uc_rc_tb", "int8_t", map(str, rc_tb), 32))
+    out.append(arr("uc_rc_len", "int8_t", map(str, rc_len), 32))
+    out.append(arr("uc_rc_kind", "int8_t", map(str, rc_kind), 32))
+    out.append(arr("uc_rc_idx", "int8_t", map(str, rc_idx), 32))
+    # RA reactant lists (<= 3), 0 = slot never written
+    ra_len = [0] * LRX
+    ra_sp = [0] * (LRX * 3)
+    for key, sps in mech["ra"].items():
+        r0 = int(key) - 1
+        if sps is None:
+            continue
+        ra_len[r0] = len(sps)
+        for t, s in enumerate(sps):
+            ra_sp[r0 * 3 + t] = s - 1
+    out.append(arr("uc_ra_len", "int8_t", map(str, ra_len), 32))
+    out.append(arr("uc_ra_sp", "int8_t", map(str, ra_sp), 32))
+    # PRD term lists per species: packed (r0 | sign<<15 | coef_flag<<14), coef is 1.000 or SRA(0)
+    prd_off, prd_len, prd_term, prd_coef = [0] * LSP, [0] * LSP, [], []
+    loss_off, loss_len, loss_term = [0] * LSP, [0] * LSP, []
+    for key, terms in mech["prd"].items():
+        k0 = int(key) - 1
+        if not terms:
+            continue
+        prd_off[k0] = len(prd_term)
+        loss_off[k0] = len(loss_term)
+        for s, fac in terms:
+            kinds = [f[0] for f in fac]
+            if kinds == ["SRA"]:
+                # SRA(i) = 0.0 (src/lib/solveh.f:671-676): a zero term
+                prd_term.append((LRX) | ((1 if s < 0 else 0) << 15) | (1 << 13))
+                prd_coef.append(0.0)
+                continue
+            if kinds == ["RA"]:
+                coef, r = None, fac[0][1]
+            else:
+                assert kinds == ["num", "RA"], fac
+                coef, r = fac[0][1], fac[1][1]
+            prd_term.append((r - 1) | ((1 if s < 0 else 0) << 15) | ((1 if coef is not None else 0) << 14))
+            prd_coef.append(0.0 if coef is None else coef)
+            if s < 0:
+                assert coef is None, "loss terms carry no coefficient in this mechanism"
+                loss_term.append(r - 1)
+        prd_len[k0] = len(prd_term) - prd_off[k0]
+        loss_len[k0] = len(loss_term) - loss_off[k0]
+    out.append(arr("uc_prd_off", "int16_t", map(str, prd_off), 16))
+    out.append(arr("uc_prd_len", "int16_t", map(str, prd_len), 16))
+    out.append(arr("uc_prd_term", "uint16_t", map(str, prd_term), 16))
+    out.append(arr("uc_prd_coef", "double", map(fmt, prd_coef)))
+    out.append(arr("uc_loss_off", "int16_t", map(str, loss_off), 16))
+    out.append(arr("uc_loss_len", "int16_t", map(str, loss_len), 16))
+    out.append(arr("uc_loss_term", "uint16_t", map(str, loss_term), 16))
+    out.append(f"#define UC_NPRD_TERMS {len(prd_term)}")
+    out.append(f"#define UC_NLOSS_TERMS {len(loss_term)}")
+    return "\n".join(out) + "\n"
+
+
+def main():
+    mech = json.loads(MECH.read_text())
+    GEN.mkdir(parents=True, exist_ok=True)
+    (GEN / "mech_tables.h").write_text(gen_tables(mech))
+    (GEN / "update_program.cuh").write_text(gen_update_program(mech))
+    print(f"wrote {GEN / 'mech_tables.h'} and {GEN / 'update_program.cuh'}")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,255 @@
+"""Python host interface to ``libunichem.so`` (the C ABI of include/unichem.h).
+
+Mirrors the reference's hot-path routines by name and argument meaning:
+
+=======================  =====================================================
+``UniChem.ckrates``      CALL CKRATES (src/lib/ckrates.f) -> RC plane
+``UniChem.omega``        rate part of CALL SOLVEH (src/lib/solveh.f:116-1145)
+``UniChem.solvesp``      CALL SOLVESP(ISOR1,RELXSP,TOLRSP,SPNORM)
+``UniChem.props``        property block of PROGRAM UNICORN (main:821-1006)
+``UniChem.cp_h``         TCP of SPGSOLV (spgsolv.f:102-173) and HENTH sums
+``UniChem.temperature``  T from h (src/lib/solveh.f:1170-1234)
+=======================  =====================================================
+
+Arrays are numpy float64, species-major ``[52, n]`` (the Fortran layout
+``FSP(LJ,LI,LSP)`` flattened), non-dimensional as in the reference. There is
+no CPU fallback: without the CUDA library or a GPU every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+LSP, LRX = 52, 544
+FP64, MIXED = 0, 1
+LIB_PATH = Path(__file__).resolve().parent / "libunichem.so"
+
+UC_ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "call order", -4: "device timeout",
+             -5: "no convergence", -6: "out of device memory"}
+
+
+class UniChemError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"unichem error {code} ({UC_ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class Inputs(ctypes.Structure):
+    """Input-card values (docs/input.uni:4-5 of the reference)."""
+    _fields_ = [(k, ctypes.c_double) for k in ("rtin", "rtot", "vref", "tref", "pref", "rref", "fo2in")]
+
+
+SCALE_FIELDS = ["alstr", "vstr", "rstr", "pstr", "tstr", "tmstr", "amstr", "acstr", "dstr", "hstr", "cpstr",
+                "akstr", "epstr", "wmstr", "gasc", "beta1", "beta2", "beta3", "beta4", "rei", "pback", "hconv",
+                "convrc", "convrm", "convrd"]
+
+
+class Scales(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in SCALE_FIELDS]
+
+
+DEFAULT_INPUTS = dict(rtin=0.0, rtot=0.100, vref=10.0, tref=294.0, pref=1.0133e5, rref=1.225, fo2in=0.233)
+
+_lib = None
+
+
+def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
+    """Load libunichem.so; raises if it is missing (no CPU fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not Path(path).exists():
+        raise UniChemError(-2, f"{path} not found: build it with `python -m unicorn_b200.build`")
+    lib = ctypes.CDLL(str(path))
+    P = ctypes.POINTER(ctypes.c_double)
+    vp = ctypes.c_void_p
+    lib.uc_init.argtypes = [ctypes.POINTER(Inputs), ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    lib.uc_get_scales.argtypes = [vp, ctypes.POINTER(Scales), P, P]
+    lib.uc_upload_fields.argtypes = [vp, P, P, P, P, P]
+    lib.uc_download_fields.argtypes = [vp, P, P, P, P, P]
+    lib.uc_rates.argtypes = [vp, ctypes.c_int, P]
+    lib.uc_omega.argtypes = [vp, ctypes.c_int, P, P, P]
+    lib.uc_props.argtypes = [vp, P, P, P]
+    lib.uc_cp_h.argtypes = [vp, P, P]
+    lib.uc_species_update.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, P, P, ctypes.POINTER(ctypes.c_int)]
+    lib.uc_temperature_from_h.argtypes = [vp, P]
+    lib.uc_sweep.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                             ctypes.c_double, P, P, ctypes.POINTER(ctypes.c_int)]
+    lib.uc_download_outputs.argtypes = [vp, P, P, P, P, P, P, P, P]
+    lib.uc_profile.argtypes = [vp, ctypes.c_int]
+    lib.uc_profile_read.argtypes = [vp, P, ctypes.POINTER(ctypes.c_int)]
+    lib.uc_sync.argtypes = [vp]
+    lib.uc_last_error.argtypes = [vp]
+    lib.uc_last_error.restype = ctypes.c_char_p
+    lib.uc_destroy.argtypes = [vp]
+    lib.uc_destroy.restype = None
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _in(a, shape=None):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None and a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+@dataclass
+class Omega:
+    qdsp: np.ndarray        # [52, n] the reference's QDSP (= -omega)
+    qdot: np.ndarray        # [n]
+    domega_dy: np.ndarray   # [52, n]
+
+    @property
+    def omega(self) -> np.ndarray:
+        return -self.qdsp
+
+
+class UniChem:
+    """A device-resident field of n cells and the chemistry/property calls on it."""
+
+    def __init__(self, n: int, inputs: dict | None = None, device: int = 0):
+        self.lib = load_library()
+        inp = dict(DEFAULT_INPUTS)
+        inp.update(inputs or {})
+        self.inputs = inp
+        self.n = int(n)
+        h = ctypes.c_void_p()
+        rc = self.lib.uc_init(ctypes.byref(Inputs(**inp)), self.n, device, ctypes.byref(h))
+        if rc != 0:
+            raise UniChemError(rc, "uc_init failed (see stderr)")
+        self._h = h
+        sc = Scales()
+        self.wm = np.zeros(LSP)
+        self.hfo = np.zeros(LSP)
+        self._ck(self.lib.uc_get_scales(h, ctypes.byref(sc), _p(self.wm), _p(self.hfo)))
+        self.scales = {k.upper(): getattr(sc, k) for k in SCALE_FIELDS}
+
+    # ------------------------------------------------------------ plumbing
+    def _ck(self, rc: int):
+        if rc != 0:
+            raise UniChemError(rc, self.lib.uc_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.uc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------ state
+    def upload(self, tk, rho, y, stmf=None, stnd=None):
+        n = self.n
+        tk, rho, y = _in(tk, (n,)), _in(rho, (n,)), _in(y, (LSP, n))
+        stmf, stnd = _in(stmf, (n,)), _in(stnd, (n,))
+        self._ck(self.lib.uc_upload_fields(self._h, _p(tk), _p(rho), _p(y), _p(stmf), _p(stnd)))
+
+    def download(self):
+        n = self.n
+        tk, rho, y, s1, s2 = np.empty(n), np.empty(n), np.empty((LSP, n)), np.empty(n), np.empty(n)
+        self._ck(self.lib.uc_download_fields(self._h, _p(tk), _p(rho), _p(y), _p(s1), _p(s2)))
+        return tk, rho, y, s1, s2
+
+    def sync(self):
+        self._ck(self.lib.uc_sync(self._h))
+
+    # ------------------------------------------------------------ hot path
+    def ckrates(self, precision: int = FP64, return_rc: bool = False):
+        rc = np.empty((LRX, self.n)) if return_rc else None
+        self._ck(self.lib.uc_rates(self._h, precision, _p(rc)))
+        return rc
+
+    def omega(self, precision: int = FP64, download: bool = True):
+        if not download:
+            self._ck(self.lib.uc_omega(self._h, precision, None, None, None))
+            return None
+        q, qd, d = np.empty((LSP, self.n)), np.empty(self.n), np.empty((LSP, self.n))
+        self._ck(self.lib.uc_omega(self._h, precision, _p(q), _p(qd), _p(d)))
+        return Omega(q, qd, d)
+
+    def props(self, download: bool = True):
+        if not download:
+            self._ck(self.lib.uc_props(self._h, None, None, None))
+            return None
+        mu, lam, d = np.empty(self.n), np.empty(self.n), np.empty((LSP, self.n))
+        self._ck(self.lib.uc_props(self._h, _p(mu), _p(lam), _p(d)))
+        return mu, lam, d
+
+    def cp_h(self, download: bool = True):
+        if not download:
+            self._ck(self.lib.uc_cp_h(self._h, None, None))
+            return None
+        cp, h = np.empty(self.n), np.empty(self.n)
+        self._ck(self.lib.uc_cp_h(self._h, _p(cp), _p(h)))
+        return cp, h
+
+    def solvesp(self, dt: float, isor: int = 100, relx: float = 0.99, tol: float = 1e-8, spnorm: float = 0.0,
+                face_sum=None, face_nbr=None) -> int:
+        fs = _in(face_sum, (LSP - 1, self.n))
+        fn = _in(face_nbr, (LSP - 1, self.n))
+        passes = ctypes.c_int(0)
+        self._ck(self.lib.uc_species_update(self._h, dt, int(isor), relx, tol, spnorm, _p(fs), _p(fn),
+                                            ctypes.byref(passes)))
+        return passes.value
+
+    def sweep(self, dt: float, precision: int = FP64, isor: int = 100, relx: float = 0.99, tol: float = 1e-8,
+              spnorm: float = 0.0, face_sum=None, face_nbr=None) -> int:
+        """One species sweep: props, cp/h, rates + omega, point-implicit update."""
+        fs = _in(face_sum, (LSP - 1, self.n))
+        fn = _in(face_nbr, (LSP - 1, self.n))
+        passes = ctypes.c_int(0)
+        self._ck(self.lib.uc_sweep(self._h, precision, dt, int(isor), relx, tol, spnorm, _p(fs), _p(fn),
+                                   ctypes.byref(passes)))
+        return passes.value
+
+    def download_outputs(self, out: dict | None = None) -> dict:
+        """Copy omega, d(omega)/dY, QDOT, transport, cp and h of the last sweep to host arrays."""
+        n = self.n
+        if out is None:
+            out = dict(qdsp=np.empty((LSP, n)), qdot=np.empty(n), domega_dy=np.empty((LSP, n)), vmu=np.empty(n),
+                       vtc=np.empty(n), vdf=np.empty((LSP, n)), cp=np.empty(n), h=np.empty(n))
+        self._ck(self.lib.uc_download_outputs(self._h, *[_p(out.get(k)) for k in
+                                                         ("qdsp", "qdot", "domega_dy", "vmu", "vtc", "vdf", "cp", "h")]))
+        return out
+
+    def profile(self, on: bool = True):
+        self._ck(self.lib.uc_profile(self._h, int(on)))
+
+    def profile_read(self) -> dict:
+        """Device time (ms) and launches per kernel kind since the last read."""
+        ms = np.zeros(5)
+        cnt = (ctypes.c_int * 5)()
+        self._ck(self.lib.uc_profile_read(self._h, _p(ms), cnt))
+        names = ["chem", "update", "props", "cp_h", "temperature"]
+        return {nm: (float(ms[i]), int(cnt[i])) for i, nm in enumerate(names)}
+
+    def temperature(self, ht):
+        """T from h; a cell whose Newton iteration ran out of steps is reported
+        as a warning, as the reference prints one and carries on."""
+        import warnings
+        ht = _in(ht, (self.n,))
+        rc = self.lib.uc_temperature_from_h(self._h, _p(ht))
+        if rc == -5:
+            warnings.warn(self.lib.uc_last_error(self._h).decode())
+        else:
+            self._ck(rc)
