@@ -125,6 +125,8 @@ def run_ours(args, rank, world, dev):
     from unicorn_b200 import unichem
     from unicorn_b200.fields import jet_field, nondimensional
     f = jet_field(NZ, NR, fuel=FUEL, t_peak=TPEAK, seed=rank)
+    if args.cells:
+        f.T, f.p, f.y = f.T[:args.cells].copy(), f.p[:args.cells].copy(), np.ascontiguousarray(f.y[:, :args.cells])
     n = f.n
     u = unichem.UniChem(n, device=dev)
     tk, rho = nondimensional(f, u.scales, u.wm)
@@ -142,7 +144,7 @@ def run_ours(args, rank, world, dev):
         u.upload(h_tk, h_rho, h_y)
 
     def step_device():
-        return u.sweep(DT, isor=ISOR, relx=RELX, tol=TOL)
+        return u.sweep(DT, isor=args.isor, relx=RELX, tol=TOL)
 
     passes_seen = []
     reset()
@@ -171,7 +173,7 @@ def run_ours(args, rank, world, dev):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         u.upload(h_tk, h_rho, h_y)
-        u.sweep(DT, isor=ISOR, relx=RELX, tol=TOL)
+        u.sweep(DT, isor=args.isor, relx=RELX, tol=TOL)
         u.download_outputs(outs)
         u.lib.uc_download_fields(u._h, None, None, unichem._p(h_yout), None, None)
     u.sync()
@@ -345,6 +347,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cells", type=int, default=0, help="use only the first N cells (profiling runs)")
+    ap.add_argument("--isor", type=int, default=ISOR, help="update passes cap (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         main_reference(args)
