@@ -163,6 +163,47 @@ typedef struct {
 } uc_device_view;
 int uc_device_view_get(uc_ctx *ctx, uc_device_view *v);
 
+/* ---------------------------------------------------------------------------
+ * Species update on caller-owned device arrays, with no device allocation.
+ *
+ * This entry point has no counterpart in the reference; it exists for callers
+ * that cannot let a library call cudaMalloc: hosts whose device memory all
+ * comes from their own allocator or pool (a Fortran code with CUDA Fortran or
+ * OpenACC device arrays, a solver held to a fixed memory budget), or code on
+ * a path where allocation is not allowed. It runs the same point-implicit
+ * update as uc_species_update, but every array is the caller's and the only
+ * scratch (the per-block residual partial sums and the pass counter) is a
+ * fixed array inside the library: UC_NOALLOC_MAX_BLOCKS doubles x 2 plus one
+ * int (16 KiB + 4 B per GPU that loads the library, held until process exit).
+ *
+ *  - ctx supplies the mechanism tables, scales and the CUDA stream; it must
+ *    come from uc_init (which is where allocation happens, once, at set-up).
+ *  - a->n cells with row stride a->npad (npad >= n, a multiple of 32);
+ *    rc [544][npad] as written by uc_rates, sour [6][npad], rho [npad],
+ *    y0 [52][npad] and soot0 [2][npad] the old time level, y [52][npad] and
+ *    soot [2][npad] updated in place, face_sum/face_nbr [51][npad] or NULL.
+ *    Padding cells (n..npad-1) are read and must hold finite values.
+ *  - Returns UC_E_ARG if npad is not a multiple of 32 or below n, or if the
+ *    device would need more than UC_NOALLOC_MAX_BLOCKS cooperating blocks.
+ *  - The first call on a device looks up the scratch array's device address
+ *    (cudaGetSymbolAddress, with that device current); make that first call
+ *    before any stream capture.
+ *  - All calls share the one scratch array and it keeps the last call's
+ *    contents; nothing in it has to start at zero (every partial sum is written
+ *    before it is read). Calls that overlap on the GPU, from any context or
+ *    stream, race on it: serialise them.
+ *  - passes (host pointer, may be NULL) receives the pass count; giving it
+ *    makes the call wait for the update to finish.
+ */
+#define UC_NOALLOC_MAX_BLOCKS 1024
+typedef struct {
+    int n, npad;
+    const double *rc, *sour, *rho, *y0, *soot0, *face_sum, *face_nbr;
+    double *y, *soot;
+} uc_update_arrays;
+int uc_species_update_noalloc(uc_ctx *ctx, const uc_update_arrays *a, double dt, int isor, double relx,
+                              double tol, double spnorm, int *passes);
+
 #ifdef __cplusplus
 }
 #endif

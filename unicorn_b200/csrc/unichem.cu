@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -680,5 +681,77 @@ extern "C" int uc_device_view_get(uc_ctx *ctx, uc_device_view *v)
     v->vmu = ctx->vmu; v->vtc = ctx->vtc; v->vdf = ctx->vdf; v->cp = ctx->cp; v->h = ctx->h;
     v->n = ctx->n; v->npad = ctx->npad;
     v->stream = (void *)ctx->stream;
+    return UC_OK;
+}
+
+// ------------------------------------------------------------------ no-allocation update
+
+// Scratch of uc_species_update_noalloc: residual partial sums of the
+// cooperating blocks (two halves, alternating by pass) and the pass counter.
+// It lives in the library image, so the call never allocates device memory.
+static __device__ __align__(256) double uc_noalloc_partial[2 * UC_NOALLOC_MAX_BLOCKS];
+static __device__ __align__(256) int uc_noalloc_passes;
+
+// Device addresses of the two arrays, looked up once per device (host code
+// may not use the symbols themselves as device pointers).
+static std::mutex g_noalloc_mu;
+static double *g_noalloc_partial[64];
+static int *g_noalloc_passes[64];
+
+static int noalloc_scratch(uc_ctx *ctx, double **partial, int **passes)
+{
+    const int dev = ctx->device;
+    if (dev < 0 || dev >= 64) return set_err(ctx, UC_E_ARG, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_partial[dev]) {
+        CK(cudaSetDevice(dev));
+        double *p = nullptr;
+        int *q = nullptr;
+        CK(cudaGetSymbolAddress((void **)&p, uc_noalloc_partial));
+        CK(cudaGetSymbolAddress((void **)&q, uc_noalloc_passes));
+        g_noalloc_partial[dev] = p;
+        g_noalloc_passes[dev] = q;
+    }
+    *partial = g_noalloc_partial[dev];
+    *passes = g_noalloc_passes[dev];
+    return UC_OK;
+}
+
+extern "C" int uc_species_update_noalloc(uc_ctx *ctx, const uc_update_arrays *arr, double dt, int isor,
+                                         double relx, double tol, double spnorm, int *passes)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!arr || !arr->rc || !arr->sour || !arr->rho || !arr->y0 || !arr->soot0 || !arr->y || !arr->soot)
+        return set_err(ctx, UC_E_ARG, "uc_species_update_noalloc: a required device array is NULL");
+    if (arr->n <= 0 || arr->npad < arr->n || arr->npad % TILE != 0)
+        return set_err(ctx, UC_E_ARG, "uc_species_update_noalloc: need 0 < n <= npad and npad a multiple of %d "
+                                      "(n=%d, npad=%d)", TILE, arr->n, arr->npad);
+    if (isor < 1 || !(relx > 0.0) || !(dt >= 0.0)) return set_err(ctx, UC_E_ARG, "invalid isor/relx/dt");
+    CK(cudaSetDevice(ctx->device));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update_fp64_kernel, UPD_THREADS, 0));
+    const int max_grid = std::max(1, per_sm) * ctx->nsm;
+    if (max_grid > UC_NOALLOC_MAX_BLOCKS)
+        return set_err(ctx, UC_E_ARG, "uc_species_update_noalloc: this device needs %d cooperating blocks, "
+                                      "more than the %d the fixed scratch holds", max_grid, UC_NOALLOC_MAX_BLOCKS);
+    double *partial = nullptr;
+    int *dpasses = nullptr;
+    RET_IF(noalloc_scratch(ctx, &partial, &dpasses));
+    CK(cudaSetDevice(ctx->device));
+    const int ntile = arr->npad / TILE;
+    UpdArgs a{};
+    a.P = ctx->dP; a.rc = arr->rc; a.sour = arr->sour; a.rho = arr->rho; a.y0 = arr->y0; a.soot0 = arr->soot0;
+    a.face_sum = arr->face_sum; a.face_nbr = arr->face_nbr; a.y = arr->y; a.soot = arr->soot;
+    a.partial = partial;
+    a.passes = dpasses;
+    a.dt = dt; a.sor1 = relx; a.tol = tol; a.spnorm = spnorm > 0.0 ? spnorm : (double)arr->n * (LSP - 1);
+    a.isor = isor; a.n = arr->n; a.npad = arr->npad; a.ntile = ntile;
+    const int grid = std::min(max_grid, std::max(1, (ntile + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32)));
+    void *args[] = {&a};
+    CK(cudaLaunchCooperativeKernel((void *)update_fp64_kernel, dim3(grid), dim3(UPD_THREADS), args, 0, ctx->stream));
+    if (passes) {
+        CK(cudaMemcpyAsync(passes, dpasses, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     return UC_OK;
 }
