@@ -21,6 +21,7 @@ extern "C" int harness_update(int n, const double *rho_a, const double *y0_a, do
             for (int m = 0; m < 6; ++m) sour[m] = sour_a[m * n + c];
             const double rho = rho_a[c];
 #define RC(r) rc_a[(r) * n + c]
+#define RC_LAST(r) rc_a[(r) * n + c]
 #define YO(k) yo[k]
 #define YN(k) yn[k]
 #define Y0(k) y0[k]
@@ -28,6 +29,8 @@ extern "C" int harness_update(int n, const double *rho_a, const double *y0_a, do
 #define WM(k) wm[k]
 #define FACE_SUM(k) 0.0
 #define FACE_NBR(k) 0.0
+#define UC_UPDATE_SYNC() do { } while (0)
+#define UC_UPDATE_BLOCK_BEGIN(b) do { } while (0)
 #define UC_UPDATE_TAIL(k) do { if (fnew < 0.0) fnew = 0.0; yn[k] = fnew; } while (0)
 #include "../unicorn_b200/csrc/generated/update_program.cuh"
             UC_UPDATE_PROGRAM();

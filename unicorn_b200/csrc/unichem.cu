@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -373,8 +374,11 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
             break;
         e = cudaFuncSetAttribute(chem_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CHEM_SMEM);
         if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "smem attribute: %s", cudaGetErrorString(e)); break; }
+        e = cudaFuncSetAttribute(update_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UPD_SMEM);
+        if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "smem attribute: %s", cudaGetErrorString(e)); break; }
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update_fp64_kernel, UPD_THREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update_fp64_kernel, UPD_THREADS, UPD_SMEM);
+        if (const char *cap = getenv("UNICHEM_UPD_CTAS_PER_SM")) per_sm = std::min(per_sm, std::max(1, atoi(cap)));
         if (per_sm < 1) per_sm = 1;
         ctx->upd_grid = std::min(per_sm * ctx->nsm, std::max(1, (ctx->ntile + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32)));
         if ((rc = dalloc(ctx, &ctx->partial, 2 * (size_t)per_sm * ctx->nsm))) break;
@@ -568,7 +572,7 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
     void *args[] = {&a};
     int slot;
     prof_begin(ctx, UC_K_UPDATE, slot);
-    CK(cudaLaunchCooperativeKernel((void *)update_fp64_kernel, dim3(ctx->upd_grid), dim3(UPD_THREADS), args, 0,
+    CK(cudaLaunchCooperativeKernel((void *)update_fp64_kernel, dim3(ctx->upd_grid), dim3(UPD_THREADS), args, UPD_SMEM,
                                    ctx->stream));
     prof_end(ctx, slot);
     if (passes) {
@@ -729,7 +733,7 @@ extern "C" int uc_species_update_noalloc(uc_ctx *ctx, const uc_update_arrays *ar
     if (isor < 1 || !(relx > 0.0) || !(dt >= 0.0)) return set_err(ctx, UC_E_ARG, "invalid isor/relx/dt");
     CK(cudaSetDevice(ctx->device));
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update_fp64_kernel, UPD_THREADS, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update_fp64_kernel, UPD_THREADS, UPD_SMEM));
     const int max_grid = std::max(1, per_sm) * ctx->nsm;
     if (max_grid > UC_NOALLOC_MAX_BLOCKS)
         return set_err(ctx, UC_E_ARG, "uc_species_update_noalloc: this device needs %d cooperating blocks, "
@@ -748,7 +752,8 @@ extern "C" int uc_species_update_noalloc(uc_ctx *ctx, const uc_update_arrays *ar
     a.isor = isor; a.n = arr->n; a.npad = arr->npad; a.ntile = ntile;
     const int grid = std::min(max_grid, std::max(1, (ntile + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32)));
     void *args[] = {&a};
-    CK(cudaLaunchCooperativeKernel((void *)update_fp64_kernel, dim3(grid), dim3(UPD_THREADS), args, 0, ctx->stream));
+    CK(cudaLaunchCooperativeKernel((void *)update_fp64_kernel, dim3(grid), dim3(UPD_THREADS), args, UPD_SMEM,
+                                   ctx->stream));
     if (passes) {
         CK(cudaMemcpyAsync(passes, dpasses, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));

@@ -1,14 +1,20 @@
 // Point-implicit species update (src/lib/solvesp.f), FP64.
 //
-// Lane = cell; every warp walks 32-cell tiles. The per-cell update program
-// is generated (generated/update_program.cuh) from the reference's statement
-// sequence with its A-terms resolved into products of RC, the pass-start Y
-// (YO) and the freshly updated Y (YN), so only those live per cell. RC
-// comes from the plane written by the rate kernel ([544][npad], coalesced
-// per warp). The relaxation passes run inside one cooperative launch: the
-// residual sum|dY| is reduced per block, the blocks meet at a grid barrier,
-// and every block sums the partials in the same order, so all of them take
-// the same convergence decision (src/lib/solvesp.f:2833).
+// Lane = cell; each warp of a CTA walks its own 32-cell tiles. The per-cell
+// update program is generated (generated/update_program.cuh) from the
+// reference's statement sequence with its A-terms resolved into products of
+// RC, the pass-start Y (YO) and the freshly updated Y (YN). Both Y sets live
+// in shared memory ([52][32] per warp each), so registers go to keeping RC
+// loads in flight. The warps of a CTA can run the program in lockstep (a
+// barrier after every species) so that the instruction cache holds only the code of
+// the current species (optional, see UC_LOCKSTEP); RC (the plane written by
+// the rate kernel, [544][npad]) is read with loads that do not allocate in L1
+// and tell L2 whether the line is read again in the pass.
+//
+// The relaxation passes run inside one cooperative launch: the residual
+// sum|dY| is reduced per CTA, the CTAs meet at a grid barrier, and every CTA
+// sums the partials in the same order, so all take the same convergence
+// decision (src/lib/solvesp.f:2833).
 #pragma once
 #include <cooperative_groups.h>
 
@@ -28,43 +34,120 @@ struct UpdArgs {
     int isor, n, npad, ntile;
 };
 
-constexpr int UPD_THREADS = 128;
+#ifndef UC_UPD_WARPS
+#define UC_UPD_WARPS 8
+#endif
+#ifndef UC_L2_HINTS
+#define UC_L2_HINTS 1
+#endif
+// Measured on B200 (C2 field, 20 passes): an L2 prefetch of the next
+// species' RC rows (UC_PF = 1, 2, 4) costs 0.82-0.84 ms/pass against 0.65
+// without, and a barrier after every species (UC_LOCKSTEP) changes nothing,
+// so both are off; the options stay for re-measurement on other parts.
+#ifndef UC_PF
+#define UC_PF 0          // species blocks of look-ahead for an L2 prefetch of RC rows (0: none)
+#endif
+#ifndef UC_LOCKSTEP
+#define UC_LOCKSTEP 0    // barrier after every species block
+#endif
+constexpr int UPD_WARPS = UC_UPD_WARPS;
+constexpr int UPD_THREADS = UPD_WARPS * 32;
+constexpr size_t UPD_SMEM = (size_t)UPD_WARPS * 2 * LSP * TILE * sizeof(double);
 
-__global__ void __launch_bounds__(UPD_THREADS) update_fp64_kernel(const UpdArgs a)
+// Read-only loads that skip L1 and carry an L2 eviction priority: lines that
+// are read again later in the pass are kept (evict_last), the last read of a
+// line in the pass lets it go first (evict_first).
+__device__ __forceinline__ uint64_t l2_policy_keep()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_drop()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ double ld_hint(const double *p, uint64_t pol)
+{
+    double v;
+#if UC_L2_HINTS
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+#else
+    asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+#endif
+    return v;
+}
+
+// Prefetch into L2 the RC rows (256 B per 32-cell tile row) that species
+// block b of the program reads; each lane pair takes one row, 16 rows per step.
+__device__ __forceinline__ void prefetch_block_rows(int b, const double *tile_base, size_t np, int lane)
+{
+    const int o = uc_upd_row_off[b], e = uc_upd_row_off[b + 1];
+    for (int i = o + (lane >> 1); i < e; i += 16) {
+        const double *p = tile_base + (size_t)uc_upd_rows[i] * np + (lane & 1) * 16;
+        asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(p));
+    }
+}
+
+__global__ void __launch_bounds__(UPD_THREADS, 1) update_fp64_kernel(const UpdArgs a)
 {
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
-    __shared__ double s_part[UPD_THREADS / 32];
+    extern __shared__ __align__(128) double s_upd[];
+    __shared__ double s_part[UPD_WARPS];
     const DevParams &P = *a.P;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int gwarp = (blockIdx.x * UPD_THREADS + threadIdx.x) >> 5;
-    const int nwarp = (gridDim.x * UPD_THREADS) >> 5;
+    double *syo = s_upd + (size_t)wib * 2 * LSP * TILE + lane;   // YO(k) = syo[k*32]
+    double *syn = syo + LSP * TILE;                              // YN(k) = syn[k*32]
+    const int nwarp = gridDim.x * UPD_WARPS;
+    const int gwarp = blockIdx.x * UPD_WARPS + wib;
+    const int rounds = (a.ntile + nwarp - 1) / nwarp;            // same trip count for every warp of the grid
     const double sor1 = a.sor1, sor2 = 1.0 - a.sor1, dt = a.dt;
     const size_t np = a.npad;
+    const uint64_t keep = l2_policy_keep(), drop = l2_policy_drop();
     int pass;
     for (pass = 1; pass <= a.isor; ++pass) {
         double rsd = 0.0;
-        for (int tile = gwarp; tile < a.ntile; tile += nwarp) {
+        for (int round = 0; round < rounds; ++round) {
+            int tile = gwarp + round * nwarp;
+            const bool own = tile < a.ntile;            // warps without a tile repeat the last one, unstored
+            if (!own) tile = a.ntile - 1;
             const size_t cell = (size_t)tile * TILE + lane;
-            const bool live = cell < (size_t)a.n;
-            double yo[LSP], yn[LSP];
-#pragma unroll
-            for (int k = 0; k < LSP - 1; ++k) { yo[k] = a.y[k * np + cell]; yn[k] = 0.0; }
+            const bool live = own && cell < (size_t)a.n;
+            for (int k = 0; k < LSP - 1; ++k) syo[k * TILE] = a.y[k * np + cell];
             const double rho = a.rho[cell];
             double crsd = 0.0;
             {
                 double &rsd = crsd;
-#define RC(r) __ldg(a.rc + (size_t)(r) * np + cell)
-#define YO(k) yo[k]
-#define YN(k) yn[k]
-#define Y0(k) __ldg(a.y0 + (size_t)(k) * np + cell)
-#define SOUR(m) __ldg(a.sour + (size_t)(m) * np + cell)
+#define RC(r) ld_hint(a.rc + (size_t)(r) * np + cell, keep)
+#define RC_LAST(r) ld_hint(a.rc + (size_t)(r) * np + cell, drop)
+#define YO(k) syo[(k) * TILE]
+#define YN(k) syn[(k) * TILE]
+#define Y0(k) ld_hint(a.y0 + (size_t)(k) * np + cell, drop)
+#define SOUR(m) ld_hint(a.sour + (size_t)(m) * np + cell, drop)
 #define WM(k) P.WM[k]
-#define FACE_SUM(k) (a.face_sum ? a.face_sum[(size_t)(k) * np + cell] : 0.0)
-#define FACE_NBR(k) (a.face_nbr ? a.face_nbr[(size_t)(k) * np + cell] : 0.0)
-#define UC_UPDATE_TAIL(k) do { if (fnew < 0.0) fnew = 0.0; yn[k] = fnew; } while (0)
+#define FACE_SUM(k) (a.face_sum ? __ldg(a.face_sum + (size_t)(k) * np + cell) : 0.0)
+#define FACE_NBR(k) (a.face_nbr ? __ldg(a.face_nbr + (size_t)(k) * np + cell) : 0.0)
+#define UC_UPDATE_TAIL(k) do { if (fnew < 0.0) fnew = 0.0; syn[(k) * TILE] = fnew; } while (0)
+#if UC_LOCKSTEP
+#define UC_UPDATE_SYNC() __syncthreads()
+#else
+#define UC_UPDATE_SYNC() do { } while (0)
+#endif
+#if UC_PF > 0
+#define UC_UPDATE_BLOCK_BEGIN(b) do { if ((b) + UC_PF < UC_UPD_NBLOCKS) prefetch_block_rows((b) + UC_PF, rc_tile, np, lane); } while (0)
+#else
+#define UC_UPDATE_BLOCK_BEGIN(b) do { } while (0)
+#endif
+                const double *rc_tile = a.rc + (size_t)tile * TILE;
+#if UC_PF > 0
+                for (int b0 = 0; b0 < UC_PF && b0 < UC_UPD_NBLOCKS; ++b0) prefetch_block_rows(b0, rc_tile, np, lane);
+#endif
                 UC_UPDATE_PROGRAM();
 #undef RC
+#undef RC_LAST
 #undef YO
 #undef YN
 #undef Y0
@@ -73,36 +156,38 @@ __global__ void __launch_bounds__(UPD_THREADS) update_fp64_kernel(const UpdArgs 
 #undef FACE_SUM
 #undef FACE_NBR
 #undef UC_UPDATE_TAIL
+#undef UC_UPDATE_SYNC
+#undef UC_UPDATE_BLOCK_BEGIN
                 // soot mass fraction and number density (solvesp.f:2807-2832)
                 const double s1 = a.soot[cell], s2 = a.soot[np + cell];
                 const double so0 = a.sour[cell], so1 = a.sour[np + cell], so2 = a.sour[2 * np + cell],
                              so3 = a.sour[3 * np + cell], so4 = a.sour[4 * np + cell], so5 = a.sour[5 * np + cell];
+                const double y2 = syn[1 * TILE], y4 = syn[3 * TILE], y5 = syn[4 * TILE], y22 = syn[21 * TILE];
                 double rhs1 = rho * a.soot0[cell] + dt * ((double)0.012011f / P.WMSTR) *
-                                                        (2.0 * so0 * yn[21] - so2 * yn[1] - so3 * yn[4] - so4 * yn[3]);
+                                                        (2.0 * so0 * y22 - so2 * y2 - so3 * y5 - so4 * y4);
                 double fnew = sor2 * s1 + rhs1 * sor1 / ((rho - 0.0) - 0.0);
                 crsd += fabs(s1 - fnew);
                 if (fnew < 0.0) fnew = 0.0;
                 const double n1 = fnew;
-                rhs1 = rho * a.soot0[np + cell] + dt * so1 * yn[21];
+                rhs1 = rho * a.soot0[np + cell] + dt * so1 * y22;
                 const double rhs2 = -(dt * so5);
                 fnew = sor2 * s2 + rhs1 * sor1 / ((rho - 0.0) - rhs2);
                 if (fnew < 0.0) fnew = 0.0;
                 if (live) {
-#pragma unroll
-                    for (int k = 0; k < LSP - 1; ++k) a.y[k * np + cell] = yn[k];
+                    for (int k = 0; k < LSP - 1; ++k) a.y[k * np + cell] = syn[k * TILE];
                     a.soot[cell] = n1;
                     a.soot[np + cell] = fnew;
                 }
             }
             if (live) rsd += crsd;
         }
-        // deterministic block reduction of the residual
+        // deterministic CTA reduction of the residual
         for (int o = 16; o > 0; o >>= 1) rsd += __shfl_xor_sync(0xffffffffu, rsd, o);
         if (lane == 0) s_part[wib] = rsd;
         __syncthreads();
         if (threadIdx.x == 0) {
             double b = 0.0;
-            for (int w = 0; w < UPD_THREADS / 32; ++w) b += s_part[w];
+            for (int w = 0; w < UPD_WARPS; ++w) b += s_part[w];
             a.partial[(pass & 1) * gridDim.x + blockIdx.x] = b;
         }
         grid.sync();

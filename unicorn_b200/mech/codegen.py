@@ -130,26 +130,59 @@ def emit_sum(terms, ctx, acc: str) -> list[str]:
 
 
 class _Ctx:
+    """Emission context: the last use of each RC(r) in a pass is emitted as
+    RC_LAST(r), so the device code can tell L2 that the line will not be
+    needed again this pass."""
+
+    def __init__(self, last_use: dict | None = None):
+        self.last_use = last_use or {}
+        self.count: dict[int, int] = {}
+
     def rc(self, r0: int) -> str:
+        self.count[r0] = self.count.get(r0, 0) + 1
+        if self.last_use.get(r0) == self.count[r0]:
+            return f"RC_LAST({r0})"
         return f"RC({r0})"
 
 
 def gen_update_program(mech: dict) -> str:
     blocks = resolve_update(mech)
-    ctx = _Ctx()
+    uses: dict[int, int] = {}
+    for b in blocks:
+        for key in ("prod", "extra", "loss"):
+            for _, t in (b[key] or []):
+                for leaf in leaves(t, []):
+                    if leaf.kind == "RC":
+                        uses[leaf.idx] = uses.get(leaf.idx, 0) + 1
+    ctx = _Ctx(uses)
+    # RC rows each species block reads, in first-use order (for L2 prefetch)
+    rows, offs = [], []
+    for b in blocks:
+        offs.append(len(rows))
+        seen = []
+        for key in ("prod", "extra", "loss"):
+            for _, t in (b[key] or []):
+                for leaf in leaves(t, []):
+                    if leaf.kind == "RC" and leaf.idx not in seen:
+                        seen.append(leaf.idx)
+        rows.extend(seen)
+    offs.append(len(rows))
     L = ["// Generated by unicorn_b200/mech/codegen.py from the update program of",
          "// src/lib/solvesp.f:85-2806 (one block per species, in the reference's order).",
-         "// Requires accessor macros RC(r) (0-based reaction slot), YO(k) (Y at the",
+         "// Requires accessor macros RC(r) (0-based reaction slot; RC_LAST(r) marks its",
+         "// last use in a pass), YO(k) (Y at the",
          "// start of the pass), YN(k) (Y after its own update), Y0(k) (old time level),",
          "// SOUR(m), WM(k), FACE_SUM(k), FACE_NBR(k); scalars rho, dt, sor1, sor2, rsd;",
-         "// and UC_UPDATE_TAIL(k), which clips fnew and stores it as YN(k).",
+         "// and UC_UPDATE_TAIL(k), which clips fnew and stores it as YN(k);",
+         "// UC_UPDATE_SYNC() runs after every species (a barrier, or nothing);",
+         "// UC_UPDATE_BLOCK_BEGIN(b) runs before species block b (e.g. to prefetch).",
          "#pragma once",
          "#define UC_UPDATE_PROGRAM() do { \\",
          "    double prod = 0.0, extra, loss, rhs1, rhs2, ppp, fnew; \\"]
     nterms = 0
-    for b in blocks:
+    for bi, b in enumerate(blocks):
         k = b["species"]
-        body = []
+        body = [f"UC_UPDATE_BLOCK_BEGIN({bi});"]
         if b["prod"] is not None:
             body += emit_sum(b["prod"], ctx, "prod")
             nterms += len(b["prod"])
@@ -166,10 +199,18 @@ def gen_update_program(mech: dict) -> str:
         body.append(f"fnew = sor2 * YO({k}) + (rhs1 - FACE_NBR({k})) * sor1 / (ppp - rhs2);")
         body.append(f"rsd += fabs(YO({k}) - fnew);")
         body.append(f"UC_UPDATE_TAIL({k});")
+        body.append("UC_UPDATE_SYNC();")
         L.append(f"    /* species {k + 1} */ \\")
         L.extend("    " + x + " \\" for x in body)
     L.append("} while (0)")
     L.insert(6, f"// {nterms} production/extra/loss terms per cell and pass")
+    L.append("")
+    L.append(f"#define UC_UPD_NBLOCKS {len(blocks)}")
+    L.append("#ifdef __CUDACC__")
+    L.append("// RC rows read by each species block (first-use order): rows [off[b], off[b+1]).")
+    L.append(f"static __device__ const int16_t uc_upd_row_off[{len(offs)}] = {{{', '.join(map(str, offs))}}};")
+    L.append(f"static __device__ const int16_t uc_upd_rows[{len(rows)}] = {{{', '.join(map(str, rows))}}};")
+    L.append("#endif")
     return "\n".join(L) + "\n"
 
 

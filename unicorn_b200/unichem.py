@@ -25,7 +25,9 @@ import numpy as np
 
 LSP, LRX = 52, 544
 FP64, MIXED = 0, 1
-LIB_PATH = Path(__file__).resolve().parent / "libunichem.so"
+import os
+
+LIB_PATH = Path(os.environ.get("UNICHEM_LIB", str(Path(__file__).resolve().parent / "libunichem.so")))
 
 UC_ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "call order", -4: "device timeout",
              -5: "no convergence", -6: "out of device memory"}
