@@ -143,8 +143,10 @@ def run_ours(args, rank, world, dev):
     def reset():
         u.upload(h_tk, h_rho, h_y)
 
+    prec = unichem.MIXED if args.precision == "mixed" else unichem.FP64
+
     def step_device():
-        return u.sweep(DT, isor=args.isor, relx=RELX, tol=TOL)
+        return u.sweep(DT, precision=prec, isor=args.isor, relx=RELX, tol=TOL)
 
     passes_seen = []
     reset()
@@ -173,7 +175,7 @@ def run_ours(args, rank, world, dev):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         u.upload(h_tk, h_rho, h_y)
-        u.sweep(DT, isor=args.isor, relx=RELX, tol=TOL)
+        u.sweep(DT, precision=prec, isor=args.isor, relx=RELX, tol=TOL)
         u.download_outputs(outs)
         u.lib.uc_download_fields(u._h, None, None, unichem._p(h_yout), None, None)
     u.sync()
@@ -262,7 +264,8 @@ def main_ours(args):
                 "warmup": args.warmup, "ms_per_step": round(res["ms_per_step"], 4), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded C2 generator; the reference ships no benchmark data)",
-                "config": workload_config(world, {"update_passes_per_step": res["passes"][-args.steps:]}),
+                "config": workload_config(world, {"update_passes_per_step": res["passes"][-args.steps:],
+                                                  "precision": args.precision}),
                 "e2e": res["e2e"], "gpu_launches": res["gpu_launches"] * world, "clocks": res["clocks"],
                 "roofline": roofline(res, res["n"], args.steps),
                 "kernel_ms": {k: round(v[0], 3) for k, v in res["kernel_ms"].items()}}
@@ -349,6 +352,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cells", type=int, default=0, help="use only the first N cells (profiling runs)")
     ap.add_argument("--isor", type=int, default=ISOR, help="update passes cap (profiling runs)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
     if args.impl == "reference":
         main_reference(args)

@@ -144,6 +144,13 @@ int uc_download_outputs(uc_ctx *ctx, double *qdsp, double *qdot, double *domega_
 int uc_profile(uc_ctx *ctx, int on);
 int uc_profile_read(uc_ctx *ctx, double *ms, int *launches);
 
+/* Counters of the last calls (synchronises the stream):
+ *   "tiles"               32-cell tiles of the context
+ *   "mixed_fp64_tiles"    tiles the last UC_MIXED rate call sent to FP64 because a
+ *                         rate left the FP32 range
+ * Returns UC_E_ARG for an unknown name. */
+int uc_stat(uc_ctx *ctx, const char *name, double *value);
+
 /* Synchronise the context's stream. */
 int uc_sync(uc_ctx *ctx);
 

@@ -32,6 +32,8 @@ struct ChemArgs {
     double *qdsp, *qdot, *dwdy;  // outputs (any may be null)
     int n, npad, ntile;
     int *status;
+    const int *tile_list;        // optional: only these tiles ([*tile_count] entries)
+    const int *tile_count;
 };
 
 constexpr size_t CHEM_SMEM = PAIRTAB_BYTES + sizeof(double) * (size_t)(LRX * TILE + 2 * LSP * TILE + SC_N * TILE) + 64;
@@ -79,7 +81,9 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_fp64_kernel(const ChemAr
 
     const double C1ST = P.C1ST, C2ND = P.C2ND, C3RD = P.C3RD, RCONV = P.RCONV;
 
-    for (int tile = blockIdx.x; tile < a.ntile; tile += gridDim.x) {
+    const int nwork = a.tile_list ? *a.tile_count : a.ntile;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int tile = a.tile_list ? a.tile_list[w] : w;
         const size_t c0 = (size_t)tile * TILE;
         const size_t cell = c0 + lane;
         // ---------------- phase 0: load
@@ -285,4 +289,32 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_fp64_kernel(const ChemAr
     }
 }
 
+}  // namespace uc
+
+namespace uc {
+// List of the tiles whose flag is set (one CTA; order of the tile index).
+__global__ void compact_tiles_kernel(const int *flag, int ntile, int *list, int *count)
+{
+    __shared__ int s_base;
+    if (threadIdx.x == 0) s_base = 0;
+    __syncthreads();
+    for (int t0 = 0; t0 < ntile; t0 += blockDim.x) {
+        const int t = t0 + threadIdx.x;
+        const int f = (t < ntile) ? flag[t] : 0;
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        __shared__ int s_warp[32];
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if (lane == 0) s_warp[w] = __popc(m);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = s_base;
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { const int c = s_warp[i]; s_warp[i] = acc; acc += c; }
+            s_base = acc;
+        }
+        __syncthreads();
+        if (f) list[s_warp[w] + __popc(m & ((1u << lane) - 1))] = t;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *count = s_base;
+}
 }  // namespace uc

@@ -11,6 +11,7 @@
 
 #include "../../include/unichem.h"
 #include "chem_kernel.cuh"
+#include "chem_mixed_kernel.cuh"
 #include "props_kernel.cuh"
 #include "update_kernel.cuh"
 
@@ -25,6 +26,10 @@ struct uc_ctx {
     DevParams *hP = nullptr;          // host copy
     DevParams *dP = nullptr;
     PairTab *dTab = nullptr;
+    PairTabM *dTabM = nullptr;
+    float *rc32 = nullptr;
+    int rc_prec = UC_FP64;            // precision of the RC plane of the last uc_rates/uc_sweep
+    int *tile_flag = nullptr, *tile_list = nullptr, *tile_count = nullptr;   // mixed form: tiles sent to FP64
     double *tk = nullptr, *rho = nullptr, *y = nullptr, *y0 = nullptr, *soot = nullptr, *soot0 = nullptr;
     double *rc = nullptr, *sour = nullptr;
     double *qdsp = nullptr, *qdot = nullptr, *dwdy = nullptr;
@@ -84,7 +89,8 @@ static int set_err(uc_ctx *c, int code, const char *fmt, ...)
 // Tables and scales of src/unicornd-mild-sd-5.f:327-483 (all reactions on,
 // IRSW=1), written for the device parameter block. Literal constants keep
 // the reference's single-precision kind where it has one.
-static void build_params(const uc_inputs &in, DevParams &P, std::vector<PairTab> &tab, uc_scales &sc)
+static void build_params(const uc_inputs &in, DevParams &P, std::vector<PairTab> &tab, std::vector<PairTabM> &tabm,
+                         uc_scales &sc)
 {
     const double RUCAL = F32(1.9872), GASC = F32(8.3144);
     double AKF[LRX], ALF[LRX], EXAF[LRX], AKLOW[LRX], ALLOW[LRX], EALOW[LRX], TROE[LRX][4];
@@ -226,6 +232,36 @@ static void build_params(const uc_inputs &in, DevParams &P, std::vector<PairTab>
         }
         for (auto &v : out) std::sort(v.begin(), v.end());
     };
+    // pair table of the mixed kernel: logarithms of the constant factors
+    tabm.assign(NPAIR, PairTabM{});
+    const double CO[4] = {0.0, P.C1ST, P.C2ND, P.C3RD};
+    for (int p = 0; p < NPAIR; ++p) {
+        const PairTab &T = tab[p];
+        PairTabM &M = tabm[p];
+        memset(&M, 0, sizeof(M));
+        M.lnakf = T.akf > 0.0 ? log(T.akf) : -1.0e300;
+        M.alf = T.alf;
+        M.exaf = T.exaf;
+        M.falloff = T.aklow != 0.0;
+        M.lnaklow = M.falloff ? log(T.aklow) : 0.0;
+        M.allow = T.allow;
+        M.ealow = T.ealow;
+        for (int c = 0; c < 4; ++c) M.troe[c] = (float)T.troe[c];
+        M.has_rev = T.has_rev; M.rut = T.rut; M.qlen = T.qlen; M.dmole = T.dmole;
+        for (int t = 0; t < T.qlen; ++t) { M.qsp[t] = T.qsp[t]; M.qsgn[t] = (t > 0 && T.qdiv[t]) ? -1 : 1; }
+        M.order0 = T.rc_order0; M.order1 = T.rc_order1; M.tb0 = T.rc_tb0; M.tb1 = T.rc_tb1;
+        double l0 = T.rc_order0 ? log(CO[T.rc_order0]) : 0.0, l1 = T.rc_order1 ? log(CO[T.rc_order1]) : 0.0;
+        for (int t = 0; t < T.rc_len0; ++t) {
+            if (T.rc_kind0[t]) M.yk0[M.ny0++] = T.rc_idx0[t];
+            else l0 -= log(P.WM[T.rc_idx0[t]]);
+        }
+        for (int t = 0; t < T.rc_len1; ++t) {
+            if (T.rc_kind1[t]) M.yk1[M.ny1++] = T.rc_idx1[t];
+            else l1 -= log(P.WM[T.rc_idx1[t]]);
+        }
+        M.lnc0 = l0;
+        M.lnc1 = l1 + (T.akf_r > 0.0 ? log(T.akf_r) : 0.0);
+    }
     std::vector<std::vector<int>> pw, sw;
     balance(pcost, CHEM_WARPS, 24, pw);
     for (int w = 0; w < CHEM_WARPS; ++w) {
@@ -253,6 +289,11 @@ static void free_ctx(uc_ctx *c)
         if (*b) { cudaFree(*b); *b = nullptr; }
     if (c->dP) cudaFree(c->dP);
     if (c->dTab) cudaFree(c->dTab);
+    if (c->dTabM) cudaFree(c->dTabM);
+    if (c->rc32) cudaFree(c->rc32);
+    if (c->tile_flag) cudaFree(c->tile_flag);
+    if (c->tile_list) cudaFree(c->tile_list);
+    if (c->tile_count) cudaFree(c->tile_count);
     if (c->status) cudaFree(c->status);
     if (c->passes) cudaFree(c->passes);
     for (auto e : c->ev_pool) cudaEventDestroy(e);
@@ -355,9 +396,11 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
         ctx->hP = new (std::nothrow) DevParams();
         if (!ctx->hP) { rc = UC_E_NOMEM; break; }
         std::vector<PairTab> tab;
-        build_params(*in, *ctx->hP, tab, ctx->sc);
+        std::vector<PairTabM> tabm;
+        build_params(*in, *ctx->hP, tab, tabm, ctx->sc);
         if (cudaMalloc((void **)&ctx->dP, sizeof(DevParams)) != cudaSuccess ||
             cudaMalloc((void **)&ctx->dTab, PAIRTAB_BYTES) != cudaSuccess ||
+            cudaMalloc((void **)&ctx->dTabM, PAIRTABM_BYTES) != cudaSuccess ||
             cudaMalloc((void **)&ctx->status, sizeof(int)) != cudaSuccess ||
             cudaMalloc((void **)&ctx->passes, sizeof(int)) != cudaSuccess) {
             rc = set_err(ctx, UC_E_NOMEM, "device allocation of the parameter block failed");
@@ -365,6 +408,7 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
         }
         cudaMemcpy(ctx->dP, ctx->hP, sizeof(DevParams), cudaMemcpyHostToDevice);
         cudaMemcpy(ctx->dTab, tab.data(), PAIRTAB_BYTES, cudaMemcpyHostToDevice);
+        cudaMemcpy(ctx->dTabM, tabm.data(), PAIRTABM_BYTES, cudaMemcpyHostToDevice);
         cudaMemset(ctx->status, 0, sizeof(int));
         const size_t np = ctx->npad;
         if ((rc = dalloc(ctx, &ctx->tk, np)) || (rc = dalloc(ctx, &ctx->rho, np)) ||
@@ -373,11 +417,15 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
             (rc = dalloc(ctx, &ctx->sour, 6 * np)))
             break;
         e = cudaFuncSetAttribute(chem_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CHEM_SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(chem_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CHEMM_SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(update_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UPD_SMEM);
         if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "smem attribute: %s", cudaGetErrorString(e)); break; }
-        e = cudaFuncSetAttribute(update_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UPD_SMEM);
+        e = cudaFuncSetAttribute(update_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UPD_SMEM);
         if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "smem attribute: %s", cudaGetErrorString(e)); break; }
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update_fp64_kernel, UPD_THREADS, UPD_SMEM);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update_kernel<double>, UPD_THREADS, UPD_SMEM);
         if (const char *cap = getenv("UNICHEM_UPD_CTAS_PER_SM")) per_sm = std::min(per_sm, std::max(1, atoi(cap)));
         if (per_sm < 1) per_sm = 1;
         ctx->upd_grid = std::min(per_sm * ctx->nsm, std::max(1, (ctx->ntile + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32)));
@@ -439,12 +487,56 @@ extern "C" int uc_download_fields(uc_ctx *ctx, double *tk, double *rho, double *
 static int launch_chem(uc_ctx *ctx, int precision, bool want_rc, bool want_omega)
 {
     if (precision != UC_FP64 && precision != UC_MIXED) return set_err(ctx, UC_E_ARG, "unknown precision %d", precision);
-    if (precision == UC_MIXED) return set_err(ctx, UC_E_ARG, "precision UC_MIXED is not built in this library version");
-    if (want_rc) RET_IF(dalloc(ctx, &ctx->rc, (size_t)LRX * ctx->npad));
+    if (precision == UC_MIXED && want_rc && !ctx->rc32) {
+        cudaError_t e = cudaMalloc((void **)&ctx->rc32, (size_t)LRX * ctx->npad * sizeof(float));
+        if (e != cudaSuccess) { ctx->rc32 = nullptr; return set_err(ctx, UC_E_NOMEM, "FP32 RC plane: %s", cudaGetErrorString(e)); }
+    }
+    if (want_rc) RET_IF(dalloc(ctx, &ctx->rc, (size_t)LRX * ctx->npad));   // mixed: FP64 plane of fallback tiles
+    if (precision == UC_MIXED && !ctx->tile_flag) {
+        if (cudaMalloc((void **)&ctx->tile_flag, ctx->ntile * sizeof(int)) != cudaSuccess ||
+            cudaMalloc((void **)&ctx->tile_list, ctx->ntile * sizeof(int)) != cudaSuccess ||
+            cudaMalloc((void **)&ctx->tile_count, sizeof(int)) != cudaSuccess)
+            return set_err(ctx, UC_E_NOMEM, "tile flag buffers");
+    }
     if (want_omega) {
         RET_IF(dalloc(ctx, &ctx->qdsp, (size_t)LSP * ctx->npad));
         RET_IF(dalloc(ctx, &ctx->qdot, ctx->npad));
         RET_IF(dalloc(ctx, &ctx->dwdy, (size_t)LSP * ctx->npad));
+    }
+    if (precision == UC_MIXED) {
+        ChemMArgs m{};
+        m.P = ctx->dP; m.tab = ctx->dTabM;
+        m.tk = ctx->tk; m.rho = ctx->rho; m.y = ctx->y; m.stmf = ctx->soot; m.stnd = ctx->soot + ctx->npad;
+        m.rc32 = want_rc ? ctx->rc32 : nullptr;
+        m.sour = ctx->sour;
+        m.qdsp = want_omega ? ctx->qdsp : nullptr;
+        m.qdot = want_omega ? ctx->qdot : nullptr;
+        m.dwdy = want_omega ? ctx->dwdy : nullptr;
+        m.n = ctx->n; m.npad = ctx->npad; m.ntile = ctx->ntile; m.status = ctx->status;
+        m.tile_flag = ctx->tile_flag;
+        const int grid = std::min(ctx->ntile, ctx->nsm);
+        int slot;
+        prof_begin(ctx, UC_K_CHEM, slot);
+        chem_mixed_kernel<<<grid, CHEM_THREADS, CHEMM_SMEM, ctx->stream>>>(m);
+        prof_end(ctx, slot);
+        CK(cudaGetLastError());
+        // tiles with a rate beyond the FP32 range: recompute them in FP64
+        compact_tiles_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->tile_flag, ctx->ntile, ctx->tile_list, ctx->tile_count);
+        CK(cudaGetLastError());
+        ChemArgs f{};
+        f.P = ctx->dP; f.tab = ctx->dTab;
+        f.tk = ctx->tk; f.rho = ctx->rho; f.y = ctx->y; f.stmf = ctx->soot; f.stnd = ctx->soot + ctx->npad;
+        f.rc = want_rc ? ctx->rc : nullptr;
+        f.sour = ctx->sour;
+        f.qdsp = m.qdsp; f.qdot = m.qdot; f.dwdy = m.dwdy;
+        f.n = ctx->n; f.npad = ctx->npad; f.ntile = ctx->ntile; f.status = ctx->status;
+        f.tile_list = ctx->tile_list; f.tile_count = ctx->tile_count;
+        prof_begin(ctx, UC_K_CHEM, slot);
+        chem_fp64_kernel<<<std::min(ctx->ntile, ctx->nsm), CHEM_THREADS, CHEM_SMEM, ctx->stream>>>(f);
+        prof_end(ctx, slot);
+        CK(cudaGetLastError());
+        if (want_rc) ctx->rc_prec = UC_MIXED;
+        return UC_OK;
     }
     ChemArgs a{};
     a.P = ctx->dP;
@@ -463,6 +555,7 @@ static int launch_chem(uc_ctx *ctx, int precision, bool want_rc, bool want_omega
     chem_fp64_kernel<<<grid, CHEM_THREADS, CHEM_SMEM, ctx->stream>>>(a);
     prof_end(ctx, slot);
     CK(cudaGetLastError());
+    if (want_rc) ctx->rc_prec = UC_FP64;
     return UC_OK;
 }
 
@@ -473,9 +566,22 @@ extern "C" int uc_rates(uc_ctx *ctx, int precision, double *rc)
     CK(cudaSetDevice(ctx->device));
     RET_IF(launch_chem(ctx, precision, true, false));
     ctx->have_rc = true;
-    if (rc) {
+    if (rc && precision == UC_FP64) {
         RET_IF(download_rows(ctx, rc, ctx->rc, LRX));
         CK(cudaStreamSynchronize(ctx->stream));
+        RET_IF(check_status(ctx));
+    } else if (rc) {
+        // FP32 plane, with the FP64 values of the tiles that fell back to FP64
+        std::vector<float> tmp((size_t)LRX * ctx->n);
+        std::vector<int> flag(ctx->ntile);
+        CK(cudaMemcpy2DAsync(tmp.data(), (size_t)ctx->n * sizeof(float), ctx->rc32, (size_t)ctx->npad * sizeof(float),
+                             (size_t)ctx->n * sizeof(float), LRX, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(flag.data(), ctx->tile_flag, ctx->ntile * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        RET_IF(download_rows(ctx, rc, ctx->rc, LRX));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (int r = 0; r < LRX; ++r)
+            for (int c = 0; c < ctx->n; ++c)
+                if (!flag[c / TILE]) rc[(size_t)r * ctx->n + c] = tmp[(size_t)r * ctx->n + c];
         RET_IF(check_status(ctx));
     }
     return UC_OK;
@@ -564,7 +670,8 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
         fn = ctx->face_nbr;
     }
     UpdArgs a{};
-    a.P = ctx->dP; a.rc = ctx->rc; a.sour = ctx->sour; a.rho = ctx->rho; a.y0 = ctx->y0; a.soot0 = ctx->soot0;
+    a.P = ctx->dP; a.rc = ctx->rc; a.rc32 = ctx->rc32; a.sour = ctx->sour;
+    a.tile_flag = ctx->rc_prec == UC_MIXED ? ctx->tile_flag : nullptr; a.rho = ctx->rho; a.y0 = ctx->y0; a.soot0 = ctx->soot0;
     a.face_sum = fs; a.face_nbr = fn; a.y = ctx->y; a.soot = ctx->soot; a.partial = ctx->partial;
     a.passes = ctx->passes;
     a.dt = dt; a.sor1 = relx; a.tol = tol; a.spnorm = spnorm > 0.0 ? spnorm : (double)ctx->n * (LSP - 1);
@@ -572,8 +679,8 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
     void *args[] = {&a};
     int slot;
     prof_begin(ctx, UC_K_UPDATE, slot);
-    CK(cudaLaunchCooperativeKernel((void *)update_fp64_kernel, dim3(ctx->upd_grid), dim3(UPD_THREADS), args, UPD_SMEM,
-                                   ctx->stream));
+    const void *kfn = ctx->rc_prec == UC_MIXED ? (const void *)update_kernel<float> : (const void *)update_kernel<double>;
+    CK(cudaLaunchCooperativeKernel(kfn, dim3(ctx->upd_grid), dim3(UPD_THREADS), args, UPD_SMEM, ctx->stream));
     prof_end(ctx, slot);
     if (passes) {
         CK(cudaMemcpyAsync(passes, ctx->passes, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -655,6 +762,22 @@ extern "C" int uc_profile_read(uc_ctx *ctx, double *ms, int *launches)
     return UC_OK;
 }
 
+extern "C" int uc_stat(uc_ctx *ctx, const char *name, double *value)
+{
+    if (!ctx || !name || !value) return UC_E_ARG;
+    if (!strcmp(name, "tiles")) { *value = ctx->ntile; return UC_OK; }
+    if (!strcmp(name, "mixed_fp64_tiles")) {
+        int c = 0;
+        if (ctx->tile_count) {
+            CK(cudaMemcpyAsync(&c, ctx->tile_count, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+        *value = c;
+        return UC_OK;
+    }
+    return set_err(ctx, UC_E_ARG, "unknown statistic '%s'", name);
+}
+
 extern "C" int uc_sync(uc_ctx *ctx)
 {
     if (!ctx) return UC_E_ARG;
@@ -733,7 +856,7 @@ extern "C" int uc_species_update_noalloc(uc_ctx *ctx, const uc_update_arrays *ar
     if (isor < 1 || !(relx > 0.0) || !(dt >= 0.0)) return set_err(ctx, UC_E_ARG, "invalid isor/relx/dt");
     CK(cudaSetDevice(ctx->device));
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update_fp64_kernel, UPD_THREADS, UPD_SMEM));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update_kernel<double>, UPD_THREADS, UPD_SMEM));
     const int max_grid = std::max(1, per_sm) * ctx->nsm;
     if (max_grid > UC_NOALLOC_MAX_BLOCKS)
         return set_err(ctx, UC_E_ARG, "uc_species_update_noalloc: this device needs %d cooperating blocks, "
@@ -752,7 +875,7 @@ extern "C" int uc_species_update_noalloc(uc_ctx *ctx, const uc_update_arrays *ar
     a.isor = isor; a.n = arr->n; a.npad = arr->npad; a.ntile = ntile;
     const int grid = std::min(max_grid, std::max(1, (ntile + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32)));
     void *args[] = {&a};
-    CK(cudaLaunchCooperativeKernel((void *)update_fp64_kernel, dim3(grid), dim3(UPD_THREADS), args, UPD_SMEM,
+    CK(cudaLaunchCooperativeKernel((void *)update_kernel<double>, dim3(grid), dim3(UPD_THREADS), args, UPD_SMEM,
                                    ctx->stream));
     if (passes) {
         CK(cudaMemcpyAsync(passes, dpasses, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));

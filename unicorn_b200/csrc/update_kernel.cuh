@@ -25,9 +25,12 @@ namespace uc {
 
 struct UpdArgs {
     const DevParams *P;
-    const double *rc, *sour, *rho, *y0, *soot0;  // y0 [52][npad]: old time level; soot0 [2][npad]
+    const double *rc;                            // [544][npad] FP64 plane (update_kernel<double>)
+    const float *rc32;                           // [544][npad] FP32 plane (update_kernel<float>)
+    const double *sour, *rho, *y0, *soot0;       // y0 [52][npad]: old time level; soot0 [2][npad]
     const double *face_sum, *face_nbr;           // [51][npad] or null
     double *y, *soot;                            // updated in place
+    const int *tile_flag;                        // update_kernel<float>: tiles whose RC is in the FP64 plane
     double *partial;                             // [2][gridDim.x]
     int *passes;                                 // out: pass count as ISOR1 reports it
     double dt, sor1, tol, spnorm;
@@ -56,7 +59,10 @@ constexpr size_t UPD_SMEM = (size_t)UPD_WARPS * 2 * LSP * TILE * sizeof(double);
 
 // Read-only loads that skip L1 and carry an L2 eviction priority: lines that
 // are read again later in the pass are kept (evict_last), the last read of a
-// line in the pass lets it go first (evict_first).
+// line in the pass lets it go first (evict_first). The asm is not volatile:
+// the data is read-only during the kernel, and the compiler must be free to
+// issue these loads early (a volatile form pins each load to its use and
+// leaves only a few loads in flight per warp).
 __device__ __forceinline__ uint64_t l2_policy_keep()
 {
     uint64_t p;
@@ -73,26 +79,44 @@ __device__ __forceinline__ double ld_hint(const double *p, uint64_t pol)
 {
     double v;
 #if UC_L2_HINTS
-    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
 #else
-    asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
 #endif
     return v;
 }
+__device__ __forceinline__ double ld_hint(const float *p, uint64_t pol)
+{
+    float v;
+#if UC_L2_HINTS
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+#else
+    asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+#endif
+    return (double)v;
+}
+
 
 // Prefetch into L2 the RC rows (256 B per 32-cell tile row) that species
 // block b of the program reads; each lane pair takes one row, 16 rows per step.
-__device__ __forceinline__ void prefetch_block_rows(int b, const double *tile_base, size_t np, int lane)
+template <typename RCT>
+__device__ __forceinline__ void prefetch_block_rows(int b, const RCT *tile_base, size_t np, int lane)
 {
     const int o = uc_upd_row_off[b], e = uc_upd_row_off[b + 1];
     for (int i = o + (lane >> 1); i < e; i += 16) {
-        const double *p = tile_base + (size_t)uc_upd_rows[i] * np + (lane & 1) * 16;
+        const RCT *p = tile_base + (size_t)uc_upd_rows[i] * np + (lane & 1) * (128 / sizeof(RCT));
         asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(p));
     }
 }
 
-__global__ void __launch_bounds__(UPD_THREADS, 1) update_fp64_kernel(const UpdArgs a)
+// RCT: storage type of the RC plane (double for the FP64 form, float for the
+// mixed form); the update itself is FP64 in both.
+template <typename RCT>
+__global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
 {
+    // the plane is addressed through the kernel parameter itself (not a local
+    // pointer copy): ptxas then rebuilds addresses from the parameter bank and
+    // the generated program fits in registers (a local copy spilled 5 KB/thread)
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
     extern __shared__ __align__(128) double s_upd[];
@@ -121,8 +145,6 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_fp64_kernel(const UpdAr
             double crsd = 0.0;
             {
                 double &rsd = crsd;
-#define RC(r) ld_hint(a.rc + (size_t)(r) * np + cell, keep)
-#define RC_LAST(r) ld_hint(a.rc + (size_t)(r) * np + cell, drop)
 #define YO(k) syo[(k) * TILE]
 #define YN(k) syn[(k) * TILE]
 #define Y0(k) ld_hint(a.y0 + (size_t)(k) * np + cell, drop)
@@ -136,18 +158,23 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_fp64_kernel(const UpdAr
 #else
 #define UC_UPDATE_SYNC() do { } while (0)
 #endif
-#if UC_PF > 0
-#define UC_UPDATE_BLOCK_BEGIN(b) do { if ((b) + UC_PF < UC_UPD_NBLOCKS) prefetch_block_rows((b) + UC_PF, rc_tile, np, lane); } while (0)
-#else
 #define UC_UPDATE_BLOCK_BEGIN(b) do { } while (0)
-#endif
-                const double *rc_tile = a.rc + (size_t)tile * TILE;
-#if UC_PF > 0
-                for (int b0 = 0; b0 < UC_PF && b0 < UC_UPD_NBLOCKS; ++b0) prefetch_block_rows(b0, rc_tile, np, lane);
-#endif
-                UC_UPDATE_PROGRAM();
+                if (sizeof(RCT) == 4 && a.tile_flag && a.tile_flag[tile]) {
+                    // a tile the mixed rate kernel sent to FP64: its RC is in the FP64 plane
+#define RC(r) ld_hint(a.rc + (size_t)(r) * np + cell, keep)
+#define RC_LAST(r) ld_hint(a.rc + (size_t)(r) * np + cell, drop)
+                    UC_UPDATE_PROGRAM();
 #undef RC
 #undef RC_LAST
+                } else {
+#define UC_RCP (sizeof(RCT) == 4 ? reinterpret_cast<const RCT *>(a.rc32) : reinterpret_cast<const RCT *>(a.rc))
+#define RC(r) ld_hint(UC_RCP + (size_t)(r) * np + cell, keep)
+#define RC_LAST(r) ld_hint(UC_RCP + (size_t)(r) * np + cell, drop)
+                    UC_UPDATE_PROGRAM();
+                }
+#undef RC
+#undef RC_LAST
+#undef UC_RCP
 #undef YO
 #undef YN
 #undef Y0

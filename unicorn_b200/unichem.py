@@ -84,6 +84,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.uc_download_outputs.argtypes = [vp, P, P, P, P, P, P, P, P]
     lib.uc_profile.argtypes = [vp, ctypes.c_int]
     lib.uc_profile_read.argtypes = [vp, P, ctypes.POINTER(ctypes.c_int)]
+    lib.uc_stat.argtypes = [vp, ctypes.c_char_p, P]
     lib.uc_sync.argtypes = [vp]
     lib.uc_last_error.argtypes = [vp]
     lib.uc_last_error.restype = ctypes.c_char_p
@@ -233,6 +234,11 @@ class UniChem:
         self._ck(self.lib.uc_download_outputs(self._h, *[_p(out.get(k)) for k in
                                                          ("qdsp", "qdot", "domega_dy", "vmu", "vtc", "vdf", "cp", "h")]))
         return out
+
+    def stat(self, name: str) -> float:
+        v = np.zeros(1)
+        self._ck(self.lib.uc_stat(self._h, name.encode(), _p(v)))
+        return float(v[0])
 
     def profile(self, on: bool = True):
         self._ck(self.lib.uc_profile(self._h, int(on)))
