@@ -121,6 +121,7 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
     cg::grid_group grid = cg::this_grid();
     extern __shared__ __align__(128) double s_upd[];
     __shared__ double s_part[UPD_WARPS];
+    __shared__ double s_wm[LSP];
     const DevParams &P = *a.P;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     double *syo = s_upd + (size_t)wib * 2 * LSP * TILE + lane;   // YO(k) = syo[k*32]
@@ -131,6 +132,8 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
     const double sor1 = a.sor1, sor2 = 1.0 - a.sor1, dt = a.dt;
     const size_t np = a.npad;
     const uint64_t keep = l2_policy_keep(), drop = l2_policy_drop();
+    for (int k = threadIdx.x; k < LSP; k += blockDim.x) s_wm[k] = P.WM[k];
+    __syncthreads();
     int pass;
     for (pass = 1; pass <= a.isor; ++pass) {
         double rsd = 0.0;
@@ -142,14 +145,17 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
             const bool live = own && cell < (size_t)a.n;
             for (int k = 0; k < LSP - 1; ++k) syo[k * TILE] = a.y[k * np + cell];
             const double rho = a.rho[cell];
+            double so[6];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) so[m] = a.sour[m * np + cell];
             double crsd = 0.0;
             {
                 double &rsd = crsd;
 #define YO(k) syo[(k) * TILE]
 #define YN(k) syn[(k) * TILE]
 #define Y0(k) ld_hint(a.y0 + (size_t)(k) * np + cell, drop)
-#define SOUR(m) ld_hint(a.sour + (size_t)(m) * np + cell, drop)
-#define WM(k) P.WM[k]
+#define SOUR(m) so[m]
+#define WM(k) s_wm[k]
 #define FACE_SUM(k) (a.face_sum ? __ldg(a.face_sum + (size_t)(k) * np + cell) : 0.0)
 #define FACE_NBR(k) (a.face_nbr ? __ldg(a.face_nbr + (size_t)(k) * np + cell) : 0.0)
 #define UC_UPDATE_TAIL(k) do { if (fnew < 0.0) fnew = 0.0; syn[(k) * TILE] = fnew; } while (0)
@@ -187,8 +193,7 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
 #undef UC_UPDATE_BLOCK_BEGIN
                 // soot mass fraction and number density (solvesp.f:2807-2832)
                 const double s1 = a.soot[cell], s2 = a.soot[np + cell];
-                const double so0 = a.sour[cell], so1 = a.sour[np + cell], so2 = a.sour[2 * np + cell],
-                             so3 = a.sour[3 * np + cell], so4 = a.sour[4 * np + cell], so5 = a.sour[5 * np + cell];
+                const double so0 = so[0], so1 = so[1], so2 = so[2], so3 = so[3], so4 = so[4], so5 = so[5];
                 const double y2 = syn[1 * TILE], y4 = syn[3 * TILE], y5 = syn[4 * TILE], y22 = syn[21 * TILE];
                 double rhs1 = rho * a.soot0[cell] + dt * ((double)0.012011f / P.WMSTR) *
                                                         (2.0 * so0 * y22 - so2 * y2 - so3 * y5 - so4 * y4);
