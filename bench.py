@@ -343,6 +343,102 @@ def main_reference(args):
         "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
 
 
+# ---------------------------------------------------------------- C3: batched stiff integration
+C3_CELLS = 1 << 20
+
+
+def cpu_baseline_c3(f, ncells=2048):
+    """The oracle's batched integration (orc_integrate, OpenMP over cells) on a bounded sample."""
+    from oracle.oracle import Oracle
+    from unicorn_b200.fields import nondimensional
+    o = Oracle()
+    tk, rho = nondimensional(f, o.scales, o.wm)
+    sl = slice(0, ncells)
+    y = np.ascontiguousarray(f.y[:, sl])
+    pnd = f.p[sl] / o.scales["PSTR"]
+    t0 = time.perf_counter()
+    q = o.omega(tk[sl], rho[sl], y)[0]
+    ns, _ = o.nsub(rho[sl], y, q, DT)
+    o.integrate(tk[sl], rho[sl], y, pnd, ns, DT)
+    dt = time.perf_counter() - t0
+    cores = os.cpu_count() or 1
+    return {"value": ncells / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {ncells} cells of the C3 batch (mean n_sub {ns.mean():.1f}), oracle/unichem_oracle.c "
+                      f"orc_integrate, -O2, OpenMP over cells, {dt:.2f} s"}
+
+
+def main_c3(args):
+    import torch
+    from unicorn_b200 import unichem
+    from unicorn_b200.fields import batch_cells, nondimensional
+    n = args.cells or C3_CELLS
+    f = batch_cells(n, seed=0)
+    prec = unichem.FP64
+    opts = dict(isor=args.isor, relx=RELX, tol=TOL)
+    u = unichem.UniChem(n)
+    tk, rho = nondimensional(f, u.scales, u.wm)
+    pnd = f.p / u.scales["PSTR"]
+    pin = lambda *s: torch.empty(s, dtype=torch.float64, pin_memory=True).numpy()
+    h_tk, h_rho, h_y, h_p = pin(n), pin(n), pin(52, n), pin(n)
+    h_tk[:], h_rho[:], h_y[:], h_p[:] = tk, rho, f.y, pnd
+    o_tk, o_rho, o_y = pin(n), pin(n), pin(52, n)
+    u.set_pressure(h_p)
+    u.upload(h_tk, h_rho, h_y)
+    tune = u.integrate_tune(DT, precision=prec, **opts)
+    for _ in range(args.warmup):
+        u.upload(h_tk, h_rho, h_y)
+        u.integrate(DT, precision=prec, **opts)
+    u.sync()
+    # device time of the integration graph only (each step restarts from the same state, uploaded before it)
+    u.profile(True)
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            u.upload(h_tk, h_rho, h_y)
+            u.integrate(DT, precision=prec, **opts)
+        kt = u.profile_read()
+    u.profile(False)
+    ms = kt["integrate"][0]
+    ns, pa = u.integrate_counts()
+    # end to end through the C ABI: inputs from pinned host memory, state back to the host
+    u.sync()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        u.upload(h_tk, h_rho, h_y)
+        u.integrate(DT, precision=prec, **opts)
+        u.lib.uc_download_fields(u._h, unichem._p(o_tk), unichem._p(o_rho), unichem._p(o_y), None, None)
+    u.sync()
+    e2e = time.perf_counter() - t0
+    u.close()
+    substeps = float(ns.sum())
+    per_sub_flop = 9.0e3 + 470 + 2 * 2189 * float(pa.sum()) / substeps
+    achieved = per_sub_flop * substeps / (ms / args.steps / 1e3) / 1e12
+    line = {"metric": "batched stiff integration cell-updates/s (one cell over dt = 1e-5 s)",
+            "value": round(n * args.steps / (ms / 1e3), 1), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded C3 generator)",
+            "config": {"workload": f"C3: {n} independent heptane-generator cells, T~U[300,2400] K, p~U[0.8,1.2] atm, "
+                                   "dt=1e-5 s, n_sub=clamp(ceil(max_k dt|w_k|/Y_k over Y_k>1e-3), 1, 200), "
+                                   f"update passes to 1e-8 per sub-step (<={args.isor})",
+                       "cells": n, "precision": "fp64", "tuned": tune,
+                       "nsub": {"mean": round(float(ns.mean()), 2), "min": int(ns.min()), "max": int(ns.max()),
+                                "frac_1": round(float((ns == 1).mean()), 4),
+                                "frac_max": round(float((ns == ns.max()).mean()), 4)},
+                       "passes_per_substep": round(float(pa.sum()) / substeps, 2),
+                       "l2": "state 470 MB > L2; all sub-step work on chip"},
+            "e2e": {"value": round(n * args.steps / e2e, 1), "unit": UNIT, "h2d_bytes_per_step": (2 + 52) * 8 * n,
+                    "d2h_bytes_per_step": (2 + 52) * 8 * n},
+            "gpu_launches": kt["integrate"][1] * (6 if tune["int_sorted"] else 3),
+            "clocks": clk.summary(),
+            "roofline": {"kernel": "integrate", "bound": "fp64", "achieved": round(achieved, 3), "peak": 37.0,
+                         "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)", "unit": "TFLOP/s",
+                         "frac": round(achieved / 37.0, 4), "traffic": None,
+                         "flops_rule": "per cell and sub-step: 9e3 rate flops + 470 transcendentals (1 op each) + "
+                                       "2 flops x 2189 update terms x passes"}}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_c3(f)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -353,8 +449,12 @@ def main():
     ap.add_argument("--cells", type=int, default=0, help="use only the first N cells (profiling runs)")
     ap.add_argument("--isor", type=int, default=ISOR, help="update passes cap (profiling runs)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
+                    help="c2: the species sweep of the 601x301 heptane field (headline); c3: batched stiff integration")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.workload == "c3":
+        main_c3(args)
+    elif args.impl == "reference":
         main_reference(args)
     else:
         main_ours(args)

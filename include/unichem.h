@@ -140,7 +140,8 @@ int uc_download_outputs(uc_ctx *ctx, double *qdsp, double *qdot, double *domega_
 #define UC_K_PROPS 2
 #define UC_K_CPH 3
 #define UC_K_TEMP 4
-#define UC_K_COUNT 5
+#define UC_K_INTEGRATE 5   /* one uc_integrate graph launch */
+#define UC_K_COUNT 6
 int uc_profile(uc_ctx *ctx, int on);
 int uc_profile_read(uc_ctx *ctx, double *ms, int *launches);
 
@@ -169,6 +170,45 @@ typedef struct {
     void *stream;   /* cudaStream_t */
 } uc_device_view;
 int uc_device_view_get(uc_ctx *ctx, uc_device_view *v);
+
+/* ---------------------------------------------------------------------------
+ * Batched stiff integration of independent cells.
+ *
+ * No single reference routine corresponds: every cell of the context is a
+ * one-cell field advanced over o->dt by n_sub sub-steps of dt/n_sub, each
+ * the reference's own chain - CKRATES (src/lib/ckrates.f), SOLVESP with its
+ * closure (src/lib/solvesp.f, SPNORM = LSP-1 so that each cell converges on
+ * its own residual, no face terms), T from the cell's constant total
+ * enthalpy (src/lib/solveh.f:1186-1234) and rho from the ideal gas at the
+ * cell's pressure (src/unicornd-mild-sd-5.f:1056-1062). The state (TK, RHO,
+ * FSP, STMF, STND) is advanced in place; read it with uc_download_fields.
+ *
+ * n_sub = clamp(ceil(x / c_tau), 1, nsub_max), x = max over species with
+ * Y_k > y_tau of dt*|QDSP_k| / (RCONV*rho*Y_k), QDSP of the start state.
+ * The whole step (rates of the start state, n_sub, a stable sort of the
+ * cells by n_sub, the persistent work-queue kernel) is one CUDA graph launch;
+ * the graph is captured on the first call and again when an option or the
+ * tuned kernel shape changes.
+ *
+ * precision: UC_FP64 (everything FP64); other values return UC_E_ARG.
+ */
+typedef struct {
+    double dt;          /* non-dimensional step (DT = 1e-3 is 1e-5 s) */
+    int isor;           /* update passes per sub-step, at most */
+    double relx, tol;   /* relaxation (RELXSP) and per-cell tolerance */
+    double c_tau;       /* time-scale factor of the sub-step count */
+    double y_tau;       /* species above this mass fraction set the time scale */
+    int nsub_max;       /* 1..1024 */
+} uc_integrate_opts;
+/* Cell pressures p/PSTR [n] (host); cells default to PBACK. */
+int uc_set_pressure(uc_ctx *ctx, const double *pnd);
+int uc_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts *o);
+/* Times each kernel shape on the current state (restored after each trial)
+ * and keeps the fastest for uc_integrate; uc_stat "int_warps", "int_sorted",
+ * "int_tune_best_ms", "int_tune_worst_ms" report the outcome. */
+int uc_integrate_tune(uc_ctx *ctx, int precision, const uc_integrate_opts *o);
+/* Per-cell sub-step counts and update passes of the last uc_integrate (host [n], either may be NULL). */
+int uc_integrate_counts(uc_ctx *ctx, int *nsub, int *passes);
 
 /* ---------------------------------------------------------------------------
  * Species update on caller-owned device arrays, with no device allocation.

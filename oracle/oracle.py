@@ -328,6 +328,26 @@ class Oracle:
         del keep
         return y, s, passes
 
+    def nsub(self, rho, y, qdsp, dt, c_tau=1.0, y_tau=1e-3, nsub_max=200):
+        """Per-cell sub-step counts of the batched integration and the ratio x they come from."""
+        n = len(rho)
+        ns, x = np.empty(n, dtype=np.int32), np.empty(n)
+        self.lib.orc_nsub(n, _dptr(_c(rho)), _dptr(_c(y)), _dptr(_c(qdsp)), ctypes.c_double(dt),
+                          ctypes.c_double(c_tau), ctypes.c_double(y_tau), int(nsub_max), _iptr(ns), _dptr(x))
+        return ns, x
+
+    def integrate(self, tk, rho, y, pnd, nsub, dt, soot=None, isor=100, relx=0.99, tol=1e-8):
+        """Batched stiff integration over dt; returns (tk, rho, y, soot, passes) after the step."""
+        n = len(tk)
+        tk, rho = np.array(tk, dtype=np.float64), np.array(rho, dtype=np.float64)
+        y = np.array(y, dtype=np.float64, order="C", copy=True)
+        s = np.array(np.zeros((2, n)) if soot is None else soot, dtype=np.float64, order="C", copy=True)
+        passes = np.empty(n, dtype=np.int32)
+        self.lib.orc_integrate(n, _dptr(tk), _dptr(rho), _dptr(y), _dptr(s), _dptr(_c(pnd)),
+                               _iptr(_c(nsub, np.int32)), ctypes.c_double(dt), int(isor), ctypes.c_double(relx),
+                               ctypes.c_double(tol), _iptr(passes))
+        return tk, rho, y, s, passes
+
     def temperature(self, tk_guess, y, ht):
         tk = np.array(tk_guess, dtype=np.float64, copy=True)
         self.lib.orc_temperature(len(tk), _dptr(tk), _dptr(_c(y)), _dptr(_c(ht)))

@@ -15,6 +15,8 @@
  *   orc_props            src/unicornd-mild-sd-5.f:821-1006 (Y clip, mu, lambda, D_k)
  *   orc_species_update   src/lib/solvesp.f:82-2915        (point-implicit update)
  *   orc_temperature      src/lib/solveh.f:1170-1234       (T from h, Newton)
+ *   orc_nsub, orc_integrate  batched stiff integration: the functions above
+ *                        chained per cell and sub-step (no single reference routine)
  * The mechanism arrives as flat tables built from the reference sources by
  * unicorn_b200/mech/extract.py and packed by oracle/oracle.py.
  *
@@ -738,46 +740,145 @@ int orc_species_update(int n, const double *rho, const double *y0, double *y, co
 
 /* solveh.f:1170-1234: temperature from the non-dimensional sensible
  * enthalpy ht (FPZ) and the mass fractions; tk holds the guess on entry. */
-void orc_temperature(int n, double *tk, const double *y, const double *ht)
+/* Newton for T at the total enthalpy ENTH (solveh.f:1186-1234); y has
+ * stride ys between species. Returns the new non-dimensional tk. */
+static double temperature_cell(double tk, const double *y, size_t ys, double ENTH)
 {
     const double TKDMIN = S.TSTR - 1.0;
+    int IPL = 0;
+    double TPOLY = T.tpol1;
+    double TKD = tk * S.TSTR;
+    double A1, A2, A3, A4, A5, A6;
+    for (;;) {
+        if (TKD > TPOLY) TKD = TPOLY / 2.0;
+        A1 = A2 = A3 = A4 = A5 = A6 = 0.0;
+        for (int k = 0; k < LSP; ++k) {
+            const double *a = T.poly + k * 14 + IPL;
+            double yk = y[(size_t)k * ys];
+            A1 = A1 + a[0] * yk / S.WM[k];
+            A2 = A2 + a[1] * yk / S.WM[k] / 2.0;
+            A3 = A3 + a[2] * yk / S.WM[k] / 3.0;
+            A4 = A4 + a[3] * yk / S.WM[k] / 4.0;
+            A5 = A5 + a[4] * yk / S.WM[k] / 5.0;
+            A6 = A6 + a[5] * yk / S.WM[k];
+        }
+        double FUNT = ((A1 + (A2 + (A3 + (A4 + A5 * TPOLY) * TPOLY) * TPOLY) * TPOLY) * TPOLY + A6)
+                      * S.GASC / S.WMSTR - ENTH;
+        if (FUNT >= 1.0e-07) break;
+        if (IPL >= 7) break;
+        IPL = 7;
+        if (TKD <= TPOLY) TKD = T.tpol2 / 2.0;
+        TPOLY = T.tpol2;
+    }
+    for (int it = 1; it <= 100; ++it) {
+        double DTKD = ((A1 + (A2 + (A3 + (A4 + A5 * TKD) * TKD) * TKD) * TKD) * TKD + A6
+                       - ENTH * S.WMSTR / S.GASC)
+                      / (A1 + (2.0 * A2 + (3.0 * A3 + (4.0 * A4 + 5.0 * A5 * TKD) * TKD) * TKD) * TKD);
+        if (fabs(DTKD) <= F(0.001)) break;
+        TKD = TKD - DTKD;
+    }
+    if (TKD > T.tpol2) TKD = T.tpol2;
+    if (TKD < TKDMIN) TKD = TKDMIN;
+    return TKD / S.TSTR;
+}
+
+void orc_temperature(int n, double *tk, const double *y, const double *ht)
+{
     for (int c = 0; c < n; ++c) {
         double ENTH = (ht[c] - F(0.5) * 0.0) * S.HSTR;
         for (int k = 0; k < LSP; ++k) ENTH = ENTH + y[(size_t)k * n + c] * S.HFO[k] * S.HSTR;
-        int IPL = 0;
-        double TPOLY = T.tpol1;
-        double TKD = tk[c] * S.TSTR;
-        double A1, A2, A3, A4, A5, A6;
-        for (;;) {
-            if (TKD > TPOLY) TKD = TPOLY / 2.0;
-            A1 = A2 = A3 = A4 = A5 = A6 = 0.0;
-            for (int k = 0; k < LSP; ++k) {
-                const double *a = T.poly + k * 14 + IPL;
-                double yk = y[(size_t)k * n + c];
-                A1 = A1 + a[0] * yk / S.WM[k];
-                A2 = A2 + a[1] * yk / S.WM[k] / 2.0;
-                A3 = A3 + a[2] * yk / S.WM[k] / 3.0;
-                A4 = A4 + a[3] * yk / S.WM[k] / 4.0;
-                A5 = A5 + a[4] * yk / S.WM[k] / 5.0;
-                A6 = A6 + a[5] * yk / S.WM[k];
+        tk[c] = temperature_cell(tk[c], y + c, (size_t)n, ENTH);
+    }
+}
+
+/* ------------------------------------------------------------- batched stiff integration */
+
+/* Total enthalpy of a cell at its own temperature, in the units of ENTH in
+ * solveh.f:1186-1205 (the polynomial of the T-from-h Newton at T, range by
+ * T > TPOL1 as in the kinetics). */
+static double enthalpy_total(double tk, const double *y, size_t ys)
+{
+    double TKD = tk * S.TSTR;
+    int ip = TKD > T.tpol1 ? 7 : 0;
+    double A1 = 0.0, A2 = 0.0, A3 = 0.0, A4 = 0.0, A5 = 0.0, A6 = 0.0;
+    for (int k = 0; k < LSP; ++k) {
+        const double *a = T.poly + k * 14 + ip;
+        double yk = y[(size_t)k * ys];
+        A1 = A1 + a[0] * yk / S.WM[k];
+        A2 = A2 + a[1] * yk / S.WM[k] / 2.0;
+        A3 = A3 + a[2] * yk / S.WM[k] / 3.0;
+        A4 = A4 + a[3] * yk / S.WM[k] / 4.0;
+        A5 = A5 + a[4] * yk / S.WM[k] / 5.0;
+        A6 = A6 + a[5] * yk / S.WM[k];
+    }
+    return ((A1 + (A2 + (A3 + (A4 + A5 * TKD) * TKD) * TKD) * TKD) * TKD + A6) * S.GASC / S.WMSTR;
+}
+
+/* Sub-step count of each cell from its chemical time scale:
+ *   x = max over species with Y_k > y_tau of dt*|QDSP_k| / (RCONV*rho*Y_k)
+ * (dY_k/dt = -QDSP_k/(RCONV*rho) in the reference's units, solveh.f:1138),
+ *   n_sub = clamp(ceil(x / c_tau), 1, nsub_max);  x_out (optional) gets x. */
+void orc_nsub(int n, const double *rho, const double *y, const double *qdsp, double dt, double c_tau,
+              double y_tau, int nsub_max, int *nsub, double *x_out)
+{
+    const double RCONV = S.VSTR / S.WMSTR / S.ALSTR * 1.0e-06;
+    for (int c = 0; c < n; ++c) {
+        double x = 0.0;
+        for (int k = 0; k < LSP; ++k) {
+            double yk = y[(size_t)k * n + c];
+            if (yk > y_tau) {
+                double v = dt * fabs(qdsp[(size_t)k * n + c]) / (RCONV * rho[c] * yk);
+                if (!(v <= x)) x = v;       /* NaN propagates */
             }
-            double FUNT = ((A1 + (A2 + (A3 + (A4 + A5 * TPOLY) * TPOLY) * TPOLY) * TPOLY) * TPOLY + A6)
-                          * S.GASC / S.WMSTR - ENTH;
-            if (FUNT >= 1.0e-07) break;
-            if (IPL >= 7) break;
-            IPL = 7;
-            if (TKD <= TPOLY) TKD = T.tpol2 / 2.0;
-            TPOLY = T.tpol2;
         }
-        for (int it = 1; it <= 100; ++it) {
-            double DTKD = ((A1 + (A2 + (A3 + (A4 + A5 * TKD) * TKD) * TKD) * TKD) * TKD + A6
-                           - ENTH * S.WMSTR / S.GASC)
-                          / (A1 + (2.0 * A2 + (3.0 * A3 + (4.0 * A4 + 5.0 * A5 * TKD) * TKD) * TKD) * TKD);
-            if (fabs(DTKD) <= F(0.001)) break;
-            TKD = TKD - DTKD;
+        double m = ceil(x / c_tau);
+        int ns = (m != m || m >= (double)nsub_max) ? nsub_max : (m < 1.0 ? 1 : (int)m);
+        nsub[c] = ns;
+        if (x_out) x_out[c] = x;
+    }
+}
+
+/* Batched stiff point-implicit integration of independent cells over dt.
+ * Each cell is its own one-cell field advanced n_sub times by dt/n_sub with
+ * the reference's own steps: rates (ckrates.f), the species update with its
+ * closure (solvesp.f; SPNORM = LSP-1, no face terms; each cell converges on
+ * its own residual), T from the cell's constant total enthalpy
+ * (solveh.f:1186-1234) and rho from the ideal gas at the cell's pressure
+ * pnd = p/PSTR (main:1056-1062). State arrays are [52][n], [n] and soot
+ * [2][n], updated in place. nsub holds the per-cell counts (orc_nsub).
+ * passes (optional) receives the update passes summed over the sub-steps. */
+void orc_integrate(int n, double *tk, double *rho, double *y, double *soot, const double *pnd,
+                   const int *nsub, double dt, int isor, double relx, double tol, int *passes)
+{
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int c = 0; c < n; ++c) {
+        cell_rates cr;
+        double yc[LSP], y0[LSP], s[2], s0[2];
+        for (int k = 0; k < LSP; ++k) yc[k] = y[(size_t)k * n + c];
+        s[0] = soot[c];
+        s[1] = soot[(size_t)n + c];
+        double t = tk[c], r = rho[c];
+        const double ENTH0 = enthalpy_total(t, yc, 1);
+        const double dts = dt / (double)nsub[c];
+        int np = 0;
+        for (int st = 0; st < nsub[c]; ++st) {
+            rates_cell(t, r, yc, s[0], s[1], &cr);
+            memcpy(y0, yc, sizeof(y0));
+            s0[0] = s[0];
+            s0[1] = s[1];
+            int p = orc_species_update(1, &r, y0, yc, cr.rc, cr.sour, s0, s, NULL, NULL, dts, isor, relx, tol,
+                                       (double)(LSP - 1));
+            np += p > isor ? isor : p;
+            t = temperature_cell(t, yc, 1, ENTH0);
+            double rbar = 0.0;
+            for (int k = 0; k < LSP; ++k) rbar = rbar + yc[k] / S.WM[k];
+            r = pnd[c] / (S.BETA1 * t * rbar);
         }
-        if (TKD > T.tpol2) TKD = T.tpol2;
-        if (TKD < TKDMIN) TKD = TKDMIN;
-        tk[c] = TKD / S.TSTR;
+        for (int k = 0; k < LSP; ++k) y[(size_t)k * n + c] = yc[k];
+        soot[c] = s[0];
+        soot[(size_t)n + c] = s[1];
+        tk[c] = t;
+        rho[c] = r;
+        if (passes) passes[c] = np;
     }
 }

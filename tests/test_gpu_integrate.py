@@ -1,0 +1,100 @@
+"""Batched stiff integration (uc_integrate) on the GPU against the oracle
+(orc_integrate) on the same seeded C3-distribution cells.
+
+Tolerances (FP64 throughout): the sub-step counts must agree except where
+the oracle's x/c_tau lies within 1e-9 of an integer (the GPU's exp/log differ
+from the host's by an ulp); the oracle is then run with the GPU's counts.
+A cell's state after up to 200 sub-steps agrees to 1e-6 relative (+1e-12
+absolute) in Y and 1e-2 K in T: the per-cell pass loop stops on a residual
+of 1e-8, so an ulp of difference in the rates can move one pass, and the T
+Newton stops on a step of 1e-3 K. Cells that end on the reference's T clamp
+are excluded (see the test).
+"""
+import numpy as np
+import pytest
+
+from unicorn_b200.fields import batch_cells, nondimensional
+
+pytestmark = pytest.mark.gpu
+DT = 1e-3
+
+
+@pytest.fixture(scope="module")
+def cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("a GPU test ran without a CUDA device")
+    from unicorn_b200 import unichem
+    return unichem
+
+
+def run_gpu(cuda, f, tk, rho, pnd, tune=False, **kw):
+    with cuda.UniChem(f.n) as u:
+        u.upload(tk, rho, f.y)
+        u.set_pressure(pnd)
+        if tune:
+            info = u.integrate_tune(DT, **kw)
+            assert info["int_warps"] in (8, 16) and info["int_sorted"] in (0, 1)
+        u.integrate(DT, **kw)
+        tk1, rho1, y1, s1, s2 = u.download()
+        ns, pa = u.integrate_counts()
+    return tk1, rho1, y1, np.stack([s1, s2]), ns, pa
+
+
+@pytest.fixture(scope="module")
+def c3(oracle):
+    f = batch_cells(333, seed=11)
+    tk, rho = nondimensional(f, oracle.scales, oracle.wm)
+    return f, tk, rho, f.p / oracle.scales["PSTR"]
+
+
+def test_integrate_matches_oracle(cuda, oracle, c3):
+    f, tk, rho, pnd = c3
+    tk1, rho1, y1, s1, ns, pa = run_gpu(cuda, f, tk, rho, pnd)
+    q = oracle.omega(tk, rho, f.y)[0]
+    ns_o, x = oracle.nsub(rho, f.y, q, DT)
+    near = np.abs(x - np.round(x)) <= 1e-9 * np.maximum(x, 1.0)
+    assert np.array_equal(ns[~near], ns_o[~near])
+    assert ns.min() >= 1 and ns.max() <= 200 and len(np.unique(ns)) > 20
+    tk_o, rho_o, y_o, s_o, pa_o = oracle.integrate(tk, rho, f.y, pnd, ns, DT)
+    sc = oracle.scales
+    # Cells whose T ends on a bound of the reference's clamp [TSTR-1, 5000 K] (solveh.f:1232-1233)
+    # have left the model: their enthalpy lies below h(TSTR-1) (cold cells whose random radical
+    # load reacts endothermically), the T Newton does not converge and where it stops after 100
+    # steps depends on the last ulp. They are counted, not compared.
+    T1, To = tk1 * sc["TSTR"], tk_o * sc["TSTR"]
+    lo, hi = sc["TSTR"] - 1.0 + 1e-6, 5000.0 - 1e-6
+    ok = (T1 > lo) & (T1 < hi) & (To > lo) & (To < hi)
+    assert ok.mean() > 0.8
+    assert np.abs(T1 - To)[ok].max() < 1e-2
+    err = np.abs(y1 - y_o) - (1e-6 * np.abs(y_o) + 1e-12)
+    assert (err[:, ok] <= 0).all(), f"worst Y excess {err[:, ok].max():.3g}"
+    assert np.allclose(rho1[ok], rho_o[ok], rtol=1e-6, atol=0)
+    assert np.abs(s1 - s_o)[:, ok].max() <= 1e-12 + 1e-6 * np.abs(s_o).max()
+    assert (np.abs(pa - pa_o)[ok] <= ns[ok]).mean() > 0.95
+
+
+def test_kernel_shapes_agree_bitwise(cuda, oracle, c3):
+    """Every tuned shape (8 or 16 warps, sorted or natural queue order) computes each cell the same way."""
+    f, tk, rho, pnd = c3
+    a = run_gpu(cuda, f, tk, rho, pnd)
+    b = run_gpu(cuda, f, tk, rho, pnd, tune=True)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
+
+
+def test_integrate_options_rejected(cuda):
+    f = batch_cells(40, seed=1)
+    with cuda.UniChem(f.n) as u:
+        tk, rho = nondimensional(f, u.scales, u.wm)
+        with pytest.raises(cuda.UniChemError):
+            u.integrate(DT)                        # no fields yet
+        u.upload(tk, rho, f.y)
+        for bad in (dict(nsub_max=0), dict(nsub_max=5000), dict(isor=0), dict(relx=1.5), dict(c_tau=0.0)):
+            with pytest.raises(cuda.UniChemError):
+                u.integrate(DT, **bad)
+        with pytest.raises(cuda.UniChemError):
+            u.integrate(DT, precision=cuda.MIXED)
+        u.integrate(DT, nsub_max=1)               # default pressure PBACK
+        ns, _ = u.integrate_counts()
+        assert (ns == 1).all()

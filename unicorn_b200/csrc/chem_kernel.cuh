@@ -49,6 +49,142 @@ __device__ __forceinline__ double gibbs_exp(const double *a, double ELOGT, doubl
     return exp(g0);
 }
 
+// Phases 1a-2 of a tile: Gibbs functions, third bodies, soot sources and
+// the RC plane of the tile in shared memory, with NW warps (NW divides 16:
+// a warp takes the pair lists of the virtual warps w, w+NW, ...). Expects the
+// tile's Y rows in sY and the scalar rows of sC; writes sRC and sG, and the
+// six soot sources to sour[m*sstride + soff] when sour is not null. Ends
+// before the barrier that publishes sRC.
+template <int NW>
+__device__ __forceinline__ void tile_rates_fp64(const DevParams &P, const PairTab *sTab, double *sRC,
+                                                const double *sY, double *sG, double *sC, double *sour,
+                                                size_t sstride, size_t soff, int lane, int warp)
+{
+    const double C1ST = P.C1ST, C2ND = P.C2ND, C3RD = P.C3RD;
+    // ---------------- phase 1a: Gibbs functions; Y/W rows (scratch in sRC)
+    {
+        const double TKD = sC[SC_TKD * TILE + lane];
+        const double ELOGT = sC[SC_LNT * TILE + lane];
+        const int ip = TKD > UC_TPOL1 ? 7 : 0;
+        for (int k = warp; k < LSP; k += NW) {
+            sG[k * TILE + lane] = gibbs_exp(P.poly + k * 14 + ip, ELOGT, TKD);
+            sRC[k * TILE + lane] = sY[k * TILE + lane] / P.WM[k];
+        }
+    }
+    __syncthreads();
+    // ---------------- phase 1b: TBODY (ordered sum)
+    if (warp == 0) {
+        double tb = sRC[lane];
+        for (int k = 1; k < LSP; ++k) tb = tb + sRC[k * TILE + lane];
+        sC[SC_TB0 * TILE + lane] = tb;
+    }
+    __syncthreads();
+    // ---------------- phase 1c: third-body groups TB001..TB010; soot sources
+    for (int j = (warp == 0 ? NW : warp); j <= 11; j += NW) {
+        if (j <= 10) {
+            const int g = j;
+            double acc = sC[SC_TB0 * TILE + lane];
+            const int o = P.tb_off[g];
+            for (int t = 0; t < P.tb_len[g]; ++t) {
+                const int k = P.tb_sp[o + t];
+                const double yk = sY[k * TILE + lane];
+                const double term = P.tb_hascoef[o + t] ? (P.tb_coef[o + t] * yk) / P.WM[k] : yk / P.WM[k];
+                acc = P.tb_sign[o + t] > 0 ? acc + term : acc - term;
+            }
+            sC[(SC_TB0 + g) * TILE + lane] = acc;
+        } else if (sour) {
+            // ckrates.f:1337-1352
+            const double PI = 3.1415927e+00, RSOOT = 1.9000e+03, SIGB = 1.38e-23, AVNO = 6.0232e+23;
+            const double CMIN = (double)100.0f, CAGL = (double)9.0f;
+            const double TKD = sC[SC_TKD * TILE + lane], rho = sC[SC_RHO * TILE + lane];
+            const double stmf = sC[SC_STMF * TILE + lane], stnd = sC[SC_STND * TILE + lane];
+            const double TBODY = sC[SC_TB0 * TILE + lane];
+            double DPST = 0.0;
+            if (stnd >= 1.0) DPST = pow(6.0 * stmf / (PI * RSOOT * stnd), (double)0.333333f);
+            const double ASST = PI * DPST * DPST * P.RSTR * rho * stnd;
+            const double SOURNU = C1ST * rho * 1.000e+04 * exp(-(2.0632e+04 / TKD)) / P.WM[21];
+            sour[soff] = SOURNU + C1ST * rho * ASST * 3.468e+03 * exp(-(1.2077e+04 / TKD)) / P.WM[21];
+            sour[sstride + soff] = 2.0 * SOURNU * AVNO / CMIN / P.WMSTR;
+            sour[2 * sstride + soff] = C1ST * rho * ASST * 1.000e+04 * pow(TKD, (double)0.5f) * exp(-(1.9626e+04 / TKD)) / P.WM[1];
+            sour[3 * sstride + soff] = (double)0.13f * C1ST * ASST * 1.060e+02 * pow(TKD, (double)-0.5f) * exp(-(0.0 / TKD)) / P.WM[4] / TBODY;
+            sour[4 * sstride + soff] = (double)0.5f * C1ST * ASST * 5.54e+00 * pow(TKD, (double)-0.5f) * exp(-(0.0 / TKD)) / P.WM[3] / TBODY;
+            sour[5 * sstride + soff] = 2.0 * C1ST * P.RSTR * CAGL * sqrt(DPST * 6.0 * SIGB * TKD / RSOOT) * rho * rho * stnd;
+        }
+    }
+    __syncthreads();
+    // ---------------- phase 2: reaction pairs -> RC plane
+    {
+        const double TKD = sC[SC_TKD * TILE + lane];
+        const double ELOGT = sC[SC_LNT * TILE + lane];
+        const double RUT = sC[SC_RUT * TILE + lane];
+        const double rho = sC[SC_RHO * TILE + lane];
+        const double CR[4] = {0.0, C1ST * rho, C2ND * (rho * rho), C3RD * (rho * rho * rho)};
+        for (int vw = warp; vw < CHEM_WARPS; vw += NW)
+        for (int i = 0; i < P.npair_of_warp[vw]; ++i) {
+            const int p = P.pair_of_warp[vw][i];
+            const PairTab &T = sTab[p];
+            double kf = T.akf * exp(T.alf * ELOGT - T.exaf / TKD);
+            double kr = 0.0;
+            if (T.has_rev) {
+                double q = sG[T.qsp[0] * TILE + lane];
+                for (int t = 1; t < T.qlen; ++t) {
+                    const double g = sG[T.qsp[t] * TILE + lane];
+                    q = T.qdiv[t] ? q / g : q * g;
+                }
+                double v = T.akf_r * kf;
+                if (T.rut < 0) v = v / RUT;
+                else if (T.rut > 0) v = v * RUT;
+                kr = v / q;
+            }
+            if (T.aklow != 0.0) {
+                // ckrates.f:740-794 (AKLOW < 0, the Tseng form, is not used by this data)
+                const double DMOLE = sC[(SC_TB0 + T.dmole) * TILE + lane] * sC[SC_DMOLEA * TILE + lane];
+                const double ACTV = T.allow * ELOGT - T.ealow / TKD;
+                const double AK0M = T.aklow * exp(ACTV) * DMOLE / (kf + 1.0e-20);
+                double RFACT;
+                if (T.troe[0] > 0.0) {
+                    double FCLOG;
+                    if (T.troe[1] == 0.0) FCLOG = log10(T.troe[0]);
+                    else FCLOG = log10((1.0 - T.troe[0]) * exp(-(TKD / T.troe[1])) +
+                                       T.troe[0] * exp(-(TKD / T.troe[2])) + exp(-(T.troe[3] / TKD)));
+                    const double CPLOG = log10(AK0M) - ((double)0.4f + (double)0.67f * FCLOG);
+                    const double z = CPLOG / ((double)0.75f - (double)1.27f * FCLOG - (double)0.14f * CPLOG);
+                    RFACT = pow(10.0, FCLOG / (1.0 + z * z));
+                } else if (T.troe[0] == 0.0) {
+                    RFACT = 1.0;
+                } else {
+                    const double l = log10(AK0M);
+                    const double XFACT = 1.0 / (1.0 + l * l);
+                    RFACT = pow(-(T.troe[0] * exp(-(T.troe[1] / TKD))) + exp(-(TKD / T.troe[2])), XFACT);
+                }
+                const double AFP = (AK0M / (1.0 + AK0M)) * RFACT;
+                kf = AFP * kf;
+                kr = AFP * kr;
+            }
+            // RC assembly, ckrates.f:796-1333
+            double rc0 = 0.0, rc1 = 0.0;
+            if (T.rc_order0) {
+                double v = CR[T.rc_order0];
+                if (T.rc_tb0 >= 0) v = v * sC[(SC_TB0 + T.rc_tb0) * TILE + lane];
+                v = v * kf;
+                for (int t = 0; t < T.rc_len0; ++t)
+                    v = T.rc_kind0[t] ? v * sY[T.rc_idx0[t] * TILE + lane] : v / P.WM[T.rc_idx0[t]];
+                rc0 = v;
+            }
+            if (T.rc_order1) {
+                double v = CR[T.rc_order1];
+                if (T.rc_tb1 >= 0) v = v * sC[(SC_TB0 + T.rc_tb1) * TILE + lane];
+                v = v * kr;
+                for (int t = 0; t < T.rc_len1; ++t)
+                    v = T.rc_kind1[t] ? v * sY[T.rc_idx1[t] * TILE + lane] : v / P.WM[T.rc_idx1[t]];
+                rc1 = v;
+            }
+            sRC[(2 * p) * TILE + lane] = rc0;
+            sRC[(2 * p + 1) * TILE + lane] = rc1;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_fp64_kernel(const ChemArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -79,7 +215,7 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_fp64_kernel(const ChemAr
         return;
     }
 
-    const double C1ST = P.C1ST, C2ND = P.C2ND, C3RD = P.C3RD, RCONV = P.RCONV;
+    const double RCONV = P.RCONV;
 
     const int nwork = a.tile_list ? *a.tile_count : a.ntile;
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
@@ -102,127 +238,7 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_fp64_kernel(const ChemAr
             sC[SC_STND * TILE + lane] = a.stnd ? a.stnd[cell] : 0.0;
         }
         __syncthreads();
-        // ---------------- phase 1a: Gibbs functions; Y/W rows (scratch in sRC)
-        {
-            const double TKD = sC[SC_TKD * TILE + lane];
-            const double ELOGT = sC[SC_LNT * TILE + lane];
-            const int ip = TKD > UC_TPOL1 ? 7 : 0;
-            for (int k = warp; k < LSP; k += CHEM_WARPS) {
-                sG[k * TILE + lane] = gibbs_exp(P.poly + k * 14 + ip, ELOGT, TKD);
-                sRC[k * TILE + lane] = sY[k * TILE + lane] / P.WM[k];
-            }
-        }
-        __syncthreads();
-        // ---------------- phase 1b: TBODY (ordered sum)
-        if (warp == 0) {
-            double tb = sRC[lane];
-            for (int k = 1; k < LSP; ++k) tb = tb + sRC[k * TILE + lane];
-            sC[SC_TB0 * TILE + lane] = tb;
-        }
-        __syncthreads();
-        // ---------------- phase 1c: third-body groups TB001..TB010; soot sources
-        if (warp >= 1 && warp <= 10) {
-            const int g = warp;
-            double acc = sC[SC_TB0 * TILE + lane];
-            const int o = P.tb_off[g];
-            for (int t = 0; t < P.tb_len[g]; ++t) {
-                const int k = P.tb_sp[o + t];
-                const double yk = sY[k * TILE + lane];
-                const double term = P.tb_hascoef[o + t] ? (P.tb_coef[o + t] * yk) / P.WM[k] : yk / P.WM[k];
-                acc = P.tb_sign[o + t] > 0 ? acc + term : acc - term;
-            }
-            sC[(SC_TB0 + g) * TILE + lane] = acc;
-        } else if (warp == 11 && a.sour) {
-            // ckrates.f:1337-1352
-            const double PI = 3.1415927e+00, RSOOT = 1.9000e+03, SIGB = 1.38e-23, AVNO = 6.0232e+23;
-            const double CMIN = (double)100.0f, CAGL = (double)9.0f;
-            const double TKD = sC[SC_TKD * TILE + lane], rho = sC[SC_RHO * TILE + lane];
-            const double stmf = sC[SC_STMF * TILE + lane], stnd = sC[SC_STND * TILE + lane];
-            const double TBODY = sC[SC_TB0 * TILE + lane];
-            double DPST = 0.0;
-            if (stnd >= 1.0) DPST = pow(6.0 * stmf / (PI * RSOOT * stnd), (double)0.333333f);
-            const double ASST = PI * DPST * DPST * P.RSTR * rho * stnd;
-            const double SOURNU = C1ST * rho * 1.000e+04 * exp(-(2.0632e+04 / TKD)) / P.WM[21];
-            const size_t np = a.npad;
-            a.sour[cell] = SOURNU + C1ST * rho * ASST * 3.468e+03 * exp(-(1.2077e+04 / TKD)) / P.WM[21];
-            a.sour[np + cell] = 2.0 * SOURNU * AVNO / CMIN / P.WMSTR;
-            a.sour[2 * np + cell] = C1ST * rho * ASST * 1.000e+04 * pow(TKD, (double)0.5f) * exp(-(1.9626e+04 / TKD)) / P.WM[1];
-            a.sour[3 * np + cell] = (double)0.13f * C1ST * ASST * 1.060e+02 * pow(TKD, (double)-0.5f) * exp(-(0.0 / TKD)) / P.WM[4] / TBODY;
-            a.sour[4 * np + cell] = (double)0.5f * C1ST * ASST * 5.54e+00 * pow(TKD, (double)-0.5f) * exp(-(0.0 / TKD)) / P.WM[3] / TBODY;
-            a.sour[5 * np + cell] = 2.0 * C1ST * P.RSTR * CAGL * sqrt(DPST * 6.0 * SIGB * TKD / RSOOT) * rho * rho * stnd;
-        }
-        __syncthreads();
-        // ---------------- phase 2: reaction pairs -> RC plane
-        {
-            const double TKD = sC[SC_TKD * TILE + lane];
-            const double ELOGT = sC[SC_LNT * TILE + lane];
-            const double RUT = sC[SC_RUT * TILE + lane];
-            const double rho = sC[SC_RHO * TILE + lane];
-            const double CR[4] = {0.0, C1ST * rho, C2ND * (rho * rho), C3RD * (rho * rho * rho)};
-            const int np = P.npair_of_warp[warp];
-            for (int i = 0; i < np; ++i) {
-                const int p = P.pair_of_warp[warp][i];
-                const PairTab &T = sTab[p];
-                double kf = T.akf * exp(T.alf * ELOGT - T.exaf / TKD);
-                double kr = 0.0;
-                if (T.has_rev) {
-                    double q = sG[T.qsp[0] * TILE + lane];
-                    for (int t = 1; t < T.qlen; ++t) {
-                        const double g = sG[T.qsp[t] * TILE + lane];
-                        q = T.qdiv[t] ? q / g : q * g;
-                    }
-                    double v = T.akf_r * kf;
-                    if (T.rut < 0) v = v / RUT;
-                    else if (T.rut > 0) v = v * RUT;
-                    kr = v / q;
-                }
-                if (T.aklow != 0.0) {
-                    // ckrates.f:740-794 (AKLOW < 0, the Tseng form, is not used by this data)
-                    const double DMOLE = sC[(SC_TB0 + T.dmole) * TILE + lane] * sC[SC_DMOLEA * TILE + lane];
-                    const double ACTV = T.allow * ELOGT - T.ealow / TKD;
-                    const double AK0M = T.aklow * exp(ACTV) * DMOLE / (kf + 1.0e-20);
-                    double RFACT;
-                    if (T.troe[0] > 0.0) {
-                        double FCLOG;
-                        if (T.troe[1] == 0.0) FCLOG = log10(T.troe[0]);
-                        else FCLOG = log10((1.0 - T.troe[0]) * exp(-(TKD / T.troe[1])) +
-                                           T.troe[0] * exp(-(TKD / T.troe[2])) + exp(-(T.troe[3] / TKD)));
-                        const double CPLOG = log10(AK0M) - ((double)0.4f + (double)0.67f * FCLOG);
-                        const double z = CPLOG / ((double)0.75f - (double)1.27f * FCLOG - (double)0.14f * CPLOG);
-                        RFACT = pow(10.0, FCLOG / (1.0 + z * z));
-                    } else if (T.troe[0] == 0.0) {
-                        RFACT = 1.0;
-                    } else {
-                        const double l = log10(AK0M);
-                        const double XFACT = 1.0 / (1.0 + l * l);
-                        RFACT = pow(-(T.troe[0] * exp(-(T.troe[1] / TKD))) + exp(-(TKD / T.troe[2])), XFACT);
-                    }
-                    const double AFP = (AK0M / (1.0 + AK0M)) * RFACT;
-                    kf = AFP * kf;
-                    kr = AFP * kr;
-                }
-                // RC assembly, ckrates.f:796-1333
-                double rc0 = 0.0, rc1 = 0.0;
-                if (T.rc_order0) {
-                    double v = CR[T.rc_order0];
-                    if (T.rc_tb0 >= 0) v = v * sC[(SC_TB0 + T.rc_tb0) * TILE + lane];
-                    v = v * kf;
-                    for (int t = 0; t < T.rc_len0; ++t)
-                        v = T.rc_kind0[t] ? v * sY[T.rc_idx0[t] * TILE + lane] : v / P.WM[T.rc_idx0[t]];
-                    rc0 = v;
-                }
-                if (T.rc_order1) {
-                    double v = CR[T.rc_order1];
-                    if (T.rc_tb1 >= 0) v = v * sC[(SC_TB0 + T.rc_tb1) * TILE + lane];
-                    v = v * kr;
-                    for (int t = 0; t < T.rc_len1; ++t)
-                        v = T.rc_kind1[t] ? v * sY[T.rc_idx1[t] * TILE + lane] : v / P.WM[T.rc_idx1[t]];
-                    rc1 = v;
-                }
-                sRC[(2 * p) * TILE + lane] = rc0;
-                sRC[(2 * p + 1) * TILE + lane] = rc1;
-            }
-        }
+        tile_rates_fp64<CHEM_WARPS>(P, sTab, sRC, sY, sG, sC, a.sour, a.npad, cell, lane, warp);
         __syncthreads();
         // ---------------- phase 3: RC out (optional), species sums
         if (a.rc)

@@ -19,6 +19,7 @@ constexpr int MAX_SPEC_PER_WARP = 8;
 constexpr int ST_OK = 0;
 constexpr int ST_TMA_TIMEOUT = 1;
 constexpr int ST_NEWTON_NOCONV = 2;
+constexpr int ST_BAD_ORDER = 3;
 
 // One reaction pair of the mechanism: forward slot 2p and reverse slot 2p+1
 // (0-based). Staged into shared memory by a bulk (TMA) copy at kernel start.
@@ -41,7 +42,7 @@ static_assert(PAIRTAB_BYTES % 16 == 0, "bulk copy size must be a multiple of 16 
 // static work split of the species phase.
 struct DevParams {
     double TSTR, RSTR, WMSTR, ALSTR, VSTR, HSTR, GASC, PBACK, CONVRC, CONVRM, CONVRD;
-    double C1ST, C2ND, C3RD, RCONV, HCONVR, TKDMIN, RSTR_WMSTR;
+    double C1ST, C2ND, C3RD, RCONV, HCONVR, TKDMIN, RSTR_WMSTR, BETA1;
     double WM[LSP], HFO[LSP];
     double poly[LSP * 14];
     double om22[LSP * 12];

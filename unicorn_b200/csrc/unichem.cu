@@ -14,6 +14,7 @@
 #include "chem_mixed_kernel.cuh"
 #include "props_kernel.cuh"
 #include "update_kernel.cuh"
+#include "integrate_kernel.cuh"
 
 using namespace uc;
 
@@ -38,6 +39,15 @@ struct uc_ctx {
     int *status = nullptr, *passes = nullptr;
     bool have_fields = false, have_rc = false;
     int upd_grid = 0;
+    // batched integration
+    double *pnd = nullptr;
+    int *nsub = nullptr, *order = nullptr, *hist = nullptr, *next_tile = nullptr, *cpasses = nullptr;
+    cudaGraph_t int_graph = nullptr;
+    cudaGraphExec_t int_exec = nullptr;
+    uc_integrate_opts int_opts{};
+    int int_prec = -1, int_gwarps = 0, int_gsorted = -1;   // what the captured graph was built for
+    int int_warps = 16, int_sorted = 1;                     // kernel shape in use (tuned)
+    double tune_best = 0.0, tune_worst = 0.0;
     // tracing: CUDA event pairs around launches
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -156,6 +166,7 @@ static void build_params(const uc_inputs &in, DevParams &P, std::vector<PairTab>
     P.HCONVR = GASC / sc.wmstr / sc.hstr;
     P.TKDMIN = sc.tstr - 1.0;
     P.RSTR_WMSTR = sc.rstr / sc.wmstr;
+    P.BETA1 = sc.beta1;
     for (int k = 0; k < LSP; ++k) {   // main:461-464
         P.WM[k] = uc_wsp[k] / 1000.0 / sc.wmstr;
         P.HFO[k] = sc.hconv * uc_poly[k * 14 + 5] / P.WM[k];
@@ -296,6 +307,14 @@ static void free_ctx(uc_ctx *c)
     if (c->tile_count) cudaFree(c->tile_count);
     if (c->status) cudaFree(c->status);
     if (c->passes) cudaFree(c->passes);
+    {
+        int **ibufs[] = {&c->nsub, &c->order, &c->hist, &c->next_tile, &c->cpasses};
+        for (auto b : ibufs)
+            if (*b) { cudaFree(*b); *b = nullptr; }
+        if (c->pnd) cudaFree(c->pnd);
+        if (c->int_exec) cudaGraphExecDestroy(c->int_exec);
+        if (c->int_graph) cudaGraphDestroy(c->int_graph);
+    }
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     c->ev_pool.clear();
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -354,6 +373,10 @@ static int check_status(uc_ctx *ctx)
     if (st == ST_TMA_TIMEOUT) {
         CK(cudaMemsetAsync(ctx->status, 0, sizeof(int), ctx->stream));
         return set_err(ctx, UC_E_TIMEOUT, "table staging (bulk copy) timed out on the device");
+    }
+    if (st == ST_BAD_ORDER) {
+        CK(cudaMemsetAsync(ctx->status, 0, sizeof(int), ctx->stream));
+        return set_err(ctx, UC_E_CUDA, "integration work order out of range (internal error)");
     }
     if (st == ST_NEWTON_NOCONV) {
         CK(cudaMemsetAsync(ctx->status, 0, sizeof(int), ctx->stream));
@@ -766,6 +789,10 @@ extern "C" int uc_stat(uc_ctx *ctx, const char *name, double *value)
 {
     if (!ctx || !name || !value) return UC_E_ARG;
     if (!strcmp(name, "tiles")) { *value = ctx->ntile; return UC_OK; }
+    if (!strcmp(name, "int_warps")) { *value = ctx->int_warps; return UC_OK; }
+    if (!strcmp(name, "int_sorted")) { *value = ctx->int_sorted; return UC_OK; }
+    if (!strcmp(name, "int_tune_best_ms")) { *value = ctx->tune_best; return UC_OK; }
+    if (!strcmp(name, "int_tune_worst_ms")) { *value = ctx->tune_worst; return UC_OK; }
     if (!strcmp(name, "mixed_fp64_tiles")) {
         int c = 0;
         if (ctx->tile_count) {
@@ -809,6 +836,236 @@ extern "C" int uc_device_view_get(uc_ctx *ctx, uc_device_view *v)
     v->n = ctx->n; v->npad = ctx->npad;
     v->stream = (void *)ctx->stream;
     return UC_OK;
+}
+
+// ------------------------------------------------------------------ batched stiff integration
+
+static bool same_opts(const uc_integrate_opts &a, const uc_integrate_opts &b)
+{
+    return a.dt == b.dt && a.isor == b.isor && a.relx == b.relx && a.tol == b.tol && a.c_tau == b.c_tau &&
+           a.y_tau == b.y_tau && a.nsub_max == b.nsub_max;
+}
+
+static int check_opts(uc_ctx *ctx, const uc_integrate_opts *o)
+{
+    if (!o) return set_err(ctx, UC_E_ARG, "integration options are required");
+    if (!(o->dt > 0.0) || o->isor < 1 || !(o->relx > 0.0 && o->relx <= 1.0) || !(o->tol >= 0.0) || !(o->c_tau > 0.0) ||
+        !(o->y_tau >= 0.0) || o->nsub_max < 1 || o->nsub_max > SORT_MAXBIN)
+        return set_err(ctx, UC_E_ARG, "integration options out of range (dt>0, isor>=1, 0<relx<=1, tol>=0, c_tau>0, "
+                                      "y_tau>=0, 1<=nsub_max<=%d)", SORT_MAXBIN);
+    return UC_OK;
+}
+
+static int integrate_buffers(uc_ctx *ctx)
+{
+    const size_t np = ctx->npad;
+    const int nchunk = (ctx->n + SORT_CHUNK - 1) / SORT_CHUNK;
+    if (!ctx->pnd) {
+        RET_IF(dalloc(ctx, &ctx->pnd, np));
+        std::vector<double> pb(np, ctx->sc.pback);
+        CK(cudaMemcpy(ctx->pnd, pb.data(), np * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    RET_IF(dalloc(ctx, &ctx->qdsp, (size_t)LSP * np));
+    int **bufs[] = {&ctx->nsub, &ctx->order, &ctx->cpasses, &ctx->hist, &ctx->next_tile};
+    const size_t counts[] = {np, np, np, (size_t)(SORT_MAXBIN + 1) * nchunk, 1};
+    for (int i = 0; i < 5; ++i)
+        if (!*bufs[i]) {
+            cudaError_t e = cudaMalloc((void **)bufs[i], counts[i] * sizeof(int));
+            if (e != cudaSuccess) {
+                *bufs[i] = nullptr;
+                return set_err(ctx, UC_E_NOMEM, "integration buffers: %s", cudaGetErrorString(e));
+            }
+        }
+    return UC_OK;
+}
+
+extern "C" int uc_set_pressure(uc_ctx *ctx, const double *pnd)
+{
+    if (!ctx || !pnd) return set_err(ctx, UC_E_ARG, "uc_set_pressure: pressures are required");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(dalloc(ctx, &ctx->pnd, ctx->npad));
+    RET_IF(upload_rows(ctx, ctx->pnd, pnd, 1));
+    return UC_OK;
+}
+
+template <int NW>
+static bool set_integrate_attr()
+{
+    return cudaFuncSetAttribute(integrate_fp64_kernel<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INT_SMEM) ==
+           cudaSuccess;
+}
+
+// Enqueue one integration step on the context's stream (graph capture or not).
+static int enqueue_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts &o, int warps, int sorted)
+{
+    const int np = ctx->npad;
+    // omega of the start state (QDSP rows) for the sub-step counts
+    if (precision == UC_MIXED) {
+        ChemMArgs m{};
+        m.P = ctx->dP; m.tab = ctx->dTabM;
+        m.tk = ctx->tk; m.rho = ctx->rho; m.y = ctx->y; m.stmf = ctx->soot; m.stnd = ctx->soot + np;
+        m.qdsp = ctx->qdsp; m.tile_flag = ctx->tile_flag;
+        m.n = ctx->n; m.npad = np; m.ntile = ctx->ntile; m.status = ctx->status;
+        chem_mixed_kernel<<<std::min(ctx->ntile, ctx->nsm), CHEM_THREADS, CHEMM_SMEM, ctx->stream>>>(m);
+        CK(cudaGetLastError());
+        compact_tiles_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->tile_flag, ctx->ntile, ctx->tile_list, ctx->tile_count);
+        CK(cudaGetLastError());
+    }
+    ChemArgs c{};
+    c.P = ctx->dP; c.tab = ctx->dTab;
+    c.tk = ctx->tk; c.rho = ctx->rho; c.y = ctx->y; c.stmf = ctx->soot; c.stnd = ctx->soot + np;
+    c.qdsp = ctx->qdsp;
+    c.n = ctx->n; c.npad = np; c.ntile = ctx->ntile; c.status = ctx->status;
+    if (precision == UC_MIXED) { c.tile_list = ctx->tile_list; c.tile_count = ctx->tile_count; }
+    chem_fp64_kernel<<<std::min(ctx->ntile, ctx->nsm), CHEM_THREADS, CHEM_SMEM, ctx->stream>>>(c);
+    CK(cudaGetLastError());
+    nsub_kernel<<<std::max(1, std::min((np + 255) / 256, ctx->nsm * 8)), 256, 0, ctx->stream>>>(
+        ctx->dP, ctx->rho, ctx->y, ctx->qdsp, ctx->n, np, o.dt, o.c_tau, o.y_tau, o.nsub_max, ctx->nsub);
+    CK(cudaGetLastError());
+    if (sorted) {
+        const int nchunk = (ctx->n + SORT_CHUNK - 1) / SORT_CHUNK;
+        sort_count_kernel<<<nchunk, 256, 0, ctx->stream>>>(ctx->nsub, ctx->n, o.nsub_max, nchunk, ctx->hist);
+        CK(cudaGetLastError());
+        sort_scan_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->hist, (o.nsub_max + 1) * nchunk);
+        CK(cudaGetLastError());
+        sort_scatter_kernel<<<nchunk, 32, 0, ctx->stream>>>(ctx->nsub, ctx->n, np, o.nsub_max, nchunk, ctx->hist,
+                                                           ctx->order);
+        CK(cudaGetLastError());
+    }
+    CK(cudaMemsetAsync(ctx->next_tile, 0, sizeof(int), ctx->stream));
+    IntArgs a{};
+    a.P = ctx->dP; a.tab = ctx->dTab;
+    a.tk = ctx->tk; a.rho = ctx->rho; a.y = ctx->y; a.soot = ctx->soot; a.pnd = ctx->pnd;
+    a.nsub = ctx->nsub; a.order = sorted ? ctx->order : nullptr; a.next_tile = ctx->next_tile;
+    a.passes = ctx->cpasses; a.status = ctx->status;
+    a.dt = o.dt; a.sor1 = o.relx; a.tol = o.tol; a.isor = o.isor;
+    a.n = ctx->n; a.npad = np; a.ntile = ctx->ntile;
+    const int grid = std::min(ctx->ntile, ctx->nsm);
+    if (warps == 16)
+        integrate_fp64_kernel<16><<<grid, 16 * 32, INT_SMEM, ctx->stream>>>(a);
+    else if (warps == 8)
+        integrate_fp64_kernel<8><<<grid, 8 * 32, INT_SMEM, ctx->stream>>>(a);
+    else
+        return set_err(ctx, UC_E_ARG, "integration kernel shape %d warps is not built", warps);
+    CK(cudaGetLastError());
+    return UC_OK;
+}
+
+static int integrate_prepare(uc_ctx *ctx, int precision, const uc_integrate_opts *o)
+{
+    if (!ctx) return UC_E_ARG;
+    if (precision != UC_FP64) return set_err(ctx, UC_E_ARG, "integration precision %d is not available", precision);
+    RET_IF(check_opts(ctx, o));
+    if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "no fields uploaded");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(integrate_buffers(ctx));
+    if (precision == UC_MIXED && !ctx->tile_flag) {
+        if (cudaMalloc((void **)&ctx->tile_flag, ctx->ntile * sizeof(int)) != cudaSuccess ||
+            cudaMalloc((void **)&ctx->tile_list, ctx->ntile * sizeof(int)) != cudaSuccess ||
+            cudaMalloc((void **)&ctx->tile_count, sizeof(int)) != cudaSuccess)
+            return set_err(ctx, UC_E_NOMEM, "tile flag buffers");
+    }
+    if (!set_integrate_attr<16>() || !set_integrate_attr<8>())
+        return set_err(ctx, UC_E_CUDA, "integration kernel shared-memory attribute");
+    return UC_OK;
+}
+
+extern "C" int uc_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts *o)
+{
+    RET_IF(integrate_prepare(ctx, precision, o));
+    const bool fresh = ctx->int_exec && ctx->int_prec == precision && ctx->int_gwarps == ctx->int_warps &&
+                       ctx->int_gsorted == ctx->int_sorted && same_opts(ctx->int_opts, *o);
+    if (!fresh) {
+        if (ctx->int_exec) { cudaGraphExecDestroy(ctx->int_exec); ctx->int_exec = nullptr; }
+        if (ctx->int_graph) { cudaGraphDestroy(ctx->int_graph); ctx->int_graph = nullptr; }
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue_integrate(ctx, precision, *o, ctx->int_warps, ctx->int_sorted);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc != UC_OK) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return set_err(ctx, UC_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&ctx->int_exec, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return set_err(ctx, UC_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        }
+        ctx->int_graph = g;
+        ctx->int_prec = precision;
+        ctx->int_gwarps = ctx->int_warps;
+        ctx->int_gsorted = ctx->int_sorted;
+        ctx->int_opts = *o;
+    }
+    int slot;
+    prof_begin(ctx, UC_K_INTEGRATE, slot);
+    CK(cudaGraphLaunch(ctx->int_exec, ctx->stream));
+    prof_end(ctx, slot);
+    return UC_OK;
+}
+
+extern "C" int uc_integrate_tune(uc_ctx *ctx, int precision, const uc_integrate_opts *o)
+{
+    RET_IF(integrate_prepare(ctx, precision, o));
+    const size_t np = ctx->npad;
+    // save the state, run each shape once from it, keep the fastest
+    double *save = nullptr;
+    const size_t nd = (size_t)(LSP + 4) * np;
+    cudaError_t e = cudaMalloc((void **)&save, nd * sizeof(double));
+    if (e != cudaSuccess) return set_err(ctx, UC_E_NOMEM, "tuning copy of the state: %s", cudaGetErrorString(e));
+    auto copy_state = [&](bool to_save) -> cudaError_t {
+        double *src[4] = {ctx->tk, ctx->rho, ctx->y, ctx->soot};
+        const size_t cnt[4] = {np, np, (size_t)LSP * np, 2 * np};
+        size_t off = 0;
+        for (int i = 0; i < 4; ++i) {
+            cudaError_t r = to_save ? cudaMemcpyAsync(save + off, src[i], cnt[i] * sizeof(double),
+                                                      cudaMemcpyDeviceToDevice, ctx->stream)
+                                    : cudaMemcpyAsync(src[i], save + off, cnt[i] * sizeof(double),
+                                                      cudaMemcpyDeviceToDevice, ctx->stream);
+            if (r != cudaSuccess) return r;
+            off += cnt[i];
+        }
+        return cudaSuccess;
+    };
+    const int shapes[4][2] = {{16, 1}, {8, 1}, {16, 0}, {8, 0}};
+    double best = 1e300, worst = 0.0;
+    int bw = 16, bs = 1, rc = UC_OK;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    if (copy_state(true) != cudaSuccess) rc = set_err(ctx, UC_E_CUDA, "tuning: state copy failed");
+    for (int i = 0; i < 4 && rc == UC_OK; ++i) {
+        cudaEventRecord(e0, ctx->stream);
+        rc = enqueue_integrate(ctx, precision, *o, shapes[i][0], shapes[i][1]);
+        cudaEventRecord(e1, ctx->stream);
+        if (rc != UC_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "tuning run failed"); break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) { best = ms; bw = shapes[i][0]; bs = shapes[i][1]; }
+        if (ms > worst) worst = ms;
+        if (copy_state(false) != cudaSuccess) rc = set_err(ctx, UC_E_CUDA, "tuning: state restore failed");
+    }
+    cudaStreamSynchronize(ctx->stream);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(save);
+    if (rc != UC_OK) return rc;
+    ctx->int_warps = bw;
+    ctx->int_sorted = bs;
+    ctx->tune_best = best;
+    ctx->tune_worst = worst;
+    const int st = check_status(ctx);
+    return st == UC_E_NOCONV ? UC_OK : st;   // a Newton that ran out of steps is reported by uc_integrate_counts
+}
+
+extern "C" int uc_integrate_counts(uc_ctx *ctx, int *nsub, int *passes)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->nsub) return set_err(ctx, UC_E_STATE, "no integration has run");
+    if (nsub) CK(cudaMemcpyAsync(nsub, ctx->nsub, (size_t)ctx->n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (passes)
+        CK(cudaMemcpyAsync(passes, ctx->cpasses, (size_t)ctx->n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_status(ctx);
 }
 
 // ------------------------------------------------------------------ no-allocation update

@@ -58,6 +58,12 @@ DEFAULT_INPUTS = dict(rtin=0.0, rtot=0.100, vref=10.0, tref=294.0, pref=1.0133e5
 _lib = None
 
 
+class IntegrateOpts(ctypes.Structure):
+    """uc_integrate_opts: batched stiff integration settings."""
+    _fields_ = [("dt", ctypes.c_double), ("isor", ctypes.c_int), ("relx", ctypes.c_double), ("tol", ctypes.c_double),
+                ("c_tau", ctypes.c_double), ("y_tau", ctypes.c_double), ("nsub_max", ctypes.c_int)]
+
+
 def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     """Load libunichem.so; raises if it is missing (no CPU fallback exists)."""
     global _lib
@@ -90,6 +96,11 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.uc_last_error.restype = ctypes.c_char_p
     lib.uc_destroy.argtypes = [vp]
     lib.uc_destroy.restype = None
+    IP = ctypes.POINTER(ctypes.c_int)
+    lib.uc_set_pressure.argtypes = [vp, P]
+    lib.uc_integrate.argtypes = [vp, ctypes.c_int, ctypes.POINTER(IntegrateOpts)]
+    lib.uc_integrate_tune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(IntegrateOpts)]
+    lib.uc_integrate_counts.argtypes = [vp, IP, IP]
     _lib = lib
     return lib
 
@@ -174,7 +185,16 @@ class UniChem:
         return tk, rho, y, s1, s2
 
     def sync(self):
-        self._ck(self.lib.uc_sync(self._h))
+        """Wait for the context's stream; a T Newton that ran out of steps is a warning
+        (the reference prints one and carries on), every other error raises."""
+        self._ck_warn(self.lib.uc_sync(self._h))
+
+    def _ck_warn(self, rc: int):
+        if rc == -5:
+            import warnings
+            warnings.warn(self.lib.uc_last_error(self._h).decode())
+        else:
+            self._ck(rc)
 
     # ------------------------------------------------------------ hot path
     def ckrates(self, precision: int = FP64, return_rc: bool = False):
@@ -245,11 +265,41 @@ class UniChem:
 
     def profile_read(self) -> dict:
         """Device time (ms) and launches per kernel kind since the last read."""
-        ms = np.zeros(5)
-        cnt = (ctypes.c_int * 5)()
+        ms = np.zeros(6)
+        cnt = (ctypes.c_int * 6)()
         self._ck(self.lib.uc_profile_read(self._h, _p(ms), cnt))
-        names = ["chem", "update", "props", "cp_h", "temperature"]
+        names = ["chem", "update", "props", "cp_h", "temperature", "integrate"]
         return {nm: (float(ms[i]), int(cnt[i])) for i, nm in enumerate(names)}
+
+    # ------------------------------------------------------------ batched integration
+    @staticmethod
+    def integrate_opts(dt: float, isor: int = 100, relx: float = 0.99, tol: float = 1e-8, c_tau: float = 1.0,
+                       y_tau: float = 1e-3, nsub_max: int = 200) -> IntegrateOpts:
+        return IntegrateOpts(dt, int(isor), relx, tol, c_tau, y_tau, int(nsub_max))
+
+    def set_pressure(self, pnd):
+        """Cell pressures p/PSTR (the reference's non-dimensional pressure)."""
+        self._ck(self.lib.uc_set_pressure(self._h, _p(_in(pnd, (self.n,)))))
+
+    def integrate(self, dt: float, precision: int = FP64, **kw):
+        """Advance every cell over dt (uc_integrate); the state stays on the device."""
+        o = self.integrate_opts(dt, **kw)
+        self._ck(self.lib.uc_integrate(self._h, precision, ctypes.byref(o)))
+
+    def integrate_tune(self, dt: float, precision: int = FP64, **kw) -> dict:
+        o = self.integrate_opts(dt, **kw)
+        self._ck(self.lib.uc_integrate_tune(self._h, precision, ctypes.byref(o)))
+        return {k: self.stat(k) for k in ("int_warps", "int_sorted", "int_tune_best_ms", "int_tune_worst_ms")}
+
+    def integrate_counts(self):
+        """(n_sub[n], update passes[n]) of the last integration."""
+        ns = np.empty(self.n, dtype=np.int32)
+        pa = np.empty(self.n, dtype=np.int32)
+        IP = ctypes.POINTER(ctypes.c_int)
+        # a T-from-h Newton that ran out of steps in some cell is a warning: the
+        # reference prints one and carries on with the clamped value, and so does the integration
+        self._ck_warn(self.lib.uc_integrate_counts(self._h, ns.ctypes.data_as(IP), pa.ctypes.data_as(IP)))
+        return ns, pa
 
     def temperature(self, ht):
         """T from h; a cell whose Newton iteration ran out of steps is reported
