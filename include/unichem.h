@@ -21,6 +21,8 @@
 #ifndef UNICHEM_H
 #define UNICHEM_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -209,6 +211,14 @@ int uc_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts *o);
 int uc_integrate_tune(uc_ctx *ctx, int precision, const uc_integrate_opts *o);
 /* Per-cell sub-step counts and update passes of the last uc_integrate (host [n], either may be NULL). */
 int uc_integrate_counts(uc_ctx *ctx, int *nsub, int *passes);
+
+/* ---------------------------------------------------------------------------
+ * The BF16 tensor-core GEMM of the surrogate network, on host buffers (no
+ * reference counterpart; the surrogate is not part of the reference):
+ * c[M][N] (FP32) = a[M][K] * b[N][K]^T with a, b BF16 bit patterns, row-major.
+ * N a multiple of 16, K a multiple of 64. Allocates and frees its own device
+ * buffers; meant for checking the kernel, not for speed. */
+int uc_gemm_bf16(int device, int M, int N, int K, const uint16_t *a, const uint16_t *b, float *c);
 
 /* ---------------------------------------------------------------------------
  * Species update on caller-owned device arrays, with no device allocation.

@@ -1,0 +1,212 @@
+// BF16 tensor-core GEMM for the surrogate network (sm_100a, tcgen05).
+//
+//   C[M, N] = A[M, K] * B[N, K]^T      (A, B bf16, row-major, K contiguous; FP32 accumulate)
+//
+// One CTA of 4 warps computes a 128 x Nt tile (Nt <= 256, a multiple of 16)
+// with the accumulator in tensor memory (TMEM, Nt columns of 128 lanes):
+//   1. all threads copy a 128 x 64 chunk of A and an Nt x 64 chunk of B from
+//      global memory into shared memory in the canonical K-major layout
+//      without swizzle (8 x 8 "core matrices" of 128 contiguous bytes; core
+//      matrices adjacent in K are 128 B apart, 8-row groups 1024 B apart);
+//   2. one thread issues four tcgen05.mma (K = 16 each) and commits them to an
+//      mbarrier; the CTA waits (bounded) before the chunk's shared memory is
+//      rewritten;
+//   3. after the last chunk each warp reads its 32 TMEM lanes (rows) with
+//      tcgen05.ld and applies the epilogue (bias, GELU, its derivative,
+//      conversions) on the way to global memory.
+// The epilogues are those the network needs: forward layers (bias + GELU,
+// keeping the pre-activation for the backward pass), the output layer (bias,
+// FP32 out), the input gradient of a hidden layer (times GELU'(z)) and the
+// weight gradient (FP32 out).
+#pragma once
+#include <cuda_bf16.h>
+#include <cstdint>
+
+#include "uc_device.cuh"
+
+namespace uc {
+
+constexpr int GM = 128;          // rows of a CTA tile (TMEM lanes)
+constexpr int GK = 64;           // K chunk staged in shared memory
+constexpr int GN_MAX = 256;      // columns of a CTA tile (TMEM columns)
+constexpr int GEMM_THREADS = 128;
+constexpr size_t GEMM_SMEM = (size_t)(GM + GN_MAX) * GK * 2 + 64;
+// dynamic shared memory asked at launch: above the tile's need, so that at most two
+// CTAs (2 x 256 TMEM columns) share an SM
+constexpr size_t GEMM_SMEM_LAUNCH = 100 * 1024;
+
+enum GemmEpi : int {
+    EPI_F32 = 0,        // C as FP32 (out_f32, ldo)
+    EPI_BIAS_GELU = 1,  // z = C + bias -> z_save (FP32), gelu(z) -> out_bf16
+    EPI_BIAS_F32 = 2,   // C + bias -> out_f32
+    EPI_DGELU = 3,      // C * gelu'(z_in) -> out_bf16 (gradient w.r.t. a hidden pre-activation)
+    EPI_BIAS_BF16 = 4,  // C + bias -> out_bf16 (no activation)
+};
+
+struct GemmArgs {
+    const __nv_bfloat16 *A;
+    const __nv_bfloat16 *B;
+    int lda, ldb;                 // row strides in elements (multiples of 8)
+    int M, N, K;                  // N, K multiples of 16 and 64 respectively
+    int epi;
+    const float *bias;            // [N]
+    const float *z_in;            // [M][ldz] (EPI_DGELU)
+    float *z_save;                // [M][ldz] (EPI_BIAS_GELU)
+    int ldz;
+    float *out_f32;               // [M][ldo]
+    __nv_bfloat16 *out_bf16;      // [M][ldo]
+    int ldo;
+    int *status;
+};
+
+__device__ __forceinline__ float gelu_f(float x)
+{
+    return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f));
+}
+__device__ __forceinline__ float gelu_grad_f(float x)
+{
+    return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.3989422804014327f * expf(-0.5f * x * x);
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;                        // descriptor version of sm_100
+    return d;                                      // base offset 0, layout type 0 (no swizzle)
+}
+
+// instruction descriptor of kind::f16: BF16 x BF16 -> FP32, both K-major, M x N
+__host__ __device__ constexpr uint32_t mma_idesc(int m, int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__global__ void __launch_bounds__(GEMM_THREADS) gemm_bf16_tc_kernel(const GemmArgs g)
+{
+    extern __shared__ __align__(1024) unsigned char gsm[];
+    unsigned char *sA = gsm;                                  // 128 x 64 bf16 = 16 KB
+    unsigned char *sB = gsm + GM * GK * 2;                    // Nt x 64 bf16 <= 32 KB
+    uint64_t *bar = reinterpret_cast<uint64_t *>(gsm + (GM + GN_MAX) * GK * 2);
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * GM, n0 = blockIdx.y * GN_MAX;
+    const int nt = min(GN_MAX, g.N - n0);                     // multiple of 16
+    const uint32_t ncols = nt <= 32 ? 32 : nt <= 64 ? 64 : nt <= 128 ? 128 : 256;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) mbar_init(bar, 1);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = mma_idesc(GM, nt);
+    const int nchunk = g.K / GK;
+    bool ok = true;
+
+    for (int kc = 0; kc < nchunk; ++kc) {
+        const int k0 = kc * GK;
+        // ---- stage A (128 x 64) and B (nt x 64), 16-byte pieces, canonical K-major layout
+        for (int i = tid; i < GM * (GK / 8); i += GEMM_THREADS) {
+            const int r = i >> 3, kb = i & 7;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (m0 + r < g.M) v = *reinterpret_cast<const uint4 *>(g.A + (size_t)(m0 + r) * g.lda + k0 + kb * 8);
+            *reinterpret_cast<uint4 *>(sA + ((r >> 3) * (GK / 8) + kb) * 128 + (r & 7) * 16) = v;
+        }
+        for (int i = tid; i < nt * (GK / 8); i += GEMM_THREADS) {
+            const int r = i >> 3, kb = i & 7;
+            const uint4 v = *reinterpret_cast<const uint4 *>(g.B + (size_t)(n0 + r) * g.ldb + k0 + kb * 8);
+            *reinterpret_cast<uint4 *>(sB + ((r >> 3) * (GK / 8) + kb) * 128 + (r & 7) * 16) = v;
+        }
+        // generic-proxy writes -> visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (tid == 0) {
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+            for (int kk = 0; kk < GK / 16; ++kk) {
+                const uint64_t ad = smem_desc(a0 + kk * 256, 128, (GK / 8) * 128);
+                const uint64_t bd = smem_desc(b0 + kk * 256, 128, (GK / 8) * 128);
+                const uint32_t acc = (kc > 0 || kk > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(bar))
+                         : "memory");
+        }
+        // the chunk's shared memory is read by the MMAs until they complete
+        const bool done = mbar_wait_bounded(bar, (uint32_t)(kc & 1), 1 << 22);
+        if (!done) {
+            if (tid == 0) atomicExch(g.status, ST_MMA_TIMEOUT);
+            mbar_wait_bounded(bar, (uint32_t)(kc & 1), 1 << 22);   // let work in flight land
+        }
+        tc_fence_after();
+        if (!__syncthreads_and(done)) { ok = false; break; }    // the same decision in every thread
+    }
+
+    // ---- epilogue: warp w reads TMEM lanes 32w..32w+31 (rows), 16 columns at a time
+    const int row = m0 + warp * 32 + lane;
+    if (ok) {
+        for (int c0 = 0; c0 < nt; c0 += 16) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < g.M) {
+                const int n = n0 + c0;
+                float x[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) x[j] = __uint_as_float(v[j]);
+                if (g.epi == EPI_F32) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) g.out_f32[(size_t)row * g.ldo + n + j] = x[j];
+                } else if (g.epi == EPI_BIAS_F32) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) g.out_f32[(size_t)row * g.ldo + n + j] = x[j] + g.bias[n + j];
+                } else if (g.epi == EPI_BIAS_GELU) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const float z = x[j] + g.bias[n + j];
+                        g.z_save[(size_t)row * g.ldz + n + j] = z;
+                        g.out_bf16[(size_t)row * g.ldo + n + j] = __float2bfloat16_rn(gelu_f(z));
+                    }
+                } else if (g.epi == EPI_DGELU) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const float z = g.z_in[(size_t)row * g.ldz + n + j];
+                        g.out_bf16[(size_t)row * g.ldo + n + j] = __float2bfloat16_rn(x[j] * gelu_grad_f(z));
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        g.out_bf16[(size_t)row * g.ldo + n + j] = __float2bfloat16_rn(x[j] + g.bias[n + j]);
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
+
+}  // namespace uc

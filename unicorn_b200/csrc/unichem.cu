@@ -15,6 +15,7 @@
 #include "props_kernel.cuh"
 #include "update_kernel.cuh"
 #include "integrate_kernel.cuh"
+#include "mlp_gemm.cuh"
 
 using namespace uc;
 
@@ -1066,6 +1067,59 @@ extern "C" int uc_integrate_counts(uc_ctx *ctx, int *nsub, int *passes)
         CK(cudaMemcpyAsync(passes, ctx->cpasses, (size_t)ctx->n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return check_status(ctx);
+}
+
+// ------------------------------------------------------------------ tensor-core GEMM
+
+// Launch C = A * B^T on the stream (see mlp_gemm.cuh for the shapes it takes).
+static cudaError_t launch_gemm(const GemmArgs &g, cudaStream_t st)
+{
+    static thread_local int attr_done = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (attr_done != dev) {
+        cudaError_t e = cudaFuncSetAttribute(gemm_bf16_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)GEMM_SMEM_LAUNCH);
+        if (e != cudaSuccess) return e;
+        attr_done = dev;
+    }
+    dim3 grid((g.M + GM - 1) / GM, (g.N + GN_MAX - 1) / GN_MAX);
+    gemm_bf16_tc_kernel<<<grid, GEMM_THREADS, GEMM_SMEM_LAUNCH, st>>>(g);
+    return cudaGetLastError();
+}
+
+static bool gemm_shape_ok(int M, int N, int K, int lda, int ldb)
+{
+    return M > 0 && N > 0 && K > 0 && N % 16 == 0 && K % GK == 0 && lda % 8 == 0 && ldb % 8 == 0 && lda >= K &&
+           ldb >= K;
+}
+
+extern "C" int uc_gemm_bf16(int device, int M, int N, int K, const uint16_t *a, const uint16_t *b, float *c)
+{
+    if (!a || !b || !c || !gemm_shape_ok(M, N, K, K, K)) return UC_E_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return UC_E_CUDA;
+    __nv_bfloat16 *dA = nullptr, *dB = nullptr;
+    float *dC = nullptr;
+    int *dst = nullptr, st = 0, rc = UC_OK;
+    if (cudaMalloc((void **)&dA, (size_t)M * K * 2) != cudaSuccess || cudaMalloc((void **)&dB, (size_t)N * K * 2) != cudaSuccess ||
+        cudaMalloc((void **)&dC, (size_t)M * N * 4) != cudaSuccess || cudaMalloc((void **)&dst, sizeof(int)) != cudaSuccess)
+        rc = UC_E_NOMEM;
+    if (rc == UC_OK) {
+        cudaMemcpy(dA, a, (size_t)M * K * 2, cudaMemcpyHostToDevice);
+        cudaMemcpy(dB, b, (size_t)N * K * 2, cudaMemcpyHostToDevice);
+        cudaMemset(dst, 0, sizeof(int));
+        GemmArgs g{};
+        g.A = dA; g.B = dB; g.lda = K; g.ldb = K; g.M = M; g.N = N; g.K = K;
+        g.epi = EPI_F32; g.out_f32 = dC; g.ldo = N; g.status = dst;
+        if (launch_gemm(g, 0) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) rc = UC_E_CUDA;
+        if (rc == UC_OK) {
+            cudaMemcpy(c, dC, (size_t)M * N * 4, cudaMemcpyDeviceToHost);
+            cudaMemcpy(&st, dst, sizeof(int), cudaMemcpyDeviceToHost);
+            if (st == ST_MMA_TIMEOUT) rc = UC_E_TIMEOUT;
+        }
+    }
+    cudaFree(dA); cudaFree(dB); cudaFree(dC); cudaFree(dst);
+    return rc;
 }
 
 // ------------------------------------------------------------------ no-allocation update
