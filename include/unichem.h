@@ -221,6 +221,39 @@ int uc_integrate_counts(uc_ctx *ctx, int *nsub, int *passes);
 int uc_gemm_bf16(int device, int M, int N, int K, const uint16_t *a, const uint16_t *b, float *c);
 
 /* ---------------------------------------------------------------------------
+ * Learned surrogate of omega (no reference counterpart: the reference always
+ * evaluates the mechanism). A 54 -> 256 x 4 (GELU) -> 52 network with BF16
+ * weights and FP32 accumulation; inputs T, ln p and ln max(Y_k, 1e-12) scaled
+ * by uc_mlp_set_norm, outputs asinh(QDSP_k / s_k) scaled likewise. Trained
+ * with Adam on states whose targets the exact FP64 kernel computes, run with
+ * a per-tile fallback to that kernel (uc_mlp_omega). All matrix products run
+ * on the tensor cores (uc_gemm_bf16's kernel).
+ */
+typedef struct uc_mlp uc_mlp;
+/* capacity: rows of the training set kept on the device (64 features + 64 targets each). */
+int uc_mlp_create(int device, unsigned long long seed, long capacity, uc_mlp **out);
+int uc_mlp_nparams(const uc_mlp *mlp);
+/* Flat FP32 parameters, per layer W[out][in] then b[out] (layers 64->256, 3 x 256->256,
+ * 256->64; padded rows/columns are zero): get (if not NULL), then set (if not NULL). */
+int uc_mlp_params(uc_mlp *mlp, float *get, const float *set);
+/* Feature means, scales and training hull [54]; target means, scales and s_k [52]. */
+int uc_mlp_set_norm(uc_mlp *mlp, const float *feat_mu, const float *feat_sd, const float *hull_lo,
+                    const float *hull_hi, const float *tgt_mu, const float *tgt_sd, const float *tgt_scale);
+/* Append the context's cells (fields and uc_set_pressure pressures) with their exact omega. */
+int uc_mlp_add_data(uc_mlp *mlp, uc_ctx *ctx);
+/* Adam (beta 0.9/0.999, eps 1e-8) over `steps` batches; loss[steps] (may be NULL). batch % 64 == 0. */
+int uc_mlp_train(uc_mlp *mlp, int steps, int batch, float lr, unsigned long long seed, float *loss);
+/* One forward+backward pass on given rows (M % 64 == 0): x [M][64] BF16 bits, t [M][64];
+ * grad [nparams] and loss receive the mean-squared-error gradient and value. */
+int uc_mlp_grad(uc_mlp *mlp, int M, const uint16_t *x, const float *t, float *grad, float *loss);
+/* Omega of the context's state (its QDSP, as uc_omega leaves it) from the surrogate with
+ * per-tile fallback to the exact FP64 kernel; stats[3]: fraction of tiles recomputed,
+ * fraction of cells outside the training hull, median sampled residual. */
+int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats);
+const char *uc_mlp_last_error(const uc_mlp *mlp);
+void uc_mlp_destroy(uc_mlp *mlp);
+
+/* ---------------------------------------------------------------------------
  * Species update on caller-owned device arrays, with no device allocation.
  *
  * This entry point has no counterpart in the reference; it exists for callers

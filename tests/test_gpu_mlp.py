@@ -59,3 +59,141 @@ def test_gemm_rejects_bad_shapes(lib):
     F = c.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
     assert lib.uc_gemm_bf16(0, 64, 20, 64, P(a), P(a), F) == -1      # N not a multiple of 16
     assert lib.uc_gemm_bf16(0, 64, 16, 40, P(a), P(a), F) == -1      # K not a multiple of 64
+
+
+# ---------------------------------------------------------------- the network
+
+def _bits_of(x):
+    return to_bf16_bits(x)
+
+
+def test_gradients_match_cpu_oracle(lib):
+    """One forward+backward pass on the tensor cores against oracle/mlp_oracle.py.
+    The device sums in FP32 where the oracle sums exactly, so a hidden value
+    close to a BF16 rounding boundary can round the other way; per layer the
+    gradients agree to 1e-2 in relative Frobenius norm (cosine > 0.9999)."""
+    from oracle import mlp_oracle as mo
+    from unicorn_b200.surrogate import Surrogate
+    rng = np.random.default_rng(3)
+    M = 512
+    x = np.zeros((M, 64), dtype=np.float32)
+    x[:, :54] = rng.standard_normal((M, 54))
+    xb = _bits_of(x)
+    t = np.zeros((M, 64), dtype=np.float32)
+    t[:, :52] = rng.standard_normal((M, 52))
+    with Surrogate(capacity=0, seed=5) as s:
+        w = s.params()
+        g, loss = s.grad(xb, t)
+    loss_o, g_o = mo.forward_backward(w, from_bf16_bits(xb).astype(np.float64), t.astype(np.float64))
+    assert abs(loss - loss_o) <= 1e-4 * loss_o
+    off = 0
+    for i, o in zip(mo.IN, mo.OUT):
+        for size in (o * i, o):
+            a, b = g[off:off + size].astype(np.float64), g_o[off:off + size]
+            off += size
+            nb = np.linalg.norm(b)
+            if nb == 0:
+                assert np.linalg.norm(a) == 0
+                continue
+            assert np.linalg.norm(a - b) <= 1e-2 * nb
+            assert a @ b / (np.linalg.norm(a) * nb) > 0.9999
+
+
+@pytest.fixture(scope="module")
+def trained(lib):
+    """A network trained on 65,536 states of the batched-integration distribution."""
+    from unicorn_b200 import unichem
+    from unicorn_b200.fields import batch_cells, nondimensional
+    from unicorn_b200.surrogate import Surrogate, raw_features
+    n = 65536
+    f = batch_cells(n, seed=21)
+    u = unichem.UniChem(n)
+    tk, rho = nondimensional(f, u.scales, u.wm)
+    pref = u.scales["PBACK"] * u.scales["PSTR"]
+    u.upload(tk, rho, f.y)
+    u.set_pressure(f.p / u.scales["PSTR"])
+    q = u.omega().qdsp
+    norm = Surrogate.norm_from_sample(raw_features(f.T, f.p / pref, f.y), q)
+    s = Surrogate(capacity=n, seed=1)
+    s.set_norm(**norm)
+    s.add_data(u)
+    loss = s.train(steps=600, batch=4096, lr=1e-3, seed=2)
+    u.close()
+    yield s, loss, norm
+    s.close()
+
+
+def test_training_reduces_the_loss(trained):
+    s, loss, _ = trained
+    assert np.isfinite(loss).all()
+    assert loss[-50:].mean() < 0.25 * loss[:10].mean()
+
+
+def _field(n, seed):
+    from unicorn_b200 import unichem
+    from unicorn_b200.fields import batch_cells, nondimensional
+    f = batch_cells(n, seed=seed)
+    u = unichem.UniChem(n)
+    tk, rho = nondimensional(f, u.scales, u.wm)
+    u.upload(tk, rho, f.y)
+    u.set_pressure(f.p / u.scales["PSTR"])
+    return f, u
+
+
+def qdsp_of(u):
+    out = {"qdsp": np.empty((52, u.n))}
+    u.download_outputs(out)
+    return out["qdsp"]
+
+
+def _err(q, e, y):
+    """per cell: max over species with Y > 1e-8 of |q - e| / max(|e|, 1e-6 max|e|)"""
+    wmax = np.abs(e).max(axis=0)
+    r = np.abs(q - e) / np.maximum(np.abs(e), 1e-6 * wmax + 1e-300)
+    r[y <= 1e-8] = 0.0
+    return r.max(axis=0)
+
+
+def test_trained_network_gains_over_untrained(trained):
+    """On a fresh field (no fallback) the trained network's omega error is far below an untrained one's."""
+    from unicorn_b200.surrogate import Surrogate
+    s, _, norm = trained
+    f, u = _field(8192, seed=99)
+    exact = u.omega().qdsp.copy()
+    s.omega(u, tol=1e300)
+    q_tr = qdsp_of(u)
+    with Surrogate(capacity=0, seed=7) as s0:
+        s0.set_norm(**norm)
+        s0.omega(u, tol=1e300)
+        q_un = qdsp_of(u)
+    e_tr, e_un = _err(q_tr, exact, f.y), _err(q_un, exact, f.y)
+    assert np.median(e_tr) < 0.2 * np.median(e_un)
+    u.close()
+
+
+def test_fallback_is_the_exact_kernel(trained):
+    """tol = 0: every tile goes back to the FP64 kernel and the result is uc_omega's, bit for bit."""
+    s, _, _ = trained
+    f, u = _field(4000, seed=5)
+    exact = u.omega().qdsp.copy()
+    st = s.omega(u, tol=0.0)
+    assert st["tiles_exact"] == 1.0
+    assert np.array_equal(qdsp_of(u), exact)
+    u.close()
+
+
+def test_cells_outside_the_hull_fall_back(trained):
+    s, _, norm = trained
+    f, u = _field(4096, seed=6)
+    tk, rho, y, _, _ = u.download()
+    hot = np.arange(0, 4096, 512)                 # one cell in every 16th tile, far above the training range
+    tk[hot] = 4000.0 / u.scales["TSTR"]
+    u.upload(tk, rho, y)
+    exact = u.omega().qdsp.copy()
+    st = s.omega(u, tol=1e300)
+    assert st["cells_outside_hull"] >= len(hot) / 4096
+    q = qdsp_of(u)
+    for c in hot:
+        t0 = (c // 32) * 32
+        assert np.array_equal(q[:, t0:t0 + 32], exact[:, t0:t0 + 32])
+    u.close()

@@ -37,7 +37,7 @@ constexpr size_t GEMM_SMEM_LAUNCH = 100 * 1024;
 
 enum GemmEpi : int {
     EPI_F32 = 0,        // C as FP32 (out_f32, ldo)
-    EPI_BIAS_GELU = 1,  // z = C + bias -> z_save (FP32), gelu(z) -> out_bf16
+    EPI_BIAS_GELU = 1,  // z = C + bias -> z_save (FP32, if given), gelu(z) -> out_bf16
     EPI_BIAS_F32 = 2,   // C + bias -> out_f32
     EPI_DGELU = 3,      // C * gelu'(z_in) -> out_bf16 (gradient w.r.t. a hidden pre-activation)
     EPI_BIAS_BF16 = 4,  // C + bias -> out_bf16 (no activation)
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(GEMM_THREADS) gemm_bf16_tc_kernel(const GemmAr
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
                         const float z = x[j] + g.bias[n + j];
-                        g.z_save[(size_t)row * g.ldz + n + j] = z;
+                        if (g.z_save) g.z_save[(size_t)row * g.ldz + n + j] = z;
                         g.out_bf16[(size_t)row * g.ldo + n + j] = __float2bfloat16_rn(gelu_f(z));
                     }
                 } else if (g.epi == EPI_DGELU) {

@@ -16,6 +16,7 @@
 #include "update_kernel.cuh"
 #include "integrate_kernel.cuh"
 #include "mlp_gemm.cuh"
+#include "mlp.cuh"
 
 using namespace uc;
 
@@ -25,6 +26,7 @@ struct uc_ctx {
     int device = 0, n = 0, npad = 0, ntile = 0, nsm = 0;
     cudaStream_t stream = nullptr;
     uc_scales sc{};
+    uc_inputs inputs{};               // the input-card values of uc_init
     DevParams *hP = nullptr;          // host copy
     DevParams *dP = nullptr;
     PairTab *dTab = nullptr;
@@ -415,6 +417,7 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
         e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "stream: %s", cudaGetErrorString(e)); break; }
         ctx->n = ncell;
+        ctx->inputs = *in;
         ctx->ntile = (ncell + TILE - 1) / TILE;
         ctx->npad = ctx->ntile * TILE;
         ctx->hP = new (std::nothrow) DevParams();
@@ -1120,6 +1123,518 @@ extern "C" int uc_gemm_bf16(int device, int M, int N, int K, const uint16_t *a, 
     }
     cudaFree(dA); cudaFree(dB); cudaFree(dC); cudaFree(dst);
     return rc;
+}
+
+// ------------------------------------------------------------------ learned surrogate
+
+struct uc_mlp {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    MlpNorm hnorm{};
+    MlpNorm *dnorm = nullptr;
+    bool have_norm = false;
+    int in[MLP_LAYERS] = {MLP_IN, MLP_H, MLP_H, MLP_H, MLP_H};
+    int out[MLP_LAYERS] = {MLP_H, MLP_H, MLP_H, MLP_H, MLP_OUT};
+    int woff[MLP_LAYERS], boff[MLP_LAYERS], bfoff[MLP_LAYERS];
+    int np = 0, nw = 0;
+    float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+    __nv_bfloat16 *wb = nullptr, *wbt = nullptr;
+    // data set
+    __nv_bfloat16 *Xall = nullptr;
+    float *Tall = nullptr;
+    long ndata = 0, cap = 0;
+    // training buffers
+    int bcap = 0;
+    __nv_bfloat16 *H[MLP_LAYERS] = {}, *G[MLP_LAYERS] = {}, *Ht = nullptr, *Gt = nullptr;
+    float *Z[MLP_LAYERS - 1] = {}, *Out = nullptr, *T = nullptr;
+    double *partial = nullptr;
+    int *d_iter = nullptr, *d_t = nullptr, *idx = nullptr;
+    long idx_cap = 0;
+    float *loss_hist = nullptr;
+    int loss_cap = 0;
+    cudaGraphExec_t train_exec = nullptr;
+    cudaGraph_t train_graph = nullptr;
+    // inference buffers
+    long icap = 0;
+    __nv_bfloat16 *IX = nullptr, *IH0 = nullptr, *IH1 = nullptr;
+    float *IOut = nullptr;
+    int *outside = nullptr, *tflag = nullptr, *tlist = nullptr, *tcount = nullptr;
+    double *tresid = nullptr;
+    uc_ctx *sample = nullptr;      // compact field of the sampled cells
+    int *status = nullptr;
+    char err[256] = {0};
+};
+
+static int mlp_err(uc_mlp *m, int code, const char *msg)
+{
+    if (m) snprintf(m->err, sizeof(m->err), "%s", msg);
+    return code;
+}
+
+#define MCK(call)                                                                             \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return mlp_err(mlp, UC_E_CUDA, cudaGetErrorString(e_));        \
+    } while (0)
+
+template <typename T>
+static int mlp_alloc(uc_mlp *mlp, T **p, size_t count)
+{
+    if (*p) return UC_OK;
+    if (cudaMalloc((void **)p, count * sizeof(T)) != cudaSuccess) {
+        *p = nullptr;
+        return mlp_err(mlp, UC_E_NOMEM, "device allocation for the surrogate failed");
+    }
+    return UC_OK;
+}
+
+static uint64_t splitmix(uint64_t &s)
+{
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+extern "C" int uc_mlp_create(int device, unsigned long long seed, long capacity, uc_mlp **out)
+{
+    if (!out || capacity < 0) return UC_E_ARG;
+    *out = nullptr;
+    uc_mlp *mlp = new (std::nothrow) uc_mlp();
+    if (!mlp) return UC_E_NOMEM;
+    mlp->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&mlp->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete mlp;
+        return UC_E_CUDA;
+    }
+    int off = 0, bo = 0;
+    for (int l = 0; l < MLP_LAYERS; ++l) {
+        mlp->woff[l] = off;
+        off += mlp->out[l] * mlp->in[l];
+        mlp->boff[l] = off;
+        off += mlp->out[l];
+        mlp->bfoff[l] = bo;
+        bo += mlp->out[l] * mlp->in[l];
+    }
+    mlp->np = off;
+    mlp->nw = bo;
+    // initial weights: uniform in +-1/sqrt(fan_in) (fan_in of the first layer: the 54 real
+    // features), zero for the padded rows and columns
+    std::vector<float> hw(mlp->np, 0.0f);
+    uint64_t st = seed;
+    for (int l = 0; l < MLP_LAYERS; ++l) {
+        const int fan = l == 0 ? MLP_NF : mlp->in[l];
+        const float bound = 1.0f / sqrtf((float)fan);
+        const int rows = l == MLP_LAYERS - 1 ? MLP_NO : mlp->out[l];
+        const int cols = l == 0 ? MLP_NF : mlp->in[l];
+        for (int o = 0; o < rows; ++o) {
+            for (int i = 0; i < cols; ++i) {
+                const double u = (double)(splitmix(st) >> 11) * (1.0 / 9007199254740992.0);
+                hw[mlp->woff[l] + o * mlp->in[l] + i] = (float)((2.0 * u - 1.0) * bound);
+            }
+            const double u = (double)(splitmix(st) >> 11) * (1.0 / 9007199254740992.0);
+            hw[mlp->boff[l] + o] = (float)((2.0 * u - 1.0) * bound);
+        }
+    }
+    int rc = UC_OK;
+    if ((rc = mlp_alloc(mlp, &mlp->w, mlp->np)) || (rc = mlp_alloc(mlp, &mlp->g, mlp->np)) ||
+        (rc = mlp_alloc(mlp, &mlp->m, mlp->np)) || (rc = mlp_alloc(mlp, &mlp->v, mlp->np)) ||
+        (rc = mlp_alloc(mlp, &mlp->wb, mlp->nw)) || (rc = mlp_alloc(mlp, &mlp->wbt, mlp->nw)) ||
+        (rc = mlp_alloc(mlp, &mlp->dnorm, 1)) || (rc = mlp_alloc(mlp, &mlp->status, 1)) ||
+        (rc = mlp_alloc(mlp, &mlp->d_iter, 1)) || (rc = mlp_alloc(mlp, &mlp->d_t, 1))) {
+        uc_mlp_destroy(mlp);
+        return rc;
+    }
+    if (capacity > 0 && ((rc = mlp_alloc(mlp, &mlp->Xall, (size_t)capacity * MLP_IN)) ||
+                         (rc = mlp_alloc(mlp, &mlp->Tall, (size_t)capacity * MLP_OUT)))) {
+        uc_mlp_destroy(mlp);
+        return rc;
+    }
+    mlp->cap = capacity;
+    cudaMemcpy(mlp->w, hw.data(), mlp->np * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemset(mlp->m, 0, mlp->np * sizeof(float));
+    cudaMemset(mlp->v, 0, mlp->np * sizeof(float));
+    cudaMemset(mlp->g, 0, mlp->np * sizeof(float));
+    cudaMemset(mlp->status, 0, sizeof(int));
+    cudaMemset(mlp->d_iter, 0, sizeof(int));
+    cudaMemset(mlp->d_t, 0, sizeof(int));
+    *out = mlp;
+    return uc_mlp_params(mlp, nullptr, hw.data());   // also writes the BF16 copies
+}
+
+extern "C" int uc_mlp_nparams(const uc_mlp *mlp) { return mlp ? mlp->np : 0; }
+
+// get (if get != NULL) then set (if set != NULL) the flat FP32 parameter vector:
+// for each layer W [out][in] then b [out]; set also rewrites the BF16 copies
+extern "C" int uc_mlp_params(uc_mlp *mlp, float *get, const float *set)
+{
+    if (!mlp) return UC_E_ARG;
+    MCK(cudaSetDevice(mlp->device));
+    MCK(cudaStreamSynchronize(mlp->stream));
+    if (get) MCK(cudaMemcpy(get, mlp->w, mlp->np * sizeof(float), cudaMemcpyDeviceToHost));
+    if (set) {
+        MCK(cudaMemcpy(mlp->w, set, mlp->np * sizeof(float), cudaMemcpyHostToDevice));
+        std::vector<__nv_bfloat16> b(mlp->nw), bt(mlp->nw);
+        for (int l = 0; l < MLP_LAYERS; ++l)
+            for (int o = 0; o < mlp->out[l]; ++o)
+                for (int i = 0; i < mlp->in[l]; ++i) {
+                    const __nv_bfloat16 x = __float2bfloat16_rn(set[mlp->woff[l] + o * mlp->in[l] + i]);
+                    b[mlp->bfoff[l] + o * mlp->in[l] + i] = x;
+                    bt[mlp->bfoff[l] + i * mlp->out[l] + o] = x;
+                }
+        MCK(cudaMemcpy(mlp->wb, b.data(), mlp->nw * 2, cudaMemcpyHostToDevice));
+        MCK(cudaMemcpy(mlp->wbt, bt.data(), mlp->nw * 2, cudaMemcpyHostToDevice));
+    }
+    return UC_OK;
+}
+
+extern "C" int uc_mlp_set_norm(uc_mlp *mlp, const float *feat_mu, const float *feat_sd, const float *hull_lo,
+                               const float *hull_hi, const float *tgt_mu, const float *tgt_sd, const float *tgt_scale)
+{
+    if (!mlp || !feat_mu || !feat_sd || !hull_lo || !hull_hi || !tgt_mu || !tgt_sd || !tgt_scale) return UC_E_ARG;
+    for (int f = 0; f < MLP_NF; ++f) {
+        if (!(feat_sd[f] > 0.0f)) return mlp_err(mlp, UC_E_ARG, "feature scales must be positive");
+        mlp->hnorm.feat_mu[f] = feat_mu[f];
+        mlp->hnorm.feat_sd[f] = feat_sd[f];
+        mlp->hnorm.hull_lo[f] = hull_lo[f];
+        mlp->hnorm.hull_hi[f] = hull_hi[f];
+    }
+    for (int k = 0; k < MLP_NO; ++k) {
+        if (!(tgt_sd[k] > 0.0f) || !(tgt_scale[k] > 0.0f)) return mlp_err(mlp, UC_E_ARG, "target scales must be positive");
+        mlp->hnorm.tgt_mu[k] = tgt_mu[k];
+        mlp->hnorm.tgt_sd[k] = tgt_sd[k];
+        mlp->hnorm.tgt_scale[k] = tgt_scale[k];
+    }
+    MCK(cudaSetDevice(mlp->device));
+    MCK(cudaMemcpy(mlp->dnorm, &mlp->hnorm, sizeof(MlpNorm), cudaMemcpyHostToDevice));
+    mlp->have_norm = true;
+    return UC_OK;
+}
+
+// Appends the context's cells to the training set: features of its fields and
+// the exact FP64 omega of that state (uc_omega) as targets.
+extern "C" int uc_mlp_add_data(uc_mlp *mlp, uc_ctx *ctx)
+{
+    if (!mlp || !ctx) return UC_E_ARG;
+    if (!mlp->have_norm) return mlp_err(mlp, UC_E_STATE, "uc_mlp_set_norm first");
+    if (!ctx->have_fields || !ctx->pnd) return mlp_err(mlp, UC_E_STATE, "the context needs fields and pressures");
+    if (ctx->device != mlp->device) return mlp_err(mlp, UC_E_ARG, "context and surrogate on different devices");
+    if (mlp->ndata + ctx->n > mlp->cap) return mlp_err(mlp, UC_E_ARG, "training set capacity exceeded");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(launch_chem(ctx, UC_FP64, false, true));
+    const int grid = ctx->nsm * 8;
+    mlp_features_kernel<<<grid, 256, 0, ctx->stream>>>(ctx->dP, mlp->dnorm, ctx->tk, ctx->pnd, ctx->y, ctx->npad, 0,
+                                                       ctx->n, mlp->Xall, (int)mlp->ndata, nullptr);
+    CK(cudaGetLastError());
+    mlp_targets_kernel<<<grid, 256, 0, ctx->stream>>>(mlp->dnorm, ctx->qdsp, ctx->npad, 0, ctx->n, mlp->Tall,
+                                                      (int)mlp->ndata);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    mlp->ndata += ctx->n;
+    return UC_OK;
+}
+
+static int mlp_gemm(uc_mlp *mlp, cudaStream_t st, const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *B, int ldb,
+                    int M, int N, int K, int epi, const float *bias, const float *z_in, float *z_save, int ldz,
+                    float *of, __nv_bfloat16 *ob, int ldo)
+{
+    GemmArgs g{};
+    g.A = A; g.B = B; g.lda = lda; g.ldb = ldb; g.M = M; g.N = N; g.K = K; g.epi = epi;
+    g.bias = bias; g.z_in = z_in; g.z_save = z_save; g.ldz = ldz; g.out_f32 = of; g.out_bf16 = ob; g.ldo = ldo;
+    g.status = mlp->status;
+    MCK(launch_gemm(g, st));
+    return UC_OK;
+}
+
+static void mlp_free_batch(uc_mlp *mlp)
+{
+    for (int l = 0; l < MLP_LAYERS; ++l) {
+        cudaFree(mlp->H[l]);
+        cudaFree(mlp->G[l]);
+        mlp->H[l] = mlp->G[l] = nullptr;
+        if (l < MLP_LAYERS - 1) { cudaFree(mlp->Z[l]); mlp->Z[l] = nullptr; }
+    }
+    void **bufs[] = {(void **)&mlp->Ht, (void **)&mlp->Gt, (void **)&mlp->Out, (void **)&mlp->T, (void **)&mlp->partial};
+    for (auto b : bufs) { cudaFree(*b); *b = nullptr; }
+    mlp->bcap = 0;
+}
+
+static int mlp_batch_buffers(uc_mlp *mlp, int B)
+{
+    if (B <= mlp->bcap) return UC_OK;
+    cudaStreamSynchronize(mlp->stream);
+    mlp_free_batch(mlp);
+    int rc;
+    for (int l = 0; l < MLP_LAYERS; ++l) {
+        if ((rc = mlp_alloc(mlp, &mlp->H[l], (size_t)B * mlp->in[l])) || (rc = mlp_alloc(mlp, &mlp->G[l], (size_t)B * mlp->out[l])))
+            return rc;
+        if (l < MLP_LAYERS - 1 && (rc = mlp_alloc(mlp, &mlp->Z[l], (size_t)B * MLP_H))) return rc;
+    }
+    if ((rc = mlp_alloc(mlp, &mlp->Ht, (size_t)B * MLP_H)) || (rc = mlp_alloc(mlp, &mlp->Gt, (size_t)B * MLP_H)) ||
+        (rc = mlp_alloc(mlp, &mlp->Out, (size_t)B * MLP_OUT)) || (rc = mlp_alloc(mlp, &mlp->T, (size_t)B * MLP_OUT)) ||
+        (rc = mlp_alloc(mlp, &mlp->partial, 1024)))
+        return rc;
+    mlp->bcap = B;
+    return UC_OK;
+}
+
+// forward and backward of one batch already in H[0] (features) and T (targets); gradients in g
+static int mlp_enqueue_fwd_bwd(uc_mlp *mlp, int B, float *loss_hist)
+{
+    cudaStream_t st = mlp->stream;
+    for (int l = 0; l < MLP_LAYERS; ++l) {
+        const bool last = l == MLP_LAYERS - 1;
+        RET_IF(mlp_gemm(mlp, st, mlp->H[l], mlp->in[l], mlp->wb + mlp->bfoff[l], mlp->in[l], B, mlp->out[l], mlp->in[l],
+                        last ? EPI_BIAS_F32 : EPI_BIAS_GELU, mlp->w + mlp->boff[l], nullptr, last ? nullptr : mlp->Z[l],
+                        MLP_H, last ? mlp->Out : nullptr, last ? nullptr : mlp->H[l + 1], last ? MLP_OUT : MLP_H));
+    }
+    const int lblk = 256;
+    mlp_loss_grad_kernel<<<lblk, 256, 0, st>>>(mlp->Out, mlp->T, B, mlp->G[MLP_LAYERS - 1], mlp->partial);
+    MCK(cudaGetLastError());
+    if (loss_hist) {
+        mlp_loss_final_kernel<<<1, 32, 0, st>>>(mlp->partial, lblk, B, mlp->d_iter, loss_hist);
+        MCK(cudaGetLastError());
+    }
+    for (int l = MLP_LAYERS - 1; l >= 0; --l) {
+        const int in = mlp->in[l], out = mlp->out[l];
+        dim3 tb(32, 8);
+        transpose_bf16_kernel<<<dim3((out + 31) / 32, (B + 31) / 32), tb, 0, st>>>(mlp->G[l], B, out, mlp->Gt);
+        transpose_bf16_kernel<<<dim3((in + 31) / 32, (B + 31) / 32), tb, 0, st>>>(mlp->H[l], B, in, mlp->Ht);
+        MCK(cudaGetLastError());
+        // dW[out][in] = G^T H over the batch
+        RET_IF(mlp_gemm(mlp, st, mlp->Gt, B, mlp->Ht, B, out, in, B, EPI_F32, nullptr, nullptr, nullptr, 0,
+                        mlp->g + mlp->woff[l], nullptr, in));
+        bias_grad_kernel<<<(out + 31) / 32, dim3(32, 8), 0, st>>>(mlp->G[l], B, out, mlp->g + mlp->boff[l]);
+        MCK(cudaGetLastError());
+        if (l > 0)   // gradient w.r.t. the previous pre-activation: (G W) * gelu'(z)
+            RET_IF(mlp_gemm(mlp, st, mlp->G[l], out, mlp->wbt + mlp->bfoff[l], out, B, in, out, EPI_DGELU, nullptr,
+                            mlp->Z[l - 1], nullptr, MLP_H, nullptr, mlp->G[l - 1], in));
+    }
+    return UC_OK;
+}
+
+static int mlp_enqueue_adam(uc_mlp *mlp, float lr)
+{
+    AdamArgs a{};
+    a.w = mlp->w; a.g = mlp->g; a.m = mlp->m; a.v = mlp->v; a.n = mlp->np;
+    a.lr = lr; a.b1 = 0.9f; a.b2 = 0.999f; a.eps = 1e-8f; a.step = mlp->d_t;
+    a.wb = mlp->wb; a.wbt = mlp->wbt;
+    for (int l = 0; l < MLP_LAYERS; ++l) {
+        a.woff[l] = mlp->woff[l]; a.wout[l] = mlp->out[l]; a.win[l] = mlp->in[l]; a.bfoff[l] = mlp->bfoff[l];
+    }
+    adam_kernel<<<592, 256, 0, mlp->stream>>>(a);
+    MCK(cudaGetLastError());
+    return UC_OK;
+}
+
+// Adam training (lr, beta 0.9/0.999, eps 1e-8) for `steps` batches of `batch`
+// rows drawn without replacement from the training set (reshuffled every
+// pass over it, generator seeded by `seed`). The whole step is one CUDA graph.
+// loss (host [steps], may be NULL) receives each batch's mean squared error.
+extern "C" int uc_mlp_train(uc_mlp *mlp, int steps, int batch, float lr, unsigned long long seed, float *loss)
+{
+    if (!mlp || steps <= 0 || batch <= 0 || batch % GK != 0 || !(lr > 0.0f)) return UC_E_ARG;
+    if (mlp->ndata < batch) return mlp_err(mlp, UC_E_STATE, "training set smaller than one batch");
+    MCK(cudaSetDevice(mlp->device));
+    RET_IF(mlp_batch_buffers(mlp, batch));
+    // index list: consecutive permutations of the data set
+    const long need = (long)steps * batch;
+    if (need > mlp->idx_cap) {
+        if (mlp->idx) cudaFree(mlp->idx);
+        mlp->idx = nullptr;
+        RET_IF(mlp_alloc(mlp, &mlp->idx, (size_t)need));
+        mlp->idx_cap = need;
+    }
+    if (steps > mlp->loss_cap) {
+        if (mlp->loss_hist) cudaFree(mlp->loss_hist);
+        mlp->loss_hist = nullptr;
+        RET_IF(mlp_alloc(mlp, &mlp->loss_hist, (size_t)steps));
+        mlp->loss_cap = steps;
+    }
+    {
+        std::vector<int> idx((size_t)need), perm((size_t)mlp->ndata);
+        uint64_t st = seed;
+        long pos = mlp->ndata;
+        for (long i = 0; i < need; ++i) {
+            if (pos == mlp->ndata) {
+                for (long j = 0; j < mlp->ndata; ++j) perm[j] = (int)j;
+                for (long j = mlp->ndata - 1; j > 0; --j) std::swap(perm[j], perm[splitmix(st) % (uint64_t)(j + 1)]);
+                pos = 0;
+            }
+            idx[i] = perm[pos++];
+        }
+        MCK(cudaMemcpy(mlp->idx, idx.data(), need * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    MCK(cudaMemsetAsync(mlp->d_iter, 0, sizeof(int), mlp->stream));
+    {   // captured afresh on every call: the buffers it names may have been reallocated
+        if (mlp->train_exec) { cudaGraphExecDestroy(mlp->train_exec); mlp->train_exec = nullptr; }
+        if (mlp->train_graph) { cudaGraphDestroy(mlp->train_graph); mlp->train_graph = nullptr; }
+        MCK(cudaStreamBeginCapture(mlp->stream, cudaStreamCaptureModeThreadLocal));
+        mlp_gather_kernel<<<256, 256, 0, mlp->stream>>>(mlp->Xall, mlp->Tall, mlp->idx, mlp->d_iter, batch, mlp->H[0], mlp->T);
+        int rc = cudaGetLastError() == cudaSuccess ? UC_OK : mlp_err(mlp, UC_E_CUDA, "gather launch");
+        if (rc == UC_OK) rc = mlp_enqueue_fwd_bwd(mlp, batch, mlp->loss_hist);
+        if (rc == UC_OK) rc = mlp_enqueue_adam(mlp, lr);
+        if (rc == UC_OK) {
+            step_incr_kernel<<<1, 32, 0, mlp->stream>>>(mlp->d_iter);
+            step_incr_kernel<<<1, 32, 0, mlp->stream>>>(mlp->d_t);
+        }
+        cudaGraph_t gph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(mlp->stream, &gph);
+        if (rc != UC_OK) { if (gph) cudaGraphDestroy(gph); return rc; }
+        if (e != cudaSuccess) return mlp_err(mlp, UC_E_CUDA, cudaGetErrorString(e));
+        if (cudaGraphInstantiate(&mlp->train_exec, gph, 0) != cudaSuccess) {
+            cudaGraphDestroy(gph);
+            return mlp_err(mlp, UC_E_CUDA, "train graph instantiate");
+        }
+        mlp->train_graph = gph;
+    }
+    for (int s = 0; s < steps; ++s) MCK(cudaGraphLaunch(mlp->train_exec, mlp->stream));
+    MCK(cudaStreamSynchronize(mlp->stream));
+    if (loss) MCK(cudaMemcpy(loss, mlp->loss_hist, steps * sizeof(float), cudaMemcpyDeviceToHost));
+    int st = 0;
+    MCK(cudaMemcpy(&st, mlp->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st == ST_MMA_TIMEOUT) return mlp_err(mlp, UC_E_TIMEOUT, "a tensor-core wait timed out");
+    return UC_OK;
+}
+
+// One forward and backward pass on given rows (no update): x [M][64] BF16 bit
+// patterns (features), t [M][64] targets; grad (host [nparams]) receives the
+// gradient of the mean squared error, loss its value. M a multiple of 64.
+extern "C" int uc_mlp_grad(uc_mlp *mlp, int M, const uint16_t *x, const float *t, float *grad, float *loss)
+{
+    if (!mlp || M <= 0 || M % GK != 0 || !x || !t) return UC_E_ARG;
+    MCK(cudaSetDevice(mlp->device));
+    RET_IF(mlp_batch_buffers(mlp, M));
+    MCK(cudaMemcpyAsync(mlp->H[0], x, (size_t)M * MLP_IN * 2, cudaMemcpyHostToDevice, mlp->stream));
+    MCK(cudaMemcpyAsync(mlp->T, t, (size_t)M * MLP_OUT * 4, cudaMemcpyHostToDevice, mlp->stream));
+    if (!mlp->loss_hist) {
+        RET_IF(mlp_alloc(mlp, &mlp->loss_hist, 1));
+        mlp->loss_cap = 1;
+    }
+    MCK(cudaMemsetAsync(mlp->d_iter, 0, sizeof(int), mlp->stream));
+    RET_IF(mlp_enqueue_fwd_bwd(mlp, M, mlp->loss_hist));
+    MCK(cudaStreamSynchronize(mlp->stream));
+    if (grad) MCK(cudaMemcpy(grad, mlp->g, mlp->np * sizeof(float), cudaMemcpyDeviceToHost));
+    if (loss) MCK(cudaMemcpy(loss, mlp->loss_hist, sizeof(float), cudaMemcpyDeviceToHost));
+    return UC_OK;
+}
+
+// Omega of the context's state from the surrogate, with fallback to the exact
+// FP64 kernel per 32-cell tile: a tile is recomputed exactly if one of its
+// cells lies outside the training hull, or if the surrogate's relative error
+// on one sampled cell of the tile exceeds tol (species with Y > 1e-8).
+// The result is the context's QDSP (as uc_omega leaves it; download with
+// uc_download_outputs). stats (host [3], may be NULL): fraction of tiles
+// recomputed, fraction of cells outside the hull, median sampled residual.
+extern "C" int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats)
+{
+    if (!mlp || !ctx || !(tol >= 0.0)) return UC_E_ARG;
+    if (!mlp->have_norm) return mlp_err(mlp, UC_E_STATE, "uc_mlp_set_norm first");
+    if (!ctx->have_fields || !ctx->pnd) return mlp_err(mlp, UC_E_STATE, "the context needs fields and pressures");
+    if (ctx->device != mlp->device) return mlp_err(mlp, UC_E_ARG, "context and surrogate on different devices");
+    CK(cudaSetDevice(ctx->device));
+    const int n = ctx->n, np = ctx->npad, nt = ctx->ntile;
+    int rc;
+    if (mlp->icap < np) {
+        if (mlp->icap) return mlp_err(mlp, UC_E_ARG, "a larger field than the first one used");
+        if ((rc = mlp_alloc(mlp, &mlp->IX, (size_t)np * MLP_IN)) || (rc = mlp_alloc(mlp, &mlp->IH0, (size_t)np * MLP_H)) ||
+            (rc = mlp_alloc(mlp, &mlp->IH1, (size_t)np * MLP_H)) || (rc = mlp_alloc(mlp, &mlp->IOut, (size_t)np * MLP_OUT)) ||
+            (rc = mlp_alloc(mlp, &mlp->outside, (size_t)np)) || (rc = mlp_alloc(mlp, &mlp->tflag, (size_t)nt)) ||
+            (rc = mlp_alloc(mlp, &mlp->tlist, (size_t)nt)) || (rc = mlp_alloc(mlp, &mlp->tcount, 1)) ||
+            (rc = mlp_alloc(mlp, &mlp->tresid, (size_t)nt)))
+            return rc;
+        mlp->icap = np;
+        if ((rc = uc_init(&ctx->inputs, nt, ctx->device, &mlp->sample)) != UC_OK)
+            return mlp_err(mlp, rc, "set-up of the sampled-cell field failed");
+    }
+    RET_IF(dalloc(ctx, &ctx->qdsp, (size_t)LSP * np));
+    cudaStream_t st = ctx->stream;
+    const int grid = ctx->nsm * 8;
+    // surrogate for every cell
+    mlp_features_kernel<<<grid, 256, 0, st>>>(ctx->dP, mlp->dnorm, ctx->tk, ctx->pnd, ctx->y, np, 0, np, mlp->IX, 0,
+                                              mlp->outside);
+    CK(cudaGetLastError());
+    __nv_bfloat16 *hin = mlp->IX, *hb[2] = {mlp->IH0, mlp->IH1};
+    for (int l = 0; l < MLP_LAYERS; ++l) {
+        const bool last = l == MLP_LAYERS - 1;
+        RET_IF(mlp_gemm(mlp, st, hin, mlp->in[l], mlp->wb + mlp->bfoff[l], mlp->in[l], np, mlp->out[l], mlp->in[l],
+                        last ? EPI_BIAS_F32 : EPI_BIAS_GELU, mlp->w + mlp->boff[l], nullptr, nullptr, 0,
+                        last ? mlp->IOut : nullptr, last ? nullptr : hb[l & 1], last ? MLP_OUT : MLP_H));
+        if (!last) hin = hb[l & 1];
+    }
+    mlp_decode_kernel<<<grid, 256, 0, st>>>(mlp->dnorm, mlp->IOut, np, ctx->qdsp, np, 0);
+    CK(cudaGetLastError());
+    // exact omega of one sampled cell per tile
+    uc_ctx *S = mlp->sample;
+    sample_gather_kernel<<<(S->npad + 255) / 256, 256, 0, st>>>(ctx->tk, ctx->rho, ctx->y, ctx->soot, np, n, nt, S->tk,
+                                                                 S->rho, S->y, S->soot, S->npad);
+    CK(cudaGetLastError());
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, st));
+    CK(cudaStreamWaitEvent(S->stream, ev, 0));
+    S->have_fields = true;
+    RET_IF(launch_chem(S, UC_FP64, false, true));
+    CK(cudaEventRecord(ev, S->stream));
+    CK(cudaStreamWaitEvent(st, ev, 0));
+    cudaEventDestroy(ev);
+    residual_flag_kernel<<<(nt + 255) / 256, 256, 0, st>>>(ctx->qdsp, ctx->y, np, n, nt, S->qdsp, S->npad, mlp->outside,
+                                                           tol, mlp->tflag, mlp->tresid);
+    CK(cudaGetLastError());
+    // exact FP64 omega for the flagged tiles
+    compact_tiles_kernel<<<1, 1024, 0, st>>>(mlp->tflag, nt, mlp->tlist, mlp->tcount);
+    CK(cudaGetLastError());
+    ChemArgs c{};
+    c.P = ctx->dP; c.tab = ctx->dTab;
+    c.tk = ctx->tk; c.rho = ctx->rho; c.y = ctx->y; c.stmf = ctx->soot; c.stnd = ctx->soot + np;
+    c.qdsp = ctx->qdsp;
+    c.n = n; c.npad = np; c.ntile = nt; c.status = ctx->status;
+    c.tile_list = mlp->tlist; c.tile_count = mlp->tcount;
+    int slot;
+    prof_begin(ctx, UC_K_CHEM, slot);
+    chem_fp64_kernel<<<std::min(nt, ctx->nsm), CHEM_THREADS, CHEM_SMEM, st>>>(c);
+    prof_end(ctx, slot);
+    CK(cudaGetLastError());
+    if (stats) {
+        int cnt = 0;
+        std::vector<int> outs(n);
+        std::vector<double> res(nt);
+        CK(cudaMemcpyAsync(&cnt, mlp->tcount, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(outs.data(), mlp->outside, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(res.data(), mlp->tresid, nt * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        long no = 0;
+        for (int v : outs) no += v;
+        std::nth_element(res.begin(), res.begin() + nt / 2, res.end());
+        stats[0] = (double)cnt / nt;
+        stats[1] = (double)no / n;
+        stats[2] = res[nt / 2];
+    }
+    int s2 = 0;
+    CK(cudaMemcpyAsync(&s2, mlp->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (s2 == ST_MMA_TIMEOUT) return set_err(ctx, UC_E_TIMEOUT, "a tensor-core wait timed out");
+    return UC_OK;
+}
+
+extern "C" const char *uc_mlp_last_error(const uc_mlp *mlp) { return mlp ? mlp->err : "null surrogate"; }
+
+extern "C" void uc_mlp_destroy(uc_mlp *mlp)
+{
+    if (!mlp) return;
+    cudaSetDevice(mlp->device);
+    if (mlp->stream) cudaStreamSynchronize(mlp->stream);
+    if (mlp->train_exec) cudaGraphExecDestroy(mlp->train_exec);
+    if (mlp->train_graph) cudaGraphDestroy(mlp->train_graph);
+    void *bufs[] = {mlp->dnorm, mlp->w, mlp->g, mlp->m, mlp->v, mlp->wb, mlp->wbt, mlp->Xall, mlp->Tall,
+                    mlp->d_iter, mlp->d_t, mlp->idx, mlp->loss_hist, mlp->IX, mlp->IH0, mlp->IH1, mlp->IOut,
+                    mlp->outside, mlp->tflag, mlp->tlist, mlp->tcount, mlp->tresid, mlp->status};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    mlp_free_batch(mlp);
+    if (mlp->sample) uc_destroy(mlp->sample);
+    if (mlp->stream) cudaStreamDestroy(mlp->stream);
+    delete mlp;
 }
 
 // ------------------------------------------------------------------ no-allocation update
