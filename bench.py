@@ -439,6 +439,218 @@ def main_c3(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- C4: learned surrogate
+C4_TRAIN, C4_FIELD = 4 << 20, 1 << 20
+MLP_FLOP_PER_CELL = 2 * (64 * 256 + 3 * 256 * 256 + 256 * 64)     # padded GEMM shapes, multiply-add = 2 flops
+
+
+def main_c4(args):
+    import torch
+    from unicorn_b200 import unichem
+    from unicorn_b200.fields import batch_cells, nondimensional
+    from unicorn_b200.surrogate import Surrogate, raw_features
+    ntrain = args.cells * 4 if args.cells else C4_TRAIN
+    nfield = args.cells or C4_FIELD
+    chunk = min(ntrain, 1 << 20)
+    steps = args.train_steps
+    # ---- training set: exact FP64 omega of C3-distribution states, in chunks
+    t0 = time.perf_counter()
+    s = Surrogate(capacity=ntrain, seed=1)
+    u = unichem.UniChem(chunk)
+    hull_lo, hull_hi, norm = None, None, None
+    for c in range(ntrain // chunk):
+        f = batch_cells(chunk, seed=100 + c)
+        tk, rho = nondimensional(f, u.scales, u.wm)
+        pref = u.scales["PBACK"] * u.scales["PSTR"]
+        u.upload(tk, rho, f.y)
+        u.set_pressure(f.p / u.scales["PSTR"])
+        feats = raw_features(f.T, f.p / pref, f.y)
+        if norm is None:
+            sub = np.arange(0, chunk, max(1, chunk // 65536))
+            q = u.omega().qdsp
+            norm = Surrogate.norm_from_sample(feats[:, sub], q[:, sub])
+            s.set_norm(**norm)
+        lo, hi = feats.min(axis=1), feats.max(axis=1)
+        hull_lo = lo if hull_lo is None else np.minimum(hull_lo, lo)
+        hull_hi = hi if hull_hi is None else np.maximum(hull_hi, hi)
+        s.add_data(u)
+    u.close()
+    norm.update(hull_lo=hull_lo, hull_hi=hull_hi)
+    s.set_norm(**norm)
+    t_data = time.perf_counter() - t0
+    # ---- training (device time of the whole run, graph per step)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = s.train(steps=steps, batch=8192, lr=1e-3, seed=3)
+    t_train = time.perf_counter() - t0
+    # ---- inference on a fresh field: exact FP64 omega vs surrogate + fallback
+    f = batch_cells(nfield, seed=7)
+    u = unichem.UniChem(nfield)
+    tk, rho = nondimensional(f, u.scales, u.wm)
+    u.upload(tk, rho, f.y)
+    u.set_pressure(f.p / u.scales["PSTR"])
+    view = unichem_view(u)
+    ext = torch.cuda.ExternalStream(view["stream"])
+    out = {"qdsp": np.empty((52, nfield))}
+
+    def timed(fn, reps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        for _ in range(reps):
+            r = fn()
+        e1.record(ext)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, r
+
+    ms_exact, _ = timed(lambda: u.omega(download=False), args.steps)
+    u.download_outputs(out)
+    exact = out["qdsp"].copy()
+    res = {}
+    with ClockSampler(0) as clk:
+        for tol in (1e-3, 1e-1, 1e300):
+            ms, _ = timed(lambda: s.omega(u, tol=tol, stats=False), args.steps)
+            st = s.omega(u, tol=tol)
+            u.download_outputs(out)
+            q = out["qdsp"]
+            wmax = np.abs(exact).max(axis=0)
+            r = np.abs(q - exact) / np.maximum(np.abs(exact), 1e-6 * wmax + 1e-300)
+            r[f.y <= 1e-8] = 0.0
+            err = r.max(axis=0)
+            res["tol=%g" % tol] = {"ms": round(ms, 3), "cell_updates_per_s": round(nfield / (ms / 1e3), 1),
+                                  "speedup_vs_fp64": round(ms_exact / ms, 3), "tiles_exact": round(st["tiles_exact"], 4),
+                                  "cells_outside_hull": round(st["cells_outside_hull"], 5),
+                                  "median_sampled_residual": st["median_residual"],
+                                  "err_vs_fp64_p50": float(np.median(err)), "err_vs_fp64_p99": float(np.quantile(err, 0.99)),
+                                  "frac_cells_err_le_1e-3": round(float((err <= 1e-3).mean()), 4)}
+    u.close()
+    s.close()
+    pure = res["tol=1e+300"]
+    tflops = MLP_FLOP_PER_CELL * nfield / (pure["ms"] / 1e3) / 1e12
+    line = {"metric": "omega cell-updates/s: learned surrogate + per-tile FP64 fallback at the stated error",
+            "value": res["tol=0.001"]["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["tol=0.001"]["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 network / f64 fallback", "data": "synthetic (seeded C3/C4 generators)",
+            "config": {"workload": f"C4: network 54-256x4-52 GELU, Adam lr 1e-3 batch 8192, {steps} steps on {ntrain} "
+                                   f"exact-FP64 states of the C3 distribution; inference on a fresh {nfield}-cell field "
+                                   "with fallback per 32-cell tile (training hull, one sampled residual per tile)",
+                       "fp64_omega_ms": round(ms_exact, 3),
+                       "fp64_omega_cell_updates_per_s": round(nfield / (ms_exact / 1e3), 1),
+                       "by_tolerance": res, "train_s": round(t_train, 2), "data_s": round(t_data, 2),
+                       "train_samples_per_s": round(steps * 8192 / t_train, 1),
+                       "loss_first": float(loss[:10].mean()), "loss_last": float(loss[-50:].mean())},
+            "e2e": None, "gpu_launches": None, "clocks": clk.summary(),
+            "roofline": {"kernel": "surrogate forward (5 tensor-core GEMMs + features/decode)", "bound": "tensor",
+                         "achieved": round(tflops, 2), "peak": 1693.5, "peak_source": "measured (bf16 burst)",
+                         "unit": "TFLOP/s", "frac": round(tflops / 1693.5, 4), "traffic": None,
+                         "flops_rule": f"{MLP_FLOP_PER_CELL} flop per cell (padded 64-256x4-64 layers) / forward time"}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- C5: in-loop sweeps
+def main_c5(args):
+    import torch
+    from unicorn_b200 import unichem
+    from unicorn_b200.fields import jet_field, nondimensional
+    from unicorn_b200.inloop import frozen_faces, omega_error
+    from unicorn_b200.surrogate import Surrogate, raw_features
+    f = jet_field(NZ, NR, fuel=FUEL, t_peak=TPEAK, seed=0)
+    n = f.n
+    checkpoints = sorted({c for c in (100, 500, 1000, args.sweeps) if c <= args.sweeps})
+    # ---- surrogate trained on four other seeded fields of the same generator
+    s = Surrogate(capacity=4 * n, seed=1)
+    u = unichem.UniChem(n)
+    pref = u.scales["PBACK"] * u.scales["PSTR"]
+    norm = None
+    for seed in (11, 12, 13, 14):
+        g = jet_field(NZ, NR, fuel=FUEL, t_peak=TPEAK, seed=seed)
+        tk, rho = nondimensional(g, u.scales, u.wm)
+        u.upload(tk, rho, g.y)
+        u.set_pressure(g.p / u.scales["PSTR"])
+        if norm is None:
+            norm = Surrogate.norm_from_sample(raw_features(g.T, g.p / pref, g.y), u.omega().qdsp)
+            s.set_norm(**norm)
+        s.add_data(u)
+    u.close()
+    loss = s.train(steps=args.train_steps, batch=8192, lr=1e-3, seed=3)
+    # ---- the in-loop runs
+    report = {}
+    timing = {}
+    ref_states = {}
+    probe = unichem.UniChem(n)
+    for name, prec in (("fp64", unichem.FP64), ("mixed", unichem.MIXED)):
+        u = unichem.UniChem(n)
+        tk, rho = nondimensional(f, u.scales, u.wm)
+        u.upload(tk, rho, f.y)
+        u.set_pressure(f.p / u.scales["PSTR"])
+        if name == "fp64":
+            vdf = u.props()[2]
+            _, _, yc, _, _ = u.download()
+            fs, fn = frozen_faces((NZ, NR), vdf, yc, DT)
+            u.upload(tk, rho, f.y)
+        u.hold_enthalpy()
+        view = unichem_view(u)
+        ext = torch.cuda.ExternalStream(view["stream"])
+        rep = {}
+        ms_total, passes = 0.0, []
+        for sw in range(1, args.sweeps + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            passes.append(u.sweep(DT, precision=prec, isor=ISOR, relx=RELX, tol=TOL, face_sum=fs, face_nbr=fn))
+            u.temperature_from_held()
+            e1.record(ext)
+            e1.synchronize()
+            ms_total += e0.elapsed_time(e1)
+            if sw in checkpoints:
+                tk1, rho1, y1, s1, _ = u.download()
+                T1 = tk1 * u.scales["TSTR"]
+                free = T1 < 5000.0 - 1e-6          # cells not held at the T clamp of solveh.f
+                entry = {"peak_T": round(float(T1.max()), 3), "peak_T_drift": round(float(T1.max() - f.T.max()), 3),
+                         "peak_T_below_clamp": round(float(T1[free].max()), 3), "mean_T": round(float(T1.mean()), 3),
+                         "cells_at_5000K": int((~free).sum()),
+                         "sumY_drift_max": float(np.abs(y1.sum(0) + s1 - 1.0).max()),
+                         "mean_passes": round(float(np.mean(passes[-100:])), 2)}
+                if name == "fp64":
+                    ref_states[sw] = (T1.copy(), y1.copy())
+                else:
+                    Tr, yr = ref_states[sw]
+                    entry.update({"vs_fp64_max_dT": float(np.abs(T1 - Tr).max()), "vs_fp64_max_dY": float(np.abs(y1 - yr).max()),
+                                  "vs_fp64_p99_dT": float(np.quantile(np.abs(T1 - Tr), 0.99))})
+                # omega of this state: FP64 kernel, mixed kernel, surrogate (no fallback / with fallback at 1e-3)
+                probe.upload(tk1, rho1, y1, s1, None)
+                probe.set_pressure(f.p / u.scales["PSTR"])
+                ex = probe.omega(unichem.FP64).qdsp
+                mx = probe.omega(unichem.MIXED).qdsp
+                s.omega(probe, tol=float("inf"), stats=False)
+                out = {"qdsp": np.empty((52, n))}
+                probe.download_outputs(out)
+                e_mx, e_ml = omega_error(mx, ex, y1), omega_error(out["qdsp"], ex, y1)
+                fb = s.omega(probe, tol=1e-3)
+                entry.update({"omega_err_mixed_p50": float(np.median(e_mx)), "omega_err_mixed_p99": float(np.quantile(e_mx, 0.99)),
+                              "omega_mixed_frac_le_1e-3": round(float((e_mx <= 1e-3).mean()), 4),
+                              "omega_err_mlp_p50": float(np.median(e_ml)), "omega_err_mlp_p99": float(np.quantile(e_ml, 0.99)),
+                              "mlp_tiles_exact_at_1e-3": round(fb["tiles_exact"], 4)})
+                rep[f"sweep_{sw}"] = entry
+        timing[name] = {"ms_per_sweep": round(ms_total / args.sweeps, 3),
+                        "cell_updates_per_s": round(n * args.sweeps / (ms_total / 1e3), 1)}
+        report[name] = rep
+        u.close()
+    probe.close()
+    s.close()
+    line = {"metric": "in-loop heptane sweeps: peak-T drift, sum-Y drift and omega error at sweeps 100/500/1000",
+            "value": timing["fp64"]["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.sweeps, "warmup": 0,
+            "ms_per_step": timing["fp64"]["ms_per_sweep"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (and mixed)", "data": "synthetic (seeded C2 generator)",
+            "config": {"workload": f"C5: 601x301 heptane field, {args.sweeps} sweeps of dt=1e-5 s, transport frozen "
+                                   "(diffusion faces from the initial field), T from held enthalpy each sweep",
+                       "timing": timing, "report": report,
+                       "surrogate": {"train_steps": args.train_steps, "train_states": 4 * n,
+                                     "loss_first": float(loss[:10].mean()), "loss_last": float(loss[-50:].mean())}}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -449,11 +661,18 @@ def main():
     ap.add_argument("--cells", type=int, default=0, help="use only the first N cells (profiling runs)")
     ap.add_argument("--isor", type=int, default=ISOR, help="update passes cap (profiling runs)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
-                    help="c2: the species sweep of the 601x301 heptane field (headline); c3: batched stiff integration")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+                    help="c2: the species sweep of the 601x301 heptane field (headline); c3: batched stiff "
+                         "integration; c4: learned surrogate with fallback; c5: in-loop sweeps")
+    ap.add_argument("--sweeps", type=int, default=1000, help="c5: sweeps")
+    ap.add_argument("--train-steps", type=int, default=2000, help="c4: Adam steps")
     args = ap.parse_args()
     if args.workload == "c3":
         main_c3(args)
+    elif args.workload == "c4":
+        main_c4(args)
+    elif args.workload == "c5":
+        main_c5(args)
     elif args.impl == "reference":
         main_reference(args)
     else:

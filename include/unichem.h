@@ -204,6 +204,13 @@ typedef struct {
 } uc_integrate_opts;
 /* Cell pressures p/PSTR [n] (host); cells default to PBACK. */
 int uc_set_pressure(uc_ctx *ctx, const double *pnd);
+/* Record each cell's total enthalpy h(T, Y) (the polynomial of solveh.f:1186-1205 at the
+ * cell's T); uc_temperature_from_held then re-solves T from it for the current Y
+ * (the Newton of src/lib/solveh.f:1170-1234) and sets rho from the ideal gas at the
+ * cell's pressure (src/unicornd-mild-sd-5.f:1056-1062): the in-loop T update of a
+ * sweep with enthalpy transport frozen. */
+int uc_hold_enthalpy(uc_ctx *ctx);
+int uc_temperature_from_held(uc_ctx *ctx);
 int uc_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts *o);
 /* Times each kernel shape on the current state (restored after each trial)
  * and keeps the fastest for uc_integrate; uc_stat "int_warps", "int_sorted",
@@ -248,7 +255,8 @@ int uc_mlp_train(uc_mlp *mlp, int steps, int batch, float lr, unsigned long long
 int uc_mlp_grad(uc_mlp *mlp, int M, const uint16_t *x, const float *t, float *grad, float *loss);
 /* Omega of the context's state (its QDSP, as uc_omega leaves it) from the surrogate with
  * per-tile fallback to the exact FP64 kernel; stats[3]: fraction of tiles recomputed,
- * fraction of cells outside the training hull, median sampled residual. */
+ * fraction of cells outside the training hull, median sampled residual. tol = +infinity
+ * gives the network's output alone (no hull check, no fallback). */
 int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats);
 const char *uc_mlp_last_error(const uc_mlp *mlp);
 void uc_mlp_destroy(uc_mlp *mlp);

@@ -126,6 +126,30 @@ __global__ void nsub_kernel(const DevParams *Pp, const double *rho, const double
     }
 }
 
+// Total enthalpy of each cell of a field (held while the composition changes)
+__global__ void hold_enthalpy_kernel(const DevParams *Pp, const double *tk, const double *y, int npad, double *enth)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < npad; c += gridDim.x * blockDim.x)
+        enth[c] = enthalpy_total(*Pp, tk[c], y + c, npad);
+}
+
+// T from the held total enthalpy and the current Y (solveh.f:1186-1234), then rho
+// from the ideal gas at the cell pressure (main:1056-1062)
+__global__ void temperature_held_kernel(const DevParams *Pp, const double *enth, const double *y, const double *pnd,
+                                        int npad, double *tk, double *rho, int *status)
+{
+    const DevParams &P = *Pp;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < npad; c += gridDim.x * blockDim.x) {
+        bool conv;
+        const double t = temperature_at(P, tk[c], y + c, npad, enth[c], &conv);
+        if (!conv && status) atomicCAS(status, ST_OK, ST_NEWTON_NOCONV);
+        double rbar = 0.0;
+        for (int k = 0; k < LSP; ++k) rbar = rbar + y[(size_t)k * npad + c] / P.WM[k];
+        tk[c] = t;
+        rho[c] = pnd[c] / (P.BETA1 * t * rbar);
+    }
+}
+
 // ---- stable counting sort of positions by n_sub, largest first.
 // Chunk j of SORT_CHUNK cells is owned by CTA j; key = nsub_max - n_sub.
 constexpr int SORT_CHUNK = 4096;

@@ -43,7 +43,7 @@ struct uc_ctx {
     bool have_fields = false, have_rc = false;
     int upd_grid = 0;
     // batched integration
-    double *pnd = nullptr;
+    double *pnd = nullptr, *enth = nullptr;
     int *nsub = nullptr, *order = nullptr, *hist = nullptr, *next_tile = nullptr, *cpasses = nullptr;
     cudaGraph_t int_graph = nullptr;
     cudaGraphExec_t int_exec = nullptr;
@@ -315,6 +315,7 @@ static void free_ctx(uc_ctx *c)
         for (auto b : ibufs)
             if (*b) { cudaFree(*b); *b = nullptr; }
         if (c->pnd) cudaFree(c->pnd);
+        if (c->enth) cudaFree(c->enth);
         if (c->int_exec) cudaGraphExecDestroy(c->int_exec);
         if (c->int_graph) cudaGraphDestroy(c->int_graph);
     }
@@ -860,15 +861,20 @@ static int check_opts(uc_ctx *ctx, const uc_integrate_opts *o)
     return UC_OK;
 }
 
+static int ensure_pressure(uc_ctx *ctx)
+{
+    if (ctx->pnd) return UC_OK;
+    RET_IF(dalloc(ctx, &ctx->pnd, ctx->npad));
+    std::vector<double> pb(ctx->npad, ctx->sc.pback);
+    CK(cudaMemcpy(ctx->pnd, pb.data(), ctx->npad * sizeof(double), cudaMemcpyHostToDevice));
+    return UC_OK;
+}
+
 static int integrate_buffers(uc_ctx *ctx)
 {
     const size_t np = ctx->npad;
     const int nchunk = (ctx->n + SORT_CHUNK - 1) / SORT_CHUNK;
-    if (!ctx->pnd) {
-        RET_IF(dalloc(ctx, &ctx->pnd, np));
-        std::vector<double> pb(np, ctx->sc.pback);
-        CK(cudaMemcpy(ctx->pnd, pb.data(), np * sizeof(double), cudaMemcpyHostToDevice));
-    }
+    RET_IF(ensure_pressure(ctx));
     RET_IF(dalloc(ctx, &ctx->qdsp, (size_t)LSP * np));
     int **bufs[] = {&ctx->nsub, &ctx->order, &ctx->cpasses, &ctx->hist, &ctx->next_tile};
     const size_t counts[] = {np, np, np, (size_t)(SORT_MAXBIN + 1) * nchunk, 1};
@@ -889,6 +895,32 @@ extern "C" int uc_set_pressure(uc_ctx *ctx, const double *pnd)
     CK(cudaSetDevice(ctx->device));
     RET_IF(dalloc(ctx, &ctx->pnd, ctx->npad));
     RET_IF(upload_rows(ctx, ctx->pnd, pnd, 1));
+    return UC_OK;
+}
+
+extern "C" int uc_hold_enthalpy(uc_ctx *ctx)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "no fields uploaded");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(dalloc(ctx, &ctx->enth, ctx->npad));
+    hold_enthalpy_kernel<<<ctx->nsm * 4, 256, 0, ctx->stream>>>(ctx->dP, ctx->tk, ctx->y, ctx->npad, ctx->enth);
+    CK(cudaGetLastError());
+    return UC_OK;
+}
+
+extern "C" int uc_temperature_from_held(uc_ctx *ctx)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->enth) return set_err(ctx, UC_E_STATE, "uc_hold_enthalpy first");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(ensure_pressure(ctx));
+    int slot;
+    prof_begin(ctx, UC_K_TEMP, slot);
+    temperature_held_kernel<<<ctx->nsm * 4, 128, 0, ctx->stream>>>(ctx->dP, ctx->enth, ctx->y, ctx->pnd, ctx->npad,
+                                                                    ctx->tk, ctx->rho, ctx->status);
+    prof_end(ctx, slot);
+    CK(cudaGetLastError());
     return UC_OK;
 }
 
@@ -1564,6 +1596,13 @@ extern "C" int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats)
     }
     mlp_decode_kernel<<<grid, 256, 0, st>>>(mlp->dnorm, mlp->IOut, np, ctx->qdsp, np, 0);
     CK(cudaGetLastError());
+    if (std::isinf(tol)) {          // the network alone: no hull check, no fallback
+        if (stats) {
+            CK(cudaStreamSynchronize(st));
+            stats[0] = stats[1] = stats[2] = 0.0;
+        }
+        return UC_OK;
+    }
     // exact omega of one sampled cell per tile
     uc_ctx *S = mlp->sample;
     sample_gather_kernel<<<(S->npad + 255) / 256, 256, 0, st>>>(ctx->tk, ctx->rho, ctx->y, ctx->soot, np, n, nt, S->tk,

@@ -130,8 +130,12 @@ class Surrogate:
         return g, float(loss[0])
 
     # ------------------------------------------------------------ inference
-    def omega(self, u: "unichem.UniChem", tol: float = 1e-3) -> dict:
-        """QDSP of u's state into u's device outputs; returns the fallback statistics."""
+    def omega(self, u: "unichem.UniChem", tol: float = 1e-3, stats: bool = True):
+        """QDSP of u's state into u's device outputs; returns the fallback statistics
+        (which cost a synchronisation and a copy), or None with stats=False."""
+        if not stats:
+            self._ck(self.lib.uc_mlp_omega(self._h, u._h, tol, None))
+            return None
         st = np.zeros(3)
         self._ck(self.lib.uc_mlp_omega(self._h, u._h, tol, st.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return {"tiles_exact": float(st[0]), "cells_outside_hull": float(st[1]), "median_residual": float(st[2])}

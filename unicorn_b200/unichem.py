@@ -98,6 +98,8 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.uc_destroy.restype = None
     IP = ctypes.POINTER(ctypes.c_int)
     lib.uc_set_pressure.argtypes = [vp, P]
+    lib.uc_hold_enthalpy.argtypes = [vp]
+    lib.uc_temperature_from_held.argtypes = [vp]
     lib.uc_integrate.argtypes = [vp, ctypes.c_int, ctypes.POINTER(IntegrateOpts)]
     lib.uc_integrate_tune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(IntegrateOpts)]
     lib.uc_integrate_counts.argtypes = [vp, IP, IP]
@@ -280,6 +282,14 @@ class UniChem:
     def set_pressure(self, pnd):
         """Cell pressures p/PSTR (the reference's non-dimensional pressure)."""
         self._ck(self.lib.uc_set_pressure(self._h, _p(_in(pnd, (self.n,)))))
+
+    def hold_enthalpy(self):
+        """Record each cell's total enthalpy (the in-loop T update keeps it)."""
+        self._ck(self.lib.uc_hold_enthalpy(self._h))
+
+    def temperature_from_held(self):
+        """T from the held enthalpy for the current Y, then rho at the cell pressure."""
+        self._ck(self.lib.uc_temperature_from_held(self._h))
 
     def integrate(self, dt: float, precision: int = FP64, **kw):
         """Advance every cell over dt (uc_integrate); the state stays on the device."""
