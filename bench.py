@@ -510,7 +510,7 @@ def main_c4(args):
     exact = out["qdsp"].copy()
     res = {}
     with ClockSampler(0) as clk:
-        for tol in (1e-3, 1e-1, 1e300):
+        for tol in (1e-3, 1e-1, 1e300, float("inf")):
             ms, _ = timed(lambda: s.omega(u, tol=tol, stats=False), args.steps)
             st = s.omega(u, tol=tol)
             u.download_outputs(out)
@@ -527,7 +527,7 @@ def main_c4(args):
                                   "frac_cells_err_le_1e-3": round(float((err <= 1e-3).mean()), 4)}
     u.close()
     s.close()
-    pure = res["tol=1e+300"]
+    pure = res["tol=inf"]          # the network alone: features, 5 tensor-core layers, decode
     tflops = MLP_FLOP_PER_CELL * nfield / (pure["ms"] / 1e3) / 1e12
     line = {"metric": "omega cell-updates/s: learned surrogate + per-tile FP64 fallback at the stated error",
             "value": res["tol=0.001"]["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
@@ -542,7 +542,7 @@ def main_c4(args):
                        "train_samples_per_s": round(steps * 8192 / t_train, 1),
                        "loss_first": float(loss[:10].mean()), "loss_last": float(loss[-50:].mean())},
             "e2e": None, "gpu_launches": None, "clocks": clk.summary(),
-            "roofline": {"kernel": "surrogate forward (5 tensor-core GEMMs + features/decode)", "bound": "tensor",
+            "roofline": {"kernel": "surrogate forward (features, 5 tensor-core layers, decode; tol=inf)", "bound": "tensor",
                          "achieved": round(tflops, 2), "peak": 1693.5, "peak_source": "measured (bf16 burst)",
                          "unit": "TFLOP/s", "frac": round(tflops / 1693.5, 4), "traffic": None,
                          "flops_rule": f"{MLP_FLOP_PER_CELL} flop per cell (padded 64-256x4-64 layers) / forward time"}}

@@ -123,7 +123,9 @@ int uc_temperature_from_h(uc_ctx *ctx, const double *ht);
  * and h, rate coefficients with omega and d(omega)/dY at the start-of-step
  * state (CKRATES + SOLVEH rates), then the point-implicit update (SOLVESP)
  * with the arguments of uc_species_update. Outputs stay on the device
- * (uc_device_view_get / the download calls).
+ * (uc_device_view_get / the download calls). With UC_MIXED the property
+ * polynomials, square roots and sums also run in FP32 (the state's clip and
+ * closure, Kc and the update stay FP64).
  * Replaces: CALL SPGSOLV's chemistry part (src/lib/spgsolv.f:102-176,1291-1298)
  * preceded by the property block of main:821-1006. */
 int uc_sweep(uc_ctx *ctx, int precision, double dt, int isor, double relx, double tol, double spnorm,
@@ -220,12 +222,14 @@ int uc_integrate_tune(uc_ctx *ctx, int precision, const uc_integrate_opts *o);
 int uc_integrate_counts(uc_ctx *ctx, int *nsub, int *passes);
 
 /* ---------------------------------------------------------------------------
- * The BF16 tensor-core GEMM of the surrogate network, on host buffers (no
+ * The BF16 tensor-core GEMMs of the surrogate network, on host buffers (no
  * reference counterpart; the surrogate is not part of the reference):
  * c[M][N] (FP32) = a[M][K] * b[N][K]^T with a, b BF16 bit patterns, row-major.
- * N a multiple of 16, K a multiple of 64. Allocates and frees its own device
- * buffers; meant for checking the kernel, not for speed. */
-int uc_gemm_bf16(int device, int M, int N, int K, const uint16_t *a, const uint16_t *b, float *c);
+ * kernel 0: the tiled GEMM (N a multiple of 16, K of 64); kernel 1: the
+ * layer kernel with b resident in shared memory (N a multiple of 64 up to 256,
+ * K in 64, 128, 256). Allocates and frees its own device buffers; meant for checking the
+ * kernels, not for speed. */
+int uc_gemm_bf16(int device, int kernel, int M, int N, int K, const uint16_t *a, const uint16_t *b, float *c);
 
 /* ---------------------------------------------------------------------------
  * Learned surrogate of omega (no reference counterpart: the reference always

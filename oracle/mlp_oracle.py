@@ -4,7 +4,8 @@ mlp_gemm.cuh), in float64 with the device's BF16 rounding points, for
 checking the tensor-core gradients. Never used by the product.
 
 Layers 64 -> 256 (GELU) -> 256 (GELU) -> 256 (GELU) -> 256 (GELU) -> 64
-(linear); the loss is the mean squared error over the first 52 outputs.
+(linear), GELU in its tanh form; the loss is the mean squared error over the
+first 52 outputs.
 Rounded to BF16 (round to nearest even) as on the device: the weights, the
 hidden activations gelu(z), the output gradient and the hidden gradients
 (G W^T) * gelu'(z); sums are exact (float64) here and FP32 on the device.
@@ -12,7 +13,6 @@ hidden activations gelu(z), the output gradient and the hidden gradients
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 IN = [64, 256, 256, 256, 256]
 OUT = [256, 256, 256, 256, 64]
@@ -36,12 +36,17 @@ def unpack(w):
     return out
 
 
+C_GELU = np.sqrt(2.0 / np.pi)
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """tanh form: z/2 (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))"""
+    return 0.5 * z * (1.0 + np.tanh(C_GELU * (z + 0.044715 * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(C_GELU * (z + 0.044715 * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * C_GELU * (1.0 + 3 * 0.044715 * z * z)
 
 
 def forward_backward(w, x, t):

@@ -67,3 +67,39 @@ def test_mixed_sweep_vs_fp64_sweep(oracle, c2_slice):
     rel = np.abs(y32 - y64)[mask] / y64[mask]
     print(f"\nmixed sweep: Y after 30 passes, median rel {np.median(rel):.2e}, max rel {rel.max():.2e}")
     assert np.all(rel <= 1e-3)
+
+
+def test_mixed_properties_vs_oracle(oracle, c2_slice):
+    """Mixed-form properties (FP32 polynomials, square roots and sums) against the FP64 oracle.
+
+    mu, lambda, D_k and cp are sums of positive terms. The median relative
+    error is at most 1e-6 (the stated property accuracy); the largest is
+    bounded by 1e-5 for mu, lambda and cp (FP32 rounding of the polynomials in
+    T up to T^5 and of the sums over the sub-mixture) and by 3e-5 for D_k,
+    whose collision integral is a quartic in T* = T/eps_ij with
+    alternating-sign coefficients (main:944-952), evaluated in FP32. The
+    mixture enthalpy h = sum Y_k h_k is a signed sum (formation enthalpies),
+    so it is compared against the scale sum |Y_k h_k|."""
+    from unicorn_b200 import unichem
+    tk, rho, y = c2_slice
+    with unichem.UniChem(len(tk)) as u:
+        u.upload(tk, rho, y)
+        u.sweep(1e-3, precision=unichem.MIXED, isor=1, tol=0.0)
+        out = {k: np.empty((52, len(tk))) if k == "vdf" else np.empty(len(tk)) for k in ("vmu", "vtc", "vdf", "cp", "h")}
+        u.download_outputs(out)
+    yc, mu, lam, dk, _ = oracle.props(tk, y)
+    cp = oracle.cp(tk, yc)
+    hk, hm = oracle.enthalpy(tk, yc)
+    stats = {}
+    for name, a, b in (("mu", out["vmu"], mu), ("lambda", out["vtc"], lam), ("D_k", out["vdf"], dk), ("cp", out["cp"], cp)):
+        rel = np.abs(a - b) / np.abs(b)
+        stats[name] = (np.median(rel), rel.max())
+    print("\nmixed properties (median, max rel): " + ", ".join(f"{k} {v[0]:.1e}/{v[1]:.1e}" for k, v in stats.items()))
+    for name, (med, mx) in stats.items():
+        assert med <= 1e-6, (name, med)
+        assert mx <= (3e-5 if name == "D_k" else 1e-5), (name, mx)
+    hscale = (np.abs(yc * hk)).sum(0)
+    rel_h = np.abs(out["h"] - hm) / hscale
+    stats["h"] = (np.median(rel_h), rel_h.max())
+    print(f"mixed h (median, max rel to sum |Y_k h_k|): {stats['h'][0]:.1e}/{stats['h'][1]:.1e}")
+    assert rel_h.max() <= 1e-5

@@ -1,6 +1,7 @@
 """The surrogate network's BF16 tensor-core kernels (tcgen05) on the GPU.
 
-GEMM: C = A B^T with BF16 operands and FP32 accumulation, checked against
+GEMM (the tiled kernel and the weight-resident layer kernel): C = A B^T with
+BF16 operands and FP32 accumulation, checked against
 the exact product of the same BF16 values (float64 on the host); tolerance
 2^-20 of the sum of |a_k b_k| per entry (FP32 accumulation of at most 8192
 terms)."""
@@ -29,20 +30,21 @@ def lib():
     from unicorn_b200 import unichem
     L = unichem.load_library()
     U16 = ctypes.POINTER(ctypes.c_uint16)
-    L.uc_gemm_bf16.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, U16, U16,
+    L.uc_gemm_bf16.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, U16, U16,
                                ctypes.POINTER(ctypes.c_float)]
     return L
 
 
-@pytest.mark.parametrize("M,N,K", [(128, 256, 64), (300, 256, 64), (128, 64, 256), (1000, 48, 128),
-                                   (256, 512, 64), (200, 16, 8192)])
-def test_gemm_matches_host(lib, M, N, K):
+@pytest.mark.parametrize("kernel,M,N,K", [(0, 128, 256, 64), (0, 300, 256, 64), (0, 128, 64, 256), (0, 1000, 48, 128),
+                                          (0, 256, 512, 64), (0, 200, 16, 8192), (1, 128, 256, 64), (1, 5000, 256, 256),
+                                          (1, 70000, 64, 256), (1, 300, 256, 128)])
+def test_gemm_matches_host(lib, kernel, M, N, K):
     rng = np.random.default_rng(M * 7 + N + K)
     a = to_bf16_bits(rng.standard_normal((M, K)))
     b = to_bf16_bits(rng.standard_normal((N, K)))
     c = np.zeros((M, N), dtype=np.float32)
     U16 = ctypes.POINTER(ctypes.c_uint16)
-    rc = lib.uc_gemm_bf16(0, M, N, K, a.ctypes.data_as(U16), b.ctypes.data_as(U16),
+    rc = lib.uc_gemm_bf16(0, kernel, M, N, K, a.ctypes.data_as(U16), b.ctypes.data_as(U16),
                           c.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
     assert rc == 0
     A, B = from_bf16_bits(a).astype(np.float64), from_bf16_bits(b).astype(np.float64)
@@ -57,8 +59,9 @@ def test_gemm_rejects_bad_shapes(lib):
     c = np.zeros(64 * 64, np.float32)
     P = lambda x: x.ctypes.data_as(U16)
     F = c.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-    assert lib.uc_gemm_bf16(0, 64, 20, 64, P(a), P(a), F) == -1      # N not a multiple of 16
-    assert lib.uc_gemm_bf16(0, 64, 16, 40, P(a), P(a), F) == -1      # K not a multiple of 64
+    assert lib.uc_gemm_bf16(0, 0, 64, 20, 64, P(a), P(a), F) == -1      # N not a multiple of 16
+    assert lib.uc_gemm_bf16(0, 0, 64, 16, 40, P(a), P(a), F) == -1      # K not a multiple of 64
+    assert lib.uc_gemm_bf16(0, 1, 64, 512, 64, P(a), P(a), F) == -1     # layer kernel: N <= 256
 
 
 # ---------------------------------------------------------------- the network

@@ -1,5 +1,6 @@
-// Property kernels, FP64: Y clip + mixture-averaged transport, cp/h, and
-// temperature from enthalpy. Thread = cell.
+// Property kernels: Y clip + mixture-averaged transport, cp/h (FP64, or with the
+// property arithmetic in FP32 for the mixed form), and temperature from
+// enthalpy (FP64). Thread = cell.
 #pragma once
 #include "uc_device.cuh"
 
@@ -22,18 +23,23 @@ __device__ __forceinline__ int ci_range(double TKDS)
     return K;
 }
 
-// Omega(1,1) quartic fit CI11 in T* (main:944-952), for the pair (i, j)
-__device__ __forceinline__ double ci11t(const DevParams &P, int i, int j, double TKD1, double TKD2, double TKD3,
-                                        double TKD4)
+// Omega(1,1) quartic fit CI11 in T* (main:944-952), for the pair (i, j); R is the
+// arithmetic type (double: the drop-in form; float: the mixed form)
+template <typename R>
+__device__ __forceinline__ R ci11t(const DevParams &P, int i, int j, R TKD1, R TKD2, R TKD3, R TKD4)
 {
     const int ij = i * LSP + j;
-    const double TKDS = TKD1 / P.ETLJ1[ij];
-    const double *c = P.ci11 + ci_range(TKDS) * 5;
-    return c[0] + c[1] * TKDS + c[2] * TKD2 / P.ETLJ2[ij] + c[3] * TKD3 / P.ETLJ3[ij] + c[4] * TKD4 / P.ETLJ4[ij];
+    const R TKDS = TKD1 / (R)P.ETLJ1[ij];
+    const double *c = P.ci11 + ci_range((double)TKDS) * 5;
+    return (R)c[0] + (R)c[1] * TKDS + (R)c[2] * TKD2 / (R)P.ETLJ2[ij] + (R)c[3] * TKD3 / (R)P.ETLJ3[ij] +
+           (R)c[4] * TKD4 / (R)P.ETLJ4[ij];
 }
 
-// src/unicornd-mild-sd-5.f:821-1006 for one cell per thread.
-__global__ void __launch_bounds__(128) props_fp64_kernel(const PropArgs a)
+// src/unicornd-mild-sd-5.f:821-1006 for one cell per thread. R = double is the
+// drop-in form; R = float runs the polynomials, square roots and property sums
+// in FP32 (the mixed form), with the clip/closure of the state in FP64.
+template <typename R>
+__global__ void __launch_bounds__(128) props_kernel(const PropArgs a)
 {
     const DevParams &P = *a.P;
     const size_t np = a.npad;
@@ -48,91 +54,93 @@ __global__ void __launch_bounds__(128) props_fp64_kernel(const PropArgs a)
         a.y[(LSP - 1) * np + c] = 1.0 - TMASS;
         // sub-mixture: species with Y >= 1e-3 plus N2 last (main:842-915)
         int8_t sub[LSP];
-        double X[LSP];
+        R X[LSP];
         int IA = 0;
-        TMASS = 0.0;
-        double TMOLE = 0.0;
+        double TMASSD = 0.0;
+        R TMOLE = 0;
         for (int k = 0; k < LSP - 1; ++k) {
             const double yk = a.y[k * np + c];
             if (yk < 1.0e-03) continue;
             sub[IA] = (int8_t)k;
-            TMASS = TMASS + yk;
-            X[IA] = yk / P.WM[k];
+            TMASSD = TMASSD + yk;
+            X[IA] = (R)(yk / P.WM[k]);
             TMOLE = TMOLE + X[IA];
             ++IA;
         }
         int LSPT = IA + 1;
         if (LSPT >= LSP) LSPT = LSP;
         sub[LSPT - 1] = LSP - 1;
-        X[LSPT - 1] = (1.0 - TMASS) / P.WM[LSP - 1];
+        X[LSPT - 1] = (R)((1.0 - TMASSD) / P.WM[LSP - 1]);
         TMOLE = TMOLE + X[LSPT - 1];
-        const double tk = a.tk[c];
-        const double TKRT = sqrt(tk);
-        const double TKD1 = tk * P.TSTR;
-        const double TKD2 = TKD1 * TKD1, TKD3 = TKD2 * TKD1, TKD4 = TKD3 * TKD1, TKD5 = TKD4 * TKD1;
-        const int IPL1 = TKD1 >= UC_TPOL1 ? 7 : 0, IPL2 = TKD1 >= UC_TPOL1 ? 6 : 0;
-        const double TKBP = tk * TKRT / P.PBACK;
-        double ATC[LSP], AMU[LSP];
+        const double tkd = a.tk[c];
+        const R tk = (R)tkd;
+        const R TKRT = sqrt(tk);
+        const R TKD1 = (R)(tkd * P.TSTR);
+        const R TKD2 = TKD1 * TKD1, TKD3 = TKD2 * TKD1, TKD4 = TKD3 * TKD1, TKD5 = TKD4 * TKD1;
+        const int IPL1 = (double)TKD1 >= UC_TPOL1 ? 7 : 0, IPL2 = (double)TKD1 >= UC_TPOL1 ? 6 : 0;
+        const R TKBP = tk * TKRT / (R)P.PBACK;
+        R ATC[LSP], AMU[LSP];
         for (int i = 0; i < LSPT; ++i) {
             const int k = sub[i];
             const double *p = P.poly + k * 14 + IPL1;
             const double *q = P.om22 + k * 12 + IPL2;
-            const double EUKEN = (double)0.115f + (double)0.354f * (p[0] + p[1] * TKD1 + p[2] * TKD2 + p[3] * TKD3 + p[4] * TKD4);
-            const double SIOME = P.cdia[k] * P.cdia[k] * (q[0] + q[1] * TKD1 + q[2] * TKD2 + q[3] * TKD3 + q[4] * TKD4 + q[5] * TKD5);
-            ATC[i] = P.CONVRC * EUKEN * TKRT / P.WMIK[k * LSP + k] / SIOME;
-            AMU[i] = P.CONVRM * TKRT * P.WMIK[k * LSP + k] / SIOME;
+            const R EUKEN = (R)(double)0.115f + (R)(double)0.354f * ((R)p[0] + (R)p[1] * TKD1 + (R)p[2] * TKD2 + (R)p[3] * TKD3 + (R)p[4] * TKD4);
+            const R SIOME = (R)P.cdia[k] * (R)P.cdia[k] *
+                            ((R)q[0] + (R)q[1] * TKD1 + (R)q[2] * TKD2 + (R)q[3] * TKD3 + (R)q[4] * TKD4 + (R)q[5] * TKD5);
+            ATC[i] = (R)P.CONVRC * EUKEN * TKRT / (R)P.WMIK[k * LSP + k] / SIOME;
+            AMU[i] = (R)P.CONVRM * TKRT * (R)P.WMIK[k * LSP + k] / SIOME;
         }
-        double VTC = 0.0, VMU = 0.0;
-        double VDFQ[LSP];
+        R VTC = 0, VMU = 0;
+        R VDFQ[LSP];
         for (int i = 0; i < LSPT; ++i) {
             const int k = sub[i];
-            double PHIK = 0.0, PHDIK = 0.0, EFDIK = 0.0;
+            R PHIK = 0, PHDIK = 0, EFDIK = 0;
             for (int j = 0; j < LSPT; ++j) {
                 if (j == i) continue;
                 const int kb = sub[j];
                 const int ij = k * LSP + kb;
-                const double t1 = 1.0 + sqrt(ATC[i] / ATC[j]) * P.WMIK[ij];
-                const double t2 = 1.0 + sqrt(AMU[i] / AMU[j]) * P.WMIK[ij];
-                PHIK = PHIK + X[j] * (t1 * t1) / P.DWMIK[ij];
-                PHDIK = PHDIK + X[j] * (t2 * t2) / P.DWMIK[ij];
+                const R t1 = (R)1 + sqrt(ATC[i] / ATC[j]) * (R)P.WMIK[ij];
+                const R t2 = (R)1 + sqrt(AMU[i] / AMU[j]) * (R)P.WMIK[ij];
+                PHIK = PHIK + X[j] * (t1 * t1) / (R)P.DWMIK[ij];
+                PHDIK = PHDIK + X[j] * (t2 * t2) / (R)P.DWMIK[ij];
                 // binary diffusion D_ij (main:940-953); the fit value is symmetric in (i, j)
-                const double CI = ci11t(P, i < j ? k : kb, i < j ? kb : k, TKD1, TKD2, TKD3, TKD4);
-                EFDIK = EFDIK + X[j] / (P.WMCD[ij] * TKBP / CI);
+                const R CI = ci11t<R>(P, i < j ? k : kb, i < j ? kb : k, TKD1, TKD2, TKD3, TKD4);
+                EFDIK = EFDIK + X[j] / ((R)P.WMCD[ij] * TKBP / CI);
             }
-            VTC = VTC + ATC[i] * X[i] / (X[i] + (double)1.065f * PHIK);
+            VTC = VTC + ATC[i] * X[i] / (X[i] + (R)(double)1.065f * PHIK);
             VMU = VMU + AMU[i] * X[i] / (X[i] + PHDIK);
-            const double AA = TMOLE - X[i];
-            if (AA <= 1.0e-10) {
+            const R AA = TMOLE - X[i];
+            if ((double)AA <= 1.0e-10) {
                 // DIFSP(i, LSPT): assigned above the diagonal only; the diagonal stays zero
-                double d = 0.0;
+                R d = 0;
                 if (i != LSPT - 1) {
                     const int kl = sub[LSPT - 1];
-                    d = P.WMCD[k * LSP + kl] * TKBP / ci11t(P, k, kl, TKD1, TKD2, TKD3, TKD4);
+                    d = (R)P.WMCD[k * LSP + kl] * TKBP / ci11t<R>(P, k, kl, TKD1, TKD2, TKD3, TKD4);
                 }
-                VDFQ[i] = P.CONVRD * d;
+                VDFQ[i] = (R)P.CONVRD * d;
             } else {
-                VDFQ[i] = P.CONVRD * (TMOLE - X[i]) / EFDIK;
+                VDFQ[i] = (R)P.CONVRD * (TMOLE - X[i]) / EFDIK;
             }
         }
-        a.vtc[c] = VTC;
-        a.vmu[c] = VMU;
+        a.vtc[c] = (double)VTC;
+        a.vmu[c] = (double)VMU;
         // D_k of every species (main:981-1003); N2 (never flagged in ISPQ) takes this path too
         int pos = 0;
         for (int k = 0; k < LSP; ++k) {
-            double v;
+            R v;
             if (k < LSP - 1 && pos < LSPT - 1 && sub[pos] == k) {
                 v = VDFQ[pos];
                 ++pos;
             } else {
-                double EFD = 0.0;
+                R EFD = 0;
                 for (int b = 0; b < LSPT; ++b) {
                     const int nb = sub[b];
-                    const double CI = ci11t(P, k, nb, TKD1, TKD2, TKD3, TKD4);
-                    EFD = EFD + X[b] / (P.WMCD[k * LSP + nb] * TKBP / CI);
+                    const R CI = ci11t<R>(P, k, nb, TKD1, TKD2, TKD3, TKD4);
+                    EFD = EFD + X[b] / ((R)P.WMCD[k * LSP + nb] * TKBP / CI);
                 }
-                v = P.CONVRD * TMOLE / EFD;
+                v = (R)P.CONVRD * TMOLE / EFD;
             }
-            a.vdf[k * np + c] = v;
+            a.vdf[k * np + c] = (double)v;
         }
     }
 }
@@ -145,27 +153,30 @@ struct CpHArgs {
     int n, npad;
 };
 
-__global__ void __launch_bounds__(256) cp_h_fp64_kernel(const CpHArgs a)
+// R = double: the drop-in form; R = float: polynomials and the species sums in FP32
+template <typename R>
+__global__ void __launch_bounds__(256) cp_h_kernel(const CpHArgs a)
 {
     const DevParams &P = *a.P;
     const size_t np = a.npad;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < (size_t)a.n; c += (size_t)gridDim.x * blockDim.x) {
-        const double TKD = a.tk[c] * P.TSTR;
-        const double TKD2 = TKD * TKD, TKD3 = TKD * TKD2, TKD4 = TKD * TKD3, TKD5 = TKD * TKD4;
-        const int ip = TKD > UC_TPOL1 ? 7 : 0;
-        double TCP = 0.0, hs = 0.0;
+        const double TKDd = a.tk[c] * P.TSTR;
+        const R TKD = (R)TKDd;
+        const R TKD2 = TKD * TKD, TKD3 = TKD * TKD2, TKD4 = TKD * TKD3, TKD5 = TKD * TKD4;
+        const int ip = TKDd > UC_TPOL1 ? 7 : 0;
+        R TCP = 0, hs = 0;
         for (int k = 0; k < LSP; ++k) {
             const double *p = P.poly + k * 14 + ip;
-            const double yk = a.y[k * np + c];
-            const double t = (p[0] + p[1] * TKD + p[2] * TKD2 + p[3] * TKD3 + p[4] * TKD4) / P.WM[k];
+            const R yk = (R)a.y[k * np + c];
+            const R t = ((R)p[0] + (R)p[1] * TKD + (R)p[2] * TKD2 + (R)p[3] * TKD3 + (R)p[4] * TKD4) / (R)P.WM[k];
             TCP = TCP + t * yk;
-            const double HSSP = (p[0] * TKD + p[1] * TKD2 / 2.0 + p[2] * TKD3 / 3.0 + p[3] * TKD4 / 4.0 + p[4] * TKD5 / 5.0) /
-                                P.WM[k] * P.HCONVR;
-            const double H = HSSP * P.WMSTR * P.HSTR + p[5] / P.WM[k] * P.GASC;
+            const R HSSP = ((R)p[0] * TKD + (R)p[1] * TKD2 / (R)2 + (R)p[2] * TKD3 / (R)3 + (R)p[3] * TKD4 / (R)4 +
+                            (R)p[4] * TKD5 / (R)5) / (R)P.WM[k] * (R)P.HCONVR;
+            const R H = HSSP * (R)P.WMSTR * (R)P.HSTR + (R)p[5] / (R)P.WM[k] * (R)P.GASC;
             hs = hs + yk * H;
         }
-        if (a.cp) a.cp[c] = TCP / P.WMSTR * P.GASC * P.TSTR / P.HSTR;
-        if (a.h) a.h[c] = hs;
+        if (a.cp) a.cp[c] = (double)(TCP / (R)P.WMSTR * (R)P.GASC * (R)P.TSTR / (R)P.HSTR);
+        if (a.h) a.h[c] = (double)hs;
     }
 }
 

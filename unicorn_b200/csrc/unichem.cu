@@ -630,7 +630,7 @@ extern "C" int uc_omega(uc_ctx *ctx, int precision, double *qdsp, double *qdot, 
     return UC_OK;
 }
 
-extern "C" int uc_props(uc_ctx *ctx, double *vmu, double *vtc, double *vdf)
+static int props_impl(uc_ctx *ctx, int precision, double *vmu, double *vtc, double *vdf)
 {
     if (!ctx) return UC_E_ARG;
     if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "uc_props before uc_upload_fields");
@@ -642,7 +642,10 @@ extern "C" int uc_props(uc_ctx *ctx, double *vmu, double *vtc, double *vdf)
     const int grid = std::min((ctx->n + 127) / 128, ctx->nsm * 16);
     int slot;
     prof_begin(ctx, UC_K_PROPS, slot);
-    props_fp64_kernel<<<grid, 128, 0, ctx->stream>>>(a);
+    if (precision == UC_MIXED)
+        props_kernel<float><<<grid, 128, 0, ctx->stream>>>(a);
+    else
+        props_kernel<double><<<grid, 128, 0, ctx->stream>>>(a);
     prof_end(ctx, slot);
     CK(cudaGetLastError());
     if (vmu || vtc || vdf) {
@@ -654,7 +657,12 @@ extern "C" int uc_props(uc_ctx *ctx, double *vmu, double *vtc, double *vdf)
     return UC_OK;
 }
 
-extern "C" int uc_cp_h(uc_ctx *ctx, double *cp, double *h)
+extern "C" int uc_props(uc_ctx *ctx, double *vmu, double *vtc, double *vdf)
+{
+    return props_impl(ctx, UC_FP64, vmu, vtc, vdf);
+}
+
+static int cp_h_impl(uc_ctx *ctx, int precision, double *cp, double *h)
 {
     if (!ctx) return UC_E_ARG;
     if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "uc_cp_h before uc_upload_fields");
@@ -665,7 +673,10 @@ extern "C" int uc_cp_h(uc_ctx *ctx, double *cp, double *h)
     const int grid = std::min((ctx->n + 255) / 256, ctx->nsm * 8);
     int slot;
     prof_begin(ctx, UC_K_CPH, slot);
-    cp_h_fp64_kernel<<<grid, 256, 0, ctx->stream>>>(a);
+    if (precision == UC_MIXED)
+        cp_h_kernel<float><<<grid, 256, 0, ctx->stream>>>(a);
+    else
+        cp_h_kernel<double><<<grid, 256, 0, ctx->stream>>>(a);
     prof_end(ctx, slot);
     CK(cudaGetLastError());
     if (cp || h) {
@@ -674,6 +685,11 @@ extern "C" int uc_cp_h(uc_ctx *ctx, double *cp, double *h)
         CK(cudaStreamSynchronize(ctx->stream));
     }
     return UC_OK;
+}
+
+extern "C" int uc_cp_h(uc_ctx *ctx, double *cp, double *h)
+{
+    return cp_h_impl(ctx, UC_FP64, cp, h);
 }
 
 extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, double tol, double spnorm,
@@ -741,8 +757,9 @@ extern "C" int uc_sweep(uc_ctx *ctx, int precision, double dt, int isor, double 
 {
     if (!ctx) return UC_E_ARG;
     if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "uc_sweep before uc_upload_fields");
-    RET_IF(uc_props(ctx, nullptr, nullptr, nullptr));
-    RET_IF(uc_cp_h(ctx, nullptr, nullptr));
+    if (precision != UC_FP64 && precision != UC_MIXED) return set_err(ctx, UC_E_ARG, "unknown precision %d", precision);
+    RET_IF(props_impl(ctx, precision, nullptr, nullptr, nullptr));
+    RET_IF(cp_h_impl(ctx, precision, nullptr, nullptr));
     CK(cudaSetDevice(ctx->device));
     RET_IF(launch_chem(ctx, precision, true, true));
     ctx->have_rc = true;
@@ -1123,15 +1140,33 @@ static cudaError_t launch_gemm(const GemmArgs &g, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// One network layer over M rows with the weights resident in shared memory (mlp_gemm.cuh).
+static cudaError_t launch_layer(const GemmArgs &g, int nsm, cudaStream_t st)
+{
+    static thread_local int attr_done = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (attr_done != dev) {
+        cudaError_t e = cudaFuncSetAttribute(gemm_w_resident_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)LW_SMEM);
+        if (e != cudaSuccess) return e;
+        attr_done = dev;
+    }
+    const int ntiles = (g.M + GM - 1) / GM;
+    gemm_w_resident_kernel<<<std::min(ntiles, nsm), LW_THREADS, LW_SMEM, st>>>(g);
+    return cudaGetLastError();
+}
+
 static bool gemm_shape_ok(int M, int N, int K, int lda, int ldb)
 {
     return M > 0 && N > 0 && K > 0 && N % 16 == 0 && K % GK == 0 && lda % 8 == 0 && ldb % 8 == 0 && lda >= K &&
            ldb >= K;
 }
 
-extern "C" int uc_gemm_bf16(int device, int M, int N, int K, const uint16_t *a, const uint16_t *b, float *c)
+extern "C" int uc_gemm_bf16(int device, int kernel, int M, int N, int K, const uint16_t *a, const uint16_t *b, float *c)
 {
     if (!a || !b || !c || !gemm_shape_ok(M, N, K, K, K)) return UC_E_ARG;
+    if (kernel != 0 && (kernel != 1 || N > 256 || N % 64 != 0 || (K != 64 && K != 128 && K != 256))) return UC_E_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return UC_E_CUDA;
     __nv_bfloat16 *dA = nullptr, *dB = nullptr;
     float *dC = nullptr;
@@ -1146,7 +1181,21 @@ extern "C" int uc_gemm_bf16(int device, int M, int N, int K, const uint16_t *a, 
         GemmArgs g{};
         g.A = dA; g.B = dB; g.lda = K; g.ldb = K; g.M = M; g.N = N; g.K = K;
         g.epi = EPI_F32; g.out_f32 = dC; g.ldo = N; g.status = dst;
-        if (launch_gemm(g, 0) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) rc = UC_E_CUDA;
+        float *zb = nullptr;
+        cudaError_t e;
+        if (kernel == 1) {                 // the layer kernel adds a bias: give it zeros
+            g.epi = EPI_BIAS_F32;
+            if (cudaMalloc((void **)&zb, N * sizeof(float)) != cudaSuccess) rc = UC_E_NOMEM;
+            else cudaMemset(zb, 0, N * sizeof(float));
+            g.bias = zb;
+            cudaDeviceProp prop;
+            cudaGetDeviceProperties(&prop, device);
+            e = rc == UC_OK ? launch_layer(g, prop.multiProcessorCount, 0) : cudaSuccess;
+        } else {
+            e = launch_gemm(g, 0);
+        }
+        if (rc == UC_OK && (e != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)) rc = UC_E_CUDA;
+        cudaFree(zb);
         if (rc == UC_OK) {
             cudaMemcpy(c, dC, (size_t)M * N * 4, cudaMemcpyDeviceToHost);
             cudaMemcpy(&st, dst, sizeof(int), cudaMemcpyDeviceToHost);
@@ -1391,6 +1440,26 @@ static void mlp_free_batch(uc_mlp *mlp)
     mlp->bcap = 0;
 }
 
+// forward layer l over M rows (weights resident in shared memory)
+static int mlp_layer(uc_mlp *mlp, cudaStream_t st, const __nv_bfloat16 *A, int lda, int l, int M, int epi,
+                     float *z_save, float *of, __nv_bfloat16 *ob)
+{
+    GemmArgs g{};
+    g.A = A; g.lda = lda; g.B = mlp->wb + mlp->bfoff[l]; g.ldb = mlp->in[l];
+    g.M = M; g.N = mlp->out[l]; g.K = mlp->in[l]; g.epi = epi; g.bias = mlp->w + mlp->boff[l];
+    g.z_save = z_save; g.ldz = MLP_H; g.out_f32 = of; g.out_bf16 = ob; g.ldo = mlp->out[l];
+    g.status = mlp->status;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static thread_local int nsm = 0, nsm_dev = -1;
+    if (nsm_dev != dev) {
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        nsm_dev = dev;
+    }
+    MCK(launch_layer(g, nsm, st));
+    return UC_OK;
+}
+
 static int mlp_batch_buffers(uc_mlp *mlp, int B)
 {
     if (B <= mlp->bcap) return UC_OK;
@@ -1416,9 +1485,8 @@ static int mlp_enqueue_fwd_bwd(uc_mlp *mlp, int B, float *loss_hist)
     cudaStream_t st = mlp->stream;
     for (int l = 0; l < MLP_LAYERS; ++l) {
         const bool last = l == MLP_LAYERS - 1;
-        RET_IF(mlp_gemm(mlp, st, mlp->H[l], mlp->in[l], mlp->wb + mlp->bfoff[l], mlp->in[l], B, mlp->out[l], mlp->in[l],
-                        last ? EPI_BIAS_F32 : EPI_BIAS_GELU, mlp->w + mlp->boff[l], nullptr, last ? nullptr : mlp->Z[l],
-                        MLP_H, last ? mlp->Out : nullptr, last ? nullptr : mlp->H[l + 1], last ? MLP_OUT : MLP_H));
+        RET_IF(mlp_layer(mlp, st, mlp->H[l], mlp->in[l], l, B, last ? EPI_BIAS_F32 : EPI_BIAS_GELU,
+                         last ? nullptr : mlp->Z[l], last ? mlp->Out : nullptr, last ? nullptr : mlp->H[l + 1]));
     }
     const int lblk = 256;
     mlp_loss_grad_kernel<<<lblk, 256, 0, st>>>(mlp->Out, mlp->T, B, mlp->G[MLP_LAYERS - 1], mlp->partial);
@@ -1589,9 +1657,8 @@ extern "C" int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats)
     __nv_bfloat16 *hin = mlp->IX, *hb[2] = {mlp->IH0, mlp->IH1};
     for (int l = 0; l < MLP_LAYERS; ++l) {
         const bool last = l == MLP_LAYERS - 1;
-        RET_IF(mlp_gemm(mlp, st, hin, mlp->in[l], mlp->wb + mlp->bfoff[l], mlp->in[l], np, mlp->out[l], mlp->in[l],
-                        last ? EPI_BIAS_F32 : EPI_BIAS_GELU, mlp->w + mlp->boff[l], nullptr, nullptr, 0,
-                        last ? mlp->IOut : nullptr, last ? nullptr : hb[l & 1], last ? MLP_OUT : MLP_H));
+        RET_IF(mlp_layer(mlp, st, hin, mlp->in[l], l, np, last ? EPI_BIAS_F32 : EPI_BIAS_GELU, nullptr,
+                         last ? mlp->IOut : nullptr, last ? nullptr : hb[l & 1]));
         if (!last) hin = hb[l & 1];
     }
     mlp_decode_kernel<<<grid, 256, 0, st>>>(mlp->dnorm, mlp->IOut, np, ctx->qdsp, np, 0);
