@@ -131,6 +131,32 @@ int uc_temperature_from_h(uc_ctx *ctx, const double *ht);
 int uc_sweep(uc_ctx *ctx, int precision, double dt, int isor, double relx, double tol, double spnorm,
              const double *face_sum, const double *face_nbr, int *passes);
 
+/* ---------------------------------------------------------------------------
+ * The species equations' face coefficients on the device.
+ * Replaces: the coefficient assembly of SPGSOLV, src/lib/spgsolv.f:233-1290
+ * (face conductances from EMU, VDFSP and the eddy viscosity; hybrid
+ * convection-diffusion coefficients E, W, N, S with the axisymmetric terms).
+ * The context's n cells must be the whole lj x li grid (J fastest), boundary
+ * cells included. Geometry: XXS, XXC [li], YYS, YYC [lj], the radial
+ * coordinate Y(J,I) [n], ISYM. Flow: U, V, TMU [n] and SIGSP.
+ * Once a grid and a flow are set, uc_sweep assembles the faces after the
+ * properties (with its dt) and the update uses them whenever no face arrays
+ * are passed: face_sum = E+W+N+S, face_nbr = N Y(J+1) + S Y(J-1) + E Y(I+1)
+ * + W Y(I-1) with the neighbours' Y at the start of the update (Jacobi over
+ * cells; the reference's lexicographic Gauss-Seidel has no parallel form),
+ * and the grid's boundary cells keep their state, as SOLVESP updates only
+ * J = 2..LJ-1, I = 2..LI-1. Every interior cell is assembled (no ISKIP).
+ * uc_set_grid(ctx, NULL) returns to the face-less update.
+ */
+typedef struct {
+    int lj, li, isym;
+    const double *xxs, *xxc, *yys, *yyc, *yr;
+} uc_grid;
+int uc_set_grid(uc_ctx *ctx, const uc_grid *g);
+int uc_set_flow(uc_ctx *ctx, const double *u, const double *v, const double *tmu, double sigsp);
+/* Assemble now (needs uc_props of the current state); e, w, n, s [51*n] host copies (may be NULL). */
+int uc_assemble_faces(uc_ctx *ctx, double dt, double *e, double *w, double *n, double *s);
+
 /* Outputs of the last uc_sweep/uc_omega/uc_props/uc_cp_h to the host (NULL = skip). */
 int uc_download_outputs(uc_ctx *ctx, double *qdsp, double *qdot, double *domega_dy, double *vmu,
                         double *vtc, double *vdf, double *cp, double *h);

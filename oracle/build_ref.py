@@ -15,6 +15,8 @@ Translated pieces (reference paths relative to the UNICORN checkout):
 * ``src/lib/solveh.f:34-57,116-1145``  h_k, RA, PRD, QDSP, QDOT  -> f77_solveh_omega
 * ``src/lib/solveh.f:34-38,1170-1234`` T from h by Newton        -> f77_solveh_temperature
 * ``src/lib/spgsolv.f:98-232``  mixture cp (TCP probed per cell) -> f77_spgsolv_cp
+* ``src/lib/spgsolv.f:98-1290`` cp, EKT/EMU, face conductances and the
+  E/W/N/S coefficients of the species equations    -> f77_spgsolv_coef
 * ``src/unicornd-mild-sd-5.f:84-113`` DATA WSP/CDIA/TLJ/CI11      -> f77_main_data
 * ``src/unicornd-mild-sd-5.f:327-483`` set-up of tables/scales    -> f77_main_setup
 * ``src/unicornd-mild-sd-5.f:821-1006`` Y clip + transport props   -> f77_main_props
@@ -68,6 +70,7 @@ def build(ref: str, lj: int, li: int, out: Path = OUT) -> Path:
         (sh, "f77_solveh_omega", [(34, 57), (116, 1145)], None, None),
         (sh, "f77_solveh_temperature", [(34, 38), (1170, 1234)], None, None),
         (spg, "f77_spgsolv_cp", [(98, 232)], None, probe_cp),
+        (spg, "f77_spgsolv_coef", [(98, 1290)], None, None),
     ]
     code = translate(frags, [data, ckr, ssp, sh, spg, main])
     code = code.replace("#include <string.h>", f"#include <string.h>\ndouble F77P_TCP[{ncell}];", 1)

@@ -348,6 +348,15 @@ class Oracle:
                                ctypes.c_double(tol), _iptr(passes))
         return tk, rho, y, s, passes
 
+    def faces(self, lj, li, rho, vdf, u, v, tmu, yr, xxs, xxc, yys, yyc, isym=1, dt=1e-3, sigsp=0.7):
+        """E/W/N/S species coefficients [51][lj*li] of the interior cells (zero elsewhere)."""
+        ne = lj * li
+        out = [np.zeros((LSP - 1, ne)) for _ in range(4)]
+        self.lib.orc_faces(lj, li, _dptr(_c(rho)), _dptr(_c(vdf)), _dptr(_c(u)), _dptr(_c(v)), _dptr(_c(tmu)),
+                           _dptr(_c(yr)), _dptr(_c(xxs)), _dptr(_c(xxc)), _dptr(_c(yys)), _dptr(_c(yyc)), int(isym),
+                           ctypes.c_double(dt), ctypes.c_double(sigsp), *[_dptr(o) for o in out])
+        return tuple(out)
+
     def temperature(self, tk_guess, y, ht):
         tk = np.array(tk_guess, dtype=np.float64, copy=True)
         self.lib.orc_temperature(len(tk), _dptr(tk), _dptr(_c(y)), _dptr(_c(ht)))

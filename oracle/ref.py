@@ -254,6 +254,8 @@ class RefUnicorn:
         self.lib.f77_ckrates()
         for blk in ("DUMMY", "DUM0", "DUMX"):
             self._block(blk)[:] = 0
+        for nm in ("STE", "STW", "STN", "STS"):          # soot face coefficients (no transport here)
+            self.var("SOLVESP", nm)[:] = 0.0
         SSP = self.var("SOLVEH", "SSP").reshape(self.LJ, self.LI, LSP, order="F")
         FSP = self.var("UNICORN", "FSP").reshape(self.LJ, self.LI, LSP, order="F")
         SSP[:] = FSP
@@ -290,3 +292,42 @@ class RefUnicorn:
             self.lib.f77_solveh_temperature()
             out[a:b] = self.var("UNICORN", "TK").reshape(self.LJ, self.LI, order="F")[j, i]
         return out
+
+    # -------------------------------------------------------------- SPGSOLV coefficients
+    SPECIES_SUFFIX = [f"{a}{b}" for a in "ABC" for b in "0123456789ABCDEFGHIJ"][:LSP - 1]
+
+    def spgsolv_coefficients(self, tk, rho, y, vtc, vdf, u, v, tmu, stdf, xxs, xxc, yys, yyc, yr,
+                             isym=1, dt=1e-3, sigsp=0.7, sigh=0.7):
+        """The E/W/N/S coefficients of the species equations (lib/spgsolv.f:98-1290) on the whole
+        compile-time grid (fields [LJ*LI], J fastest; vdf, y [52][LJ*LI]; geometry XXS/XXC [LI],
+        YYS/YYC [LJ], Y(J,I) radial coordinate [LJ*LI]). Returns e, w, n, s [51][LJ*LI] for the
+        interior cells (boundary entries as the routine leaves them)."""
+        LJ, LI = self.LJ, self.LI
+        S = "SPGSOLV"
+        sh = lambda a: np.asarray(a, dtype=np.float64).reshape(LJ, LI, order="F")
+        self.var(S, "TK")[:] = sh(tk)
+        self.var(S, "RHO")[:] = sh(rho)
+        for k in range(LSP):
+            nm = "F" + (self.SPECIES_SUFFIX[k] if k < LSP - 1 else "CB")
+            self.var(S, nm)[:] = sh(y[k])
+        self.var(S, "VTC")[:] = sh(vtc)
+        VDF = self.var(S, "VDF")
+        for k in range(LSP):
+            VDF[:, :, k] = sh(vdf[k])
+        for nm, a in (("U", u), ("V", v), ("TMU", tmu), ("STDF", stdf), ("Y", yr)):
+            self.var(S, nm)[:] = sh(a)
+        self.var(S, "XXS")[:] = xxs
+        self.var(S, "XXC")[:] = xxc
+        self.var(S, "YYS")[:] = yys
+        self.var(S, "YYC")[:] = yyc
+        self.var(S, "ISKIP")[:] = 0
+        self.scalar(S, "ISYM", isym)
+        self.scalar(S, "DT", dt)
+        ctypes.c_double.in_dll(self.lib, "F77A_SPGSOLV_SIGSP").value = sigsp
+        ctypes.c_double.in_dll(self.lib, "F77A_SPGSOLV_SIGH").value = sigh
+        self.lib.f77_spgsolv_coef()
+        out = []
+        for face in "EWPQ":
+            out.append(np.stack([self.var(S, face + self.SPECIES_SUFFIX[k]).reshape(-1, order="F")
+                                 for k in range(LSP - 1)]))
+        return tuple(o.copy() for o in out)

@@ -882,3 +882,57 @@ void orc_integrate(int n, double *tk, double *rho, double *y, double *soot, cons
         if (passes) passes[c] = np;
     }
 }
+
+/* ------------------------------------------------------------- species face coefficients */
+
+/* E/W/N/S coefficients of the species equations (spgsolv.f:233-348 face
+ * conductances, :350-1290 hybrid convection-diffusion coefficients) for the
+ * interior cells J=2..LJ-1, I=2..LI-1 of an lj x li grid (J fastest; cell
+ * c = (I-1)*lj + (J-1)). rho, u, v, tmu, yr [lj*li]; vdf [52][lj*li];
+ * xxs, xxc [li]; yys, yyc [lj]. Outputs e, w, n, s [51][lj*li]; boundary
+ * entries are left untouched. Every cell is assembled (no ISKIP). */
+void orc_faces(int lj, int li, const double *rho, const double *vdf, const double *u, const double *v,
+               const double *tmu, const double *yr, const double *xxs, const double *xxc, const double *yys,
+               const double *yyc, int isym, double dt, double sigsp, double *e, double *w, double *n, double *s)
+{
+    const size_t ne = (size_t)lj * li;
+    const double SYM = (double)isym;
+#define CI(j, i) ((size_t)(i) * lj + (j))          /* 0-based (j, i) */
+#define EMU(j, i) (S.REI * S.BETA3 * rho[CI(j, i)])
+    for (int i = 1; i < li - 1; ++i) {
+        for (int j = 1; j < lj - 1; ++j) {
+            const size_t c = CI(j, i);
+            const double DTBRX = dt / xxc[i], DTBRY = dt / yyc[j];
+            const double RHOUE = 0.5 * (rho[CI(j, i + 1)] + rho[c]) * u[CI(j, i + 1)];
+            const double RHOUW = 0.5 * (rho[c] + rho[CI(j, i - 1)]) * u[c];
+            const double RHOVN = 0.5 * (rho[CI(j + 1, i)] + rho[c]) * v[CI(j + 1, i)];
+            const double RHOVS = 0.5 * (rho[c] + rho[CI(j - 1, i)]) * v[c];
+            const double SYM1 = SYM * dt * 0.5 * EMU(j, i) / yr[c];
+            const double SYM2 = SYM * dt * 0.5 * S.REI * tmu[c] / sigsp / yr[c];
+            /* turbulent parts of the conductances of the faces E (= W of I+1), W, N (= S of J+1), S */
+            const double TURE = S.REI * (tmu[CI(j, i + 1)] + tmu[c]) / sigsp;
+            const double TURW = S.REI * (tmu[c] + tmu[CI(j, i - 1)]) / sigsp;
+            const double TURN = S.REI * (tmu[CI(j + 1, i)] + tmu[c]) / sigsp;
+            const double TURS = S.REI * (tmu[c] + tmu[CI(j - 1, i)]) / sigsp;
+            for (int k = 0; k < LSP - 1; ++k) {
+                const double *d = vdf + (size_t)k * ne;
+                const double DE = (EMU(j, i + 1) * d[CI(j, i + 1)] + EMU(j, i) * d[c] + TURE) / xxs[i + 1];
+                const double DW = (EMU(j, i) * d[c] + EMU(j, i - 1) * d[CI(j, i - 1)] + TURW) / xxs[i];
+                const double DN = (EMU(j + 1, i) * d[CI(j + 1, i)] + EMU(j, i) * d[c] + TURN) / yys[j + 1];
+                const double DS = (EMU(j, i) * d[c] + EMU(j - 1, i) * d[CI(j - 1, i)] + TURS) / yys[j];
+                const double SYMA = SYM1 * d[c] + SYM2;
+                double cv;
+                cv = fabs(RHOUE); if (DE >= cv) cv = DE;
+                e[(size_t)k * ne + c] = DTBRX * 0.5 * (RHOUE - cv);
+                cv = fabs(RHOUW); if (DW >= cv) cv = DW;
+                w[(size_t)k * ne + c] = DTBRX * 0.5 * (-RHOUW - cv);
+                cv = fabs(RHOVN); if (DN >= cv) cv = DN;
+                n[(size_t)k * ne + c] = DTBRY * 0.5 * (RHOVN - cv) - SYMA / yys[j + 1];
+                cv = fabs(RHOVS); if (DS >= cv) cv = DS;
+                s[(size_t)k * ne + c] = DTBRY * 0.5 * (-RHOVS - cv) + SYMA / yys[j];
+            }
+        }
+    }
+#undef CI
+#undef EMU
+}

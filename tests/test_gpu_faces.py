@@ -1,0 +1,87 @@
+"""Species-equation faces assembled on the GPU (uc_set_grid / uc_set_flow /
+uc_assemble_faces) against the oracle's restatement (itself pinned bit for
+bit to the reference's assembly, tests/test_faces_oracle.py), and a sweep
+that uses them against the oracle's update with the same faces.
+
+Tolerances: the coefficients to 1e-10 of the largest |coefficient| of the
+cell and species (the hybrid form takes max(|rho u|, D), so an ulp in D can
+change which branch holds; the coefficients themselves are differences of
+O(1) terms); the swept Y to 1e-9 relative (the FP64 update tolerance)."""
+import numpy as np
+import pytest
+
+from test_faces_oracle import grid_case
+
+pytestmark = pytest.mark.gpu
+LJ, LI = 61, 101          # the C1 grid: 101 (z) x 61 (r)
+
+
+@pytest.fixture(scope="module")
+def cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("a GPU test ran without a CUDA device")
+    from unicorn_b200 import unichem
+    return unichem
+
+
+@pytest.fixture(scope="module")
+def case(oracle):
+    return grid_case(oracle, LJ, LI, 4)
+
+
+def interior_mask():
+    J, I = np.meshgrid(np.arange(LJ), np.arange(LI), indexing="ij")
+    return ((J > 0) & (J < LJ - 1) & (I > 0) & (I < LI - 1)).reshape(-1, order="F")
+
+
+def test_faces_match_oracle(cuda, oracle, case):
+    g = case
+    n = LJ * LI
+    with cuda.UniChem(n) as u:
+        u.upload(g["tk"], g["rho"], g["y"])
+        u.props()
+        u.set_grid(LJ, LI, g["xxs"], g["xxc"], g["yys"], g["yyc"], g["yr"], isym=1)
+        u.set_flow(g["u"], g["v"], g["tmu"], 0.7)
+        faces = u.assemble_faces(1e-3)
+    yc, mu, lam, vdf, _ = oracle.props(g["tk"], g["y"])
+    ref = oracle.faces(LJ, LI, g["rho"], vdf, g["u"], g["v"], g["tmu"], g["yr"], g["xxs"], g["xxc"], g["yys"],
+                       g["yyc"], isym=1, dt=1e-3, sigsp=0.7)
+    inside = interior_mask()
+    scale = np.max(np.abs(np.stack(ref)), axis=0)
+    for a, b in zip(faces, ref):
+        assert np.all(np.abs(a - b)[:, inside] <= 1e-10 * scale[:, inside] + 1e-300)
+        assert np.all(a[:, ~inside] == 0.0)
+
+
+def test_sweep_with_faces_matches_oracle(cuda, oracle, case):
+    g = case
+    n = LJ * LI
+    dt = 1e-3
+    with cuda.UniChem(n) as u:
+        u.upload(g["tk"], g["rho"], g["y"])
+        u.set_grid(LJ, LI, g["xxs"], g["xxc"], g["yys"], g["yyc"], g["yr"], isym=1)
+        u.set_flow(g["u"], g["v"], g["tmu"], 0.7)
+        u.sweep(dt, isor=4, tol=0.0)
+        _, _, y_gpu, _, _ = u.download()
+    yc, mu, lam, vdf, _ = oracle.props(g["tk"], g["y"])
+    e, w, nn, s = oracle.faces(LJ, LI, g["rho"], vdf, g["u"], g["v"], g["tmu"], g["yr"], g["xxs"], g["xxc"],
+                               g["yys"], g["yyc"], isym=1, dt=dt, sigsp=0.7)
+    inside = interior_mask()
+    Y = yc[:51]
+    fsum = np.where(inside, e + w + nn + s, 0.0)
+    fnbr = np.zeros_like(fsum)
+    idx = np.nonzero(inside)[0]
+    fnbr[:, idx] = (nn[:, idx] * Y[:, idx + 1] + s[:, idx] * Y[:, idx - 1] + e[:, idx] * Y[:, idx + LJ]
+                    + w[:, idx] * Y[:, idx - LJ])
+    rc, sour = oracle.rates(g["tk"], g["rho"], yc)
+    y_o, _, _ = oracle.species_update(g["rho"], yc, rc, sour, dt, isor=4, tol=0.0, face_sum=fsum, face_nbr=fnbr)
+    err = np.abs(y_gpu - y_o)[:, inside] - (1e-9 * np.abs(y_o[:, inside]) + 1e-18)
+    assert (err <= 0).all(), err.max()
+    assert np.array_equal(y_gpu[:, ~inside], yc[:, ~inside])        # boundary cells are held
+    # the faces move the interior: the same sweep without them differs
+    with cuda.UniChem(n) as u:
+        u.upload(g["tk"], g["rho"], g["y"])
+        u.sweep(dt, isor=4, tol=0.0)
+        _, _, y_nf, _, _ = u.download()
+    assert np.abs(y_nf - y_gpu)[:, inside].max() > 1e-6

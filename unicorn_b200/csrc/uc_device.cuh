@@ -43,7 +43,7 @@ static_assert(PAIRTAB_BYTES % 16 == 0, "bulk copy size must be a multiple of 16 
 // static work split of the species phase.
 struct DevParams {
     double TSTR, RSTR, WMSTR, ALSTR, VSTR, HSTR, GASC, PBACK, CONVRC, CONVRM, CONVRD;
-    double C1ST, C2ND, C3RD, RCONV, HCONVR, TKDMIN, RSTR_WMSTR, BETA1;
+    double C1ST, C2ND, C3RD, RCONV, HCONVR, TKDMIN, RSTR_WMSTR, BETA1, BETA3, REI;
     double WM[LSP], HFO[LSP];
     double poly[LSP * 14];
     double om22[LSP * 12];

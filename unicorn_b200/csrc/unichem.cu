@@ -15,6 +15,7 @@
 #include "props_kernel.cuh"
 #include "update_kernel.cuh"
 #include "integrate_kernel.cuh"
+#include "faces_kernel.cuh"
 #include "mlp_gemm.cuh"
 #include "mlp.cuh"
 
@@ -42,6 +43,14 @@ struct uc_ctx {
     int *status = nullptr, *passes = nullptr;
     bool have_fields = false, have_rc = false;
     int upd_grid = 0;
+    // species-equation faces assembled on the device (grid, flow, coefficients)
+    int lj = 0, li = 0, isym = 0;
+    double sigsp = 0.0;
+    double *g_xxs = nullptr, *g_xxc = nullptr, *g_yys = nullptr, *g_yyc = nullptr, *g_yr = nullptr;
+    double *f_u = nullptr, *f_v = nullptr, *f_tmu = nullptr;
+    double *fe = nullptr, *fw = nullptr, *fn = nullptr, *fs = nullptr;
+    uint8_t *hold = nullptr;
+    bool have_grid = false, have_flow = false, faces_ready = false;
     // batched integration
     double *pnd = nullptr, *enth = nullptr;
     int *nsub = nullptr, *order = nullptr, *hist = nullptr, *next_tile = nullptr, *cpasses = nullptr;
@@ -170,6 +179,8 @@ static void build_params(const uc_inputs &in, DevParams &P, std::vector<PairTab>
     P.TKDMIN = sc.tstr - 1.0;
     P.RSTR_WMSTR = sc.rstr / sc.wmstr;
     P.BETA1 = sc.beta1;
+    P.BETA3 = sc.beta3;
+    P.REI = sc.rei;
     for (int k = 0; k < LSP; ++k) {   // main:461-464
         P.WM[k] = uc_wsp[k] / 1000.0 / sc.wmstr;
         P.HFO[k] = sc.hconv * uc_poly[k * 14 + 5] / P.WM[k];
@@ -316,6 +327,10 @@ static void free_ctx(uc_ctx *c)
             if (*b) { cudaFree(*b); *b = nullptr; }
         if (c->pnd) cudaFree(c->pnd);
         if (c->enth) cudaFree(c->enth);
+        void *fb[] = {c->g_xxs, c->g_xxc, c->g_yys, c->g_yyc, c->g_yr, c->f_u, c->f_v, c->f_tmu,
+                      c->fe, c->fw, c->fn, c->fs, c->hold};
+        for (void *b : fb)
+            if (b) cudaFree(b);
         if (c->int_exec) cudaGraphExecDestroy(c->int_exec);
         if (c->int_graph) cudaGraphDestroy(c->int_graph);
     }
@@ -703,6 +718,20 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
     CK(cudaMemcpyAsync(ctx->y0, ctx->y, (size_t)LSP * ctx->npad * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->soot0, ctx->soot, 2 * (size_t)ctx->npad * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     const double *fs = nullptr, *fn = nullptr;
+    const uint8_t *hold = nullptr;
+    if (!face_sum && !face_nbr && ctx->faces_ready) {
+        // assembled coefficients with the neighbours' Y of this moment
+        RET_IF(dalloc(ctx, &ctx->face_sum, (size_t)(LSP - 1) * ctx->npad));
+        RET_IF(dalloc(ctx, &ctx->face_nbr, (size_t)(LSP - 1) * ctx->npad));
+        CK(cudaMemsetAsync(ctx->face_sum, 0, (size_t)(LSP - 1) * ctx->npad * sizeof(double), ctx->stream));
+        CK(cudaMemsetAsync(ctx->face_nbr, 0, (size_t)(LSP - 1) * ctx->npad * sizeof(double), ctx->stream));
+        faces_apply_kernel<<<ctx->nsm * 4, 256, 0, ctx->stream>>>(ctx->lj, ctx->li, ctx->npad, ctx->fe, ctx->fw, ctx->fn,
+                                                                ctx->fs, ctx->y, ctx->face_sum, ctx->face_nbr);
+        CK(cudaGetLastError());
+        fs = ctx->face_sum;
+        fn = ctx->face_nbr;
+        hold = ctx->hold;
+    }
     if (face_sum) {
         RET_IF(dalloc(ctx, &ctx->face_sum, (size_t)(LSP - 1) * ctx->npad));
         RET_IF(upload_rows(ctx, ctx->face_sum, face_sum, LSP - 1));
@@ -717,6 +746,7 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
     a.P = ctx->dP; a.rc = ctx->rc; a.rc32 = ctx->rc32; a.sour = ctx->sour;
     a.tile_flag = ctx->rc_prec == UC_MIXED ? ctx->tile_flag : nullptr; a.rho = ctx->rho; a.y0 = ctx->y0; a.soot0 = ctx->soot0;
     a.face_sum = fs; a.face_nbr = fn; a.y = ctx->y; a.soot = ctx->soot; a.partial = ctx->partial;
+    a.hold = hold;
     a.passes = ctx->passes;
     a.dt = dt; a.sor1 = relx; a.tol = tol; a.spnorm = spnorm > 0.0 ? spnorm : (double)ctx->n * (LSP - 1);
     a.isor = isor; a.n = ctx->n; a.npad = ctx->npad; a.ntile = ctx->ntile;
@@ -759,6 +789,8 @@ extern "C" int uc_sweep(uc_ctx *ctx, int precision, double dt, int isor, double 
     if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "uc_sweep before uc_upload_fields");
     if (precision != UC_FP64 && precision != UC_MIXED) return set_err(ctx, UC_E_ARG, "unknown precision %d", precision);
     RET_IF(props_impl(ctx, precision, nullptr, nullptr, nullptr));
+    if (ctx->have_grid && ctx->have_flow && !face_sum && !face_nbr)
+        RET_IF(uc_assemble_faces(ctx, dt, nullptr, nullptr, nullptr, nullptr));
     RET_IF(cp_h_impl(ctx, precision, nullptr, nullptr));
     CK(cudaSetDevice(ctx->device));
     RET_IF(launch_chem(ctx, precision, true, true));
@@ -857,6 +889,91 @@ extern "C" int uc_device_view_get(uc_ctx *ctx, uc_device_view *v)
     v->vmu = ctx->vmu; v->vtc = ctx->vtc; v->vdf = ctx->vdf; v->cp = ctx->cp; v->h = ctx->h;
     v->n = ctx->n; v->npad = ctx->npad;
     v->stream = (void *)ctx->stream;
+    return UC_OK;
+}
+
+// ------------------------------------------------------------------ species-equation faces
+
+static int upload_vec(uc_ctx *ctx, double **dst, const double *src, size_t n)
+{
+    RET_IF(dalloc(ctx, dst, n));
+    CK(cudaMemcpyAsync(*dst, src, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    return UC_OK;
+}
+
+extern "C" int uc_set_grid(uc_ctx *ctx, const uc_grid *g)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!g) {
+        ctx->have_grid = ctx->faces_ready = false;
+        return UC_OK;
+    }
+    if (g->lj < 3 || g->li < 3 || (long)g->lj * g->li != ctx->n || !g->xxs || !g->xxc || !g->yys || !g->yyc || !g->yr)
+        return set_err(ctx, UC_E_ARG, "uc_set_grid: the context's cells must be the lj x li grid (lj, li >= 3)");
+    CK(cudaSetDevice(ctx->device));
+    ctx->lj = g->lj;
+    ctx->li = g->li;
+    ctx->isym = g->isym;
+    RET_IF(upload_vec(ctx, &ctx->g_xxs, g->xxs, g->li));
+    RET_IF(upload_vec(ctx, &ctx->g_xxc, g->xxc, g->li));
+    RET_IF(upload_vec(ctx, &ctx->g_yys, g->yys, g->lj));
+    RET_IF(upload_vec(ctx, &ctx->g_yyc, g->yyc, g->lj));
+    RET_IF(dalloc(ctx, &ctx->g_yr, ctx->npad));
+    RET_IF(upload_rows(ctx, ctx->g_yr, g->yr, 1));
+    if (!ctx->hold) {
+        if (cudaMalloc((void **)&ctx->hold, ctx->npad) != cudaSuccess) { ctx->hold = nullptr; return set_err(ctx, UC_E_NOMEM, "hold mask"); }
+    }
+    hold_mask_kernel<<<ctx->nsm, 256, 0, ctx->stream>>>(g->lj, g->li, ctx->npad, ctx->hold);
+    CK(cudaGetLastError());
+    ctx->have_grid = true;
+    ctx->faces_ready = false;
+    return UC_OK;
+}
+
+extern "C" int uc_set_flow(uc_ctx *ctx, const double *u, const double *v, const double *tmu, double sigsp)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!u || !v || !tmu || !(sigsp > 0.0)) return set_err(ctx, UC_E_ARG, "uc_set_flow: u, v, tmu and sigsp > 0 are required");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(dalloc(ctx, &ctx->f_u, ctx->npad));
+    RET_IF(dalloc(ctx, &ctx->f_v, ctx->npad));
+    RET_IF(dalloc(ctx, &ctx->f_tmu, ctx->npad));
+    RET_IF(upload_rows(ctx, ctx->f_u, u, 1));
+    RET_IF(upload_rows(ctx, ctx->f_v, v, 1));
+    RET_IF(upload_rows(ctx, ctx->f_tmu, tmu, 1));
+    ctx->sigsp = sigsp;
+    ctx->have_flow = true;
+    return UC_OK;
+}
+
+extern "C" int uc_assemble_faces(uc_ctx *ctx, double dt, double *e, double *w, double *n, double *s)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->have_grid || !ctx->have_flow) return set_err(ctx, UC_E_STATE, "uc_set_grid and uc_set_flow first");
+    if (!ctx->vdf) return set_err(ctx, UC_E_STATE, "the faces need the diffusivities of uc_props");
+    CK(cudaSetDevice(ctx->device));
+    const size_t rows = (size_t)(LSP - 1) * ctx->npad;
+    RET_IF(dalloc(ctx, &ctx->fe, rows));
+    RET_IF(dalloc(ctx, &ctx->fw, rows));
+    RET_IF(dalloc(ctx, &ctx->fn, rows));
+    RET_IF(dalloc(ctx, &ctx->fs, rows));
+    if (!ctx->faces_ready)
+        for (double *b : {ctx->fe, ctx->fw, ctx->fn, ctx->fs}) CK(cudaMemsetAsync(b, 0, rows * sizeof(double), ctx->stream));
+    FaceArgs a{};
+    a.P = ctx->dP; a.lj = ctx->lj; a.li = ctx->li; a.npad = ctx->npad; a.isym = ctx->isym;
+    a.rho = ctx->rho; a.vdf = ctx->vdf; a.u = ctx->f_u; a.v = ctx->f_v; a.tmu = ctx->f_tmu; a.yr = ctx->g_yr;
+    a.xxs = ctx->g_xxs; a.xxc = ctx->g_xxc; a.yys = ctx->g_yys; a.yyc = ctx->g_yyc;
+    a.dt = dt; a.sigsp = ctx->sigsp; a.e = ctx->fe; a.w = ctx->fw; a.n = ctx->fn; a.s = ctx->fs;
+    faces_kernel<<<std::max(1, std::min((ctx->n + 127) / 128, ctx->nsm * 8)), 128, 0, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    ctx->faces_ready = true;
+    if (e || w || n || s) {
+        RET_IF(download_rows(ctx, e, ctx->fe, LSP - 1));
+        RET_IF(download_rows(ctx, w, ctx->fw, LSP - 1));
+        RET_IF(download_rows(ctx, n, ctx->fn, LSP - 1));
+        RET_IF(download_rows(ctx, s, ctx->fs, LSP - 1));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     return UC_OK;
 }
 

@@ -31,6 +31,7 @@ struct UpdArgs {
     const double *face_sum, *face_nbr;           // [51][npad] or null
     double *y, *soot;                            // updated in place
     const int *tile_flag;                        // update_kernel<float>: tiles whose RC is in the FP64 plane
+    const uint8_t *hold;                         // optional [npad]: cells that keep their state (grid boundary)
     double *partial;                             // [2][gridDim.x]
     int *passes;                                 // out: pass count as ISOR1 reports it
     double dt, sor1, tol, spnorm;
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
             const bool own = tile < a.ntile;            // warps without a tile repeat the last one, unstored
             if (!own) tile = a.ntile - 1;
             const size_t cell = (size_t)tile * TILE + lane;
-            const bool live = own && cell < (size_t)a.n;
+            const bool live = own && cell < (size_t)a.n && !(a.hold && a.hold[cell]);
             for (int k = 0; k < LSP - 1; ++k) syo[k * TILE] = a.y[k * np + cell];
             const double rho = a.rho[cell];
             double so[6];
@@ -231,6 +232,7 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
     // N2 closure and renormalisation (solvesp.f:2839-2915)
     for (size_t cell = (size_t)blockIdx.x * UPD_THREADS + threadIdx.x; cell < (size_t)a.n;
          cell += (size_t)gridDim.x * UPD_THREADS) {
+        if (a.hold && a.hold[cell]) continue;
         double ft = a.y[cell];
         for (int k = 1; k < LSP - 1; ++k) ft = ft + a.y[k * np + cell];
         ft = ft + a.soot[cell];

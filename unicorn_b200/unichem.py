@@ -58,6 +58,12 @@ DEFAULT_INPUTS = dict(rtin=0.0, rtot=0.100, vref=10.0, tref=294.0, pref=1.0133e5
 _lib = None
 
 
+class Grid(ctypes.Structure):
+    """uc_grid: the lj x li grid of the species-equation faces."""
+    _fields_ = [("lj", ctypes.c_int), ("li", ctypes.c_int), ("isym", ctypes.c_int)] + \
+               [(k, ctypes.POINTER(ctypes.c_double)) for k in ("xxs", "xxc", "yys", "yyc", "yr")]
+
+
 class IntegrateOpts(ctypes.Structure):
     """uc_integrate_opts: batched stiff integration settings."""
     _fields_ = [("dt", ctypes.c_double), ("isor", ctypes.c_int), ("relx", ctypes.c_double), ("tol", ctypes.c_double),
@@ -98,6 +104,9 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.uc_destroy.restype = None
     IP = ctypes.POINTER(ctypes.c_int)
     lib.uc_set_pressure.argtypes = [vp, P]
+    lib.uc_set_grid.argtypes = [vp, ctypes.POINTER(Grid)]
+    lib.uc_set_flow.argtypes = [vp, P, P, P, ctypes.c_double]
+    lib.uc_assemble_faces.argtypes = [vp, ctypes.c_double, P, P, P, P]
     lib.uc_hold_enthalpy.argtypes = [vp]
     lib.uc_temperature_from_held.argtypes = [vp]
     lib.uc_integrate.argtypes = [vp, ctypes.c_int, ctypes.POINTER(IntegrateOpts)]
@@ -272,6 +281,27 @@ class UniChem:
         self._ck(self.lib.uc_profile_read(self._h, _p(ms), cnt))
         names = ["chem", "update", "props", "cp_h", "temperature", "integrate"]
         return {nm: (float(ms[i]), int(cnt[i])) for i, nm in enumerate(names)}
+
+    # ------------------------------------------------------------ species-equation faces
+    def set_grid(self, lj: int, li: int, xxs, xxc, yys, yyc, yr, isym: int = 1):
+        """Grid of the face assembly (SPGSOLV geometry); the context's cells are the lj x li grid."""
+        arrs = [_in(a) for a in (xxs, xxc, yys, yyc, yr)]
+        self._grid_keep = arrs
+        g = Grid(int(lj), int(li), int(isym), *[_p(a) for a in arrs])
+        self._ck(self.lib.uc_set_grid(self._h, ctypes.byref(g)))
+
+    def clear_grid(self):
+        self._ck(self.lib.uc_set_grid(self._h, None))
+
+    def set_flow(self, u, v, tmu, sigsp: float = 0.7):
+        n = self.n
+        self._ck(self.lib.uc_set_flow(self._h, _p(_in(u, (n,))), _p(_in(v, (n,))), _p(_in(tmu, (n,))), sigsp))
+
+    def assemble_faces(self, dt: float):
+        """E, W, N, S [51, n] of the current state (uc_props must have run)."""
+        out = [np.empty((LSP - 1, self.n)) for _ in range(4)]
+        self._ck(self.lib.uc_assemble_faces(self._h, dt, *[_p(o) for o in out]))
+        return tuple(out)
 
     # ------------------------------------------------------------ batched integration
     @staticmethod
