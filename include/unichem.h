@@ -157,6 +157,16 @@ int uc_set_flow(uc_ctx *ctx, const double *u, const double *v, const double *tmu
 /* Assemble now (needs uc_props of the current state); e, w, n, s [51*n] host copies (may be NULL). */
 int uc_assemble_faces(uc_ctx *ctx, double dt, double *e, double *w, double *n, double *s);
 
+/* FDETAIL fields of the current state on the cell corners of the lj x li grid
+ * (the context's cells): out [218][n] in the order of the reference's record
+ * z, r, RHO, v, u, T, QDOT, VMU, VTC, CP, then Y_k, D_k, QDSP_k, h_k per species,
+ * dimensional as the reference writes them. x, y: node coordinates [n]; u, v [n].
+ * Needs omega and the properties of the state (after uc_sweep).
+ * Replaces: the field computation of SUBROUTINE STDATA, src/lib/stdata.f:26-118
+ * (the host writes the file; unicorn_b200/fdetail.py writes the reference's layout). */
+int uc_fdetail(uc_ctx *ctx, int lj, int li, const double *x, const double *y, const double *u,
+               const double *v, double *out);
+
 /* Outputs of the last uc_sweep/uc_omega/uc_props/uc_cp_h to the host (NULL = skip). */
 int uc_download_outputs(uc_ctx *ctx, double *qdsp, double *qdot, double *domega_dy, double *vmu,
                         double *vtc, double *vdf, double *cp, double *h);

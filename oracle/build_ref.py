@@ -17,6 +17,7 @@ Translated pieces (reference paths relative to the UNICORN checkout):
 * ``src/lib/spgsolv.f:98-232``  mixture cp (TCP probed per cell) -> f77_spgsolv_cp
 * ``src/lib/spgsolv.f:98-1290`` cp, EKT/EMU, face conductances and the
   E/W/N/S coefficients of the species equations    -> f77_spgsolv_coef
+* ``src/lib/stdata.f:26-118``   regular-grid fields, cp and h_k of FDETAIL -> f77_stdata_rg
 * ``src/unicornd-mild-sd-5.f:84-113`` DATA WSP/CDIA/TLJ/CI11      -> f77_main_data
 * ``src/unicornd-mild-sd-5.f:327-483`` set-up of tables/scales    -> f77_main_setup
 * ``src/unicornd-mild-sd-5.f:821-1006`` Y clip + transport props   -> f77_main_props
@@ -57,6 +58,7 @@ def build(ref: str, lj: int, li: int, out: Path = OUT) -> Path:
     ssp = build_units(str(src / "lib/solvesp.f"), ov)[0]
     sh = build_units(str(src / "lib/solveh.f"), ov)[0]
     spg = build_units(str(src / "lib/spgsolv.f"), ov)[0]
+    std = build_units(str(src / "lib/stdata.f"), ov)[0]
     main = [u for u in build_units(str(src / "unicornd-mild-sd-5.f"), ov_main) if u.kind == "program"][0]
     ncell = lj * li
     probe_cp = {173: f"F77P_TCP[(L_I-1)*{lj} + (L_J-1)] = L_TCP;"}
@@ -71,15 +73,16 @@ def build(ref: str, lj: int, li: int, out: Path = OUT) -> Path:
         (sh, "f77_solveh_temperature", [(34, 38), (1170, 1234)], None, None),
         (spg, "f77_spgsolv_cp", [(98, 232)], None, probe_cp),
         (spg, "f77_spgsolv_coef", [(98, 1290)], None, None),
+        (std, "f77_stdata_rg", [(26, 118)], None, None),
     ]
-    code = translate(frags, [data, ckr, ssp, sh, spg, main])
+    code = translate(frags, [data, ckr, ssp, sh, spg, std, main])
     code = code.replace("#include <string.h>", f"#include <string.h>\ndouble F77P_TCP[{ncell}];", 1)
     out.mkdir(parents=True, exist_ok=True)
     cfile = out / "unicorn_ref.c"
     cfile.write_text(code)
     # layout of COMMON variables (main program's view) and main locals for the driver
     layout = {"LJ": lj, "LI": li, "units": {}, "main_locals": {}, "args": {}}
-    for u in (main, ckr, ssp, sh, spg, data):
+    for u in (main, ckr, ssp, sh, spg, std, data):
         layout["units"][u.name] = {
             name: {"block": v.common, "offset": v.offset, "type": v.type, "dims": v.dims}
             for name, v in u.vars.items() if v.common}

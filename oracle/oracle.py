@@ -357,6 +357,13 @@ class Oracle:
                            ctypes.c_double(dt), ctypes.c_double(sigsp), *[_dptr(o) for o in out])
         return tuple(out)
 
+    def fdetail(self, lj, li, x, y, rho, u, v, tk, qdot, vmu, vtc, fsp, vdf, qdsp):
+        """FDETAIL fields [10 + 4*52, lj*li] (stdata.f:26-118)."""
+        out = np.zeros((10 + 4 * LSP, lj * li))
+        self.lib.orc_fdetail(lj, li, *[_dptr(_c(a)) for a in (x, y, rho, u, v, tk, qdot, vmu, vtc, fsp, vdf, qdsp)],
+                             _dptr(out))
+        return out
+
     def temperature(self, tk_guess, y, ht):
         tk = np.array(tk_guess, dtype=np.float64, copy=True)
         self.lib.orc_temperature(len(tk), _dptr(tk), _dptr(_c(y)), _dptr(_c(ht)))

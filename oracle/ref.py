@@ -331,3 +331,28 @@ class RefUnicorn:
             out.append(np.stack([self.var(S, face + self.SPECIES_SUFFIX[k]).reshape(-1, order="F")
                                  for k in range(LSP - 1)]))
         return tuple(o.copy() for o in out)
+
+    # -------------------------------------------------------------- FDETAIL fields
+    FD_NAMES = ["XRG", "YRG", "RHORG", "URG", "VRG", "TKRG", "QRG", "VMURG", "VTCRG", "CP"]
+
+    def stdata_fields(self, x, y, rho, u, v, tk, qdot, vmu, vtc, fsp, vdf, qdsp):
+        """lib/stdata.f:26-118 on the whole compile-time grid: returns [10 + 4*52, LJ*LI] in the
+        order of the FDETAIL record (10 scalars, then Y, D, QDSP, h of every species)."""
+        LJ, LI = self.LJ, self.LI
+        S = "STDATA"
+        sh = lambda a: np.asarray(a, dtype=np.float64).reshape(LJ, LI, order="F")
+        for nm, a in (("X", x), ("Y", y), ("RHO", rho), ("U", u), ("V", v), ("TK", tk), ("QDOT", qdot),
+                      ("VMU", vmu), ("VTC", vtc)):
+            self.var(S, nm)[:] = sh(a)
+        F, VD, Q = self.var(S, "FSP"), self.var(S, "VDF"), self.var(S, "QDSP")
+        for k in range(LSP):
+            F[:, :, k] = sh(fsp[k])
+            VD[:, :, k] = sh(vdf[k])
+            Q[:, :, k] = sh(qdsp[k])
+        self.lib.f77_stdata_rg()
+        rows = [self.var(S, nm).reshape(-1, order="F").copy() for nm in self.FD_NAMES]
+        FR, VR, QR, EN = (self.var(S, nm) for nm in ("FSPRG", "VDFRG", "QSPRG", "ENTH"))
+        for k in range(LSP):
+            for A in (FR, VR, QR, EN):
+                rows.append(A[:, :, k].reshape(-1, order="F").copy())
+        return np.stack(rows)

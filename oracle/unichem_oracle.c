@@ -936,3 +936,69 @@ void orc_faces(int lj, int li, const double *rho, const double *vdf, const doubl
 #undef CI
 #undef EMU
 }
+
+/* ------------------------------------------------------------- FDETAIL fields */
+
+/* stdata.f:26-118: corner averages of an lj x li grid (J fastest), the last
+ * row and column copied, dimensional scales; cp and h_k at the corner T.
+ * out [10 + 4*52][lj*li] in the order of the FDETAIL record. */
+void orc_fdetail(int lj, int li, const double *x, const double *y, const double *rho, const double *u,
+                 const double *v, const double *tk, const double *qdot, const double *vmu, const double *vtc,
+                 const double *fsp, const double *vdf, const double *qdsp, double *out)
+{
+    const size_t ne = (size_t)lj * li;
+    const double XSHIFT = 0.5 * (x[0] + x[lj]), YSHIFT = 0.5 * (y[0] + y[1]);
+#define O(r, p) out[(size_t)(r) * ne + (p)]
+    /* interior corners (stdata.f:1320-1326) */
+    for (int i = 0; i < li - 1; ++i)
+        for (int j = 0; j < lj - 1; ++j) {
+            const size_t c = (size_t)i * lj + j, cN = c + 1, cE = c + lj, cNE = c + lj + 1;
+            O(0, c) = (0.5 * (x[c] + x[cE]) - XSHIFT) * S.ALSTR;
+            O(1, c) = (0.5 * (y[c] + y[cN]) - YSHIFT) * S.ALSTR;
+            O(2, c) = 0.25 * (rho[c] + rho[cN] + rho[cE] + rho[cNE]) * S.RSTR;
+            O(5, c) = 0.25 * (tk[c] + tk[cN] + tk[cE] + tk[cNE]) * S.TSTR;
+            O(6, c) = 0.25 * (qdot[c] + qdot[cN] + qdot[cE] + qdot[cNE]);
+            O(7, c) = 0.25 * (vmu[c] + vmu[cN] + vmu[cE] + vmu[cNE]) * S.AMSTR;
+            O(8, c) = 0.25 * (vtc[c] + vtc[cN] + vtc[cE] + vtc[cNE]) * S.ACSTR;
+            O(3, c) = 0.5 * (u[cE] + u[cNE]) * S.VSTR;
+            O(4, c) = 0.5 * (v[cN] + v[cNE]) * S.VSTR;
+            double FTOT = 0.0;
+            for (int k = 0; k < LSP; ++k) {
+                const size_t kk = (size_t)k * ne;
+                O(10 + 4 * k + 1, c) = 0.25 * (vdf[kk + c] + vdf[kk + cN] + vdf[kk + cE] + vdf[kk + cNE]) * S.DSTR;
+                O(10 + 4 * k + 2, c) = 0.25 * (qdsp[kk + c] + qdsp[kk + cN] + qdsp[kk + cE] + qdsp[kk + cNE]);
+                if (k < LSP - 1) {
+                    O(10 + 4 * k, c) = 0.25 * (fsp[kk + c] + fsp[kk + cN] + fsp[kk + cE] + fsp[kk + cNE]);
+                    FTOT = FTOT + O(10 + 4 * k, c);
+                }
+            }
+            O(10 + 4 * (LSP - 1), c) = 1.0 - FTOT;
+        }
+    /* last row, then last column (stdata.f:1322-1325) */
+    for (int i = 0; i < li; ++i) {
+        const size_t p = (size_t)i * lj + (lj - 1), q = p - 1;
+        for (int r = 0; r < 10 + 4 * LSP; ++r) O(r, p) = O(r, q);
+        O(1, p) = y[p] * S.ALSTR;
+    }
+    for (int j = 0; j < lj; ++j) {
+        const size_t p = (size_t)(li - 1) * lj + j, q = p - lj;
+        for (int r = 0; r < 10 + 4 * LSP; ++r) O(r, p) = O(r, q);
+        O(0, p) = x[p] * S.ALSTR;
+    }
+    /* cp and h_k at the corner temperature (stdata.f:91-118) */
+    for (size_t p = 0; p < ne; ++p) {
+        const double TKD = O(5, p);
+        const double TKD2 = TKD * TKD, TKD3 = TKD * TKD2, TKD4 = TKD * TKD3, TKD5 = TKD * TKD4;
+        const int ip = TKD > T.tpol1 ? 7 : 0;
+        double TCP = 0.0;
+        for (int k = 0; k < LSP; ++k) {
+            const double *a = T.poly + k * 14 + ip;
+            TCP = TCP + (a[0] + a[1] * TKD + a[2] * TKD2 + a[3] * TKD3 + a[4] * TKD4) * O(10 + 4 * k, p) * S.GASC
+                        / S.WM[k] / S.WMSTR;
+            O(10 + 4 * k + 3, p) = (a[0] * TKD + a[1] * TKD2 / 2.0 + a[2] * TKD3 / 3.0 + a[3] * TKD4 / 4.0
+                                    + a[4] * TKD5 / 5.0 + a[5]) * S.GASC / S.WM[k] / S.WMSTR;
+        }
+        O(9, p) = TCP;
+    }
+#undef O
+}

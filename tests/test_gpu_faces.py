@@ -85,3 +85,30 @@ def test_sweep_with_faces_matches_oracle(cuda, oracle, case):
         u.sweep(dt, isor=4, tol=0.0)
         _, _, y_nf, _, _ = u.download()
     assert np.abs(y_nf - y_gpu)[:, inside].max() > 1e-6
+
+
+def test_fdetail_fields_match_oracle(cuda, oracle, case, tmp_path):
+    """uc_fdetail (regular-grid fields of stdata.f:26-118) after a sweep, against the oracle on
+    the same device state, and the file the writer makes of them."""
+    from unicorn_b200.fdetail import read_fdetail, write_fdetail
+    g = case
+    n = LJ * LI
+    rng = np.random.default_rng(9)
+    xs, ys = np.cumsum(rng.uniform(0.5, 1.5, LI)) / LJ, np.cumsum(rng.uniform(0.5, 1.5, LJ)) / LJ
+    x = np.tile(xs[None, :], (LJ, 1)).reshape(-1, order="F")
+    y = np.tile(ys[:, None], (1, LI)).reshape(-1, order="F")
+    with cuda.UniChem(n) as u:
+        u.upload(g["tk"], g["rho"], g["y"])
+        u.sweep(1e-3, isor=2, tol=0.0)
+        tk, rho, yy, _, _ = u.download()
+        out = {k: np.empty((52, n)) if k in ("qdsp", "vdf") else np.empty(n) for k in ("qdsp", "qdot", "vmu", "vtc", "vdf")}
+        u.download_outputs(out)
+        fd = u.fdetail(LJ, LI, x, y, g["u"], g["v"])
+    ref = oracle.fdetail(LJ, LI, x, y, rho, g["u"], g["v"], tk, out["qdot"], out["vmu"], out["vtc"], yy, out["vdf"],
+                         out["qdsp"])
+    scale = np.abs(ref).max(axis=1, keepdims=True)
+    assert np.all(np.abs(fd - ref) <= 1e-12 * np.abs(ref) + 1e-14 * scale)
+    p = tmp_path / "FDETAIL"
+    write_fdetail(p, fd, LJ, LI, itr=1, ttime=1e-5)
+    _, _, _, back = read_fdetail(p)
+    assert np.allclose(back, fd, rtol=5.1e-7, atol=0)

@@ -16,6 +16,7 @@
 #include "update_kernel.cuh"
 #include "integrate_kernel.cuh"
 #include "faces_kernel.cuh"
+#include "fdetail_kernel.cuh"
 #include "mlp_gemm.cuh"
 #include "mlp.cuh"
 
@@ -51,6 +52,7 @@ struct uc_ctx {
     double *fe = nullptr, *fw = nullptr, *fn = nullptr, *fs = nullptr;
     uint8_t *hold = nullptr;
     bool have_grid = false, have_flow = false, faces_ready = false;
+    double *fd_x = nullptr, *fd_y = nullptr, *fd_u = nullptr, *fd_v = nullptr, *fd_out = nullptr;
     // batched integration
     double *pnd = nullptr, *enth = nullptr;
     int *nsub = nullptr, *order = nullptr, *hist = nullptr, *next_tile = nullptr, *cpasses = nullptr;
@@ -328,7 +330,7 @@ static void free_ctx(uc_ctx *c)
         if (c->pnd) cudaFree(c->pnd);
         if (c->enth) cudaFree(c->enth);
         void *fb[] = {c->g_xxs, c->g_xxc, c->g_yys, c->g_yyc, c->g_yr, c->f_u, c->f_v, c->f_tmu,
-                      c->fe, c->fw, c->fn, c->fs, c->hold};
+                      c->fe, c->fw, c->fn, c->fs, c->hold, c->fd_x, c->fd_y, c->fd_u, c->fd_v, c->fd_out};
         for (void *b : fb)
             if (b) cudaFree(b);
         if (c->int_exec) cudaGraphExecDestroy(c->int_exec);
@@ -974,6 +976,41 @@ extern "C" int uc_assemble_faces(uc_ctx *ctx, double dt, double *e, double *w, d
         RET_IF(download_rows(ctx, s, ctx->fs, LSP - 1));
         CK(cudaStreamSynchronize(ctx->stream));
     }
+    return UC_OK;
+}
+
+// ------------------------------------------------------------------ FDETAIL fields
+
+extern "C" int uc_fdetail(uc_ctx *ctx, int lj, int li, const double *x, const double *y, const double *u,
+                          const double *v, double *out)
+{
+    if (!ctx) return UC_E_ARG;
+    if (lj < 2 || li < 2 || (long)lj * li != ctx->n || !x || !y || !u || !v || !out)
+        return set_err(ctx, UC_E_ARG, "uc_fdetail: the context's cells must be the lj x li grid; x, y, u, v, out required");
+    if (!ctx->qdsp || !ctx->qdot || !ctx->vmu || !ctx->vtc || !ctx->vdf)
+        return set_err(ctx, UC_E_STATE, "uc_fdetail needs omega and the properties of the state (uc_sweep)");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(dalloc(ctx, &ctx->fd_x, ctx->npad));
+    RET_IF(dalloc(ctx, &ctx->fd_y, ctx->npad));
+    RET_IF(dalloc(ctx, &ctx->fd_u, ctx->npad));
+    RET_IF(dalloc(ctx, &ctx->fd_v, ctx->npad));
+    RET_IF(dalloc(ctx, &ctx->fd_out, (size_t)FD_ROWS * ctx->npad));
+    RET_IF(upload_rows(ctx, ctx->fd_x, x, 1));
+    RET_IF(upload_rows(ctx, ctx->fd_y, y, 1));
+    RET_IF(upload_rows(ctx, ctx->fd_u, u, 1));
+    RET_IF(upload_rows(ctx, ctx->fd_v, v, 1));
+    FdArgs a{};
+    a.P = ctx->dP; a.lj = lj; a.li = li; a.npad = ctx->npad;
+    a.x = ctx->fd_x; a.y = ctx->fd_y; a.u = ctx->fd_u; a.v = ctx->fd_v;
+    a.rho = ctx->rho; a.tk = ctx->tk; a.qdot = ctx->qdot; a.vmu = ctx->vmu; a.vtc = ctx->vtc;
+    a.fsp = ctx->y; a.vdf = ctx->vdf; a.qdsp = ctx->qdsp;
+    a.ALSTR = ctx->sc.alstr; a.RSTR = ctx->sc.rstr; a.TSTR = ctx->sc.tstr; a.AMSTR = ctx->sc.amstr;
+    a.ACSTR = ctx->sc.acstr; a.VSTR = ctx->sc.vstr; a.DSTR = ctx->sc.dstr;
+    a.out = ctx->fd_out;
+    fdetail_kernel<<<std::max(1, std::min((ctx->n + 255) / 256, ctx->nsm * 8)), 256, 0, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    RET_IF(download_rows(ctx, out, ctx->fd_out, FD_ROWS));
+    CK(cudaStreamSynchronize(ctx->stream));
     return UC_OK;
 }
 

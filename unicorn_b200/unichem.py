@@ -107,6 +107,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.uc_set_grid.argtypes = [vp, ctypes.POINTER(Grid)]
     lib.uc_set_flow.argtypes = [vp, P, P, P, ctypes.c_double]
     lib.uc_assemble_faces.argtypes = [vp, ctypes.c_double, P, P, P, P]
+    lib.uc_fdetail.argtypes = [vp, ctypes.c_int, ctypes.c_int, P, P, P, P, P]
     lib.uc_hold_enthalpy.argtypes = [vp]
     lib.uc_temperature_from_held.argtypes = [vp]
     lib.uc_integrate.argtypes = [vp, ctypes.c_int, ctypes.POINTER(IntegrateOpts)]
@@ -302,6 +303,14 @@ class UniChem:
         out = [np.empty((LSP - 1, self.n)) for _ in range(4)]
         self._ck(self.lib.uc_assemble_faces(self._h, dt, *[_p(o) for o in out]))
         return tuple(out)
+
+    def fdetail(self, lj: int, li: int, x, y, u, v) -> np.ndarray:
+        """FDETAIL fields [218, n] of the current state (uc_fdetail)."""
+        n = self.n
+        out = np.empty((218, n))
+        self._ck(self.lib.uc_fdetail(self._h, int(lj), int(li), _p(_in(x, (n,))), _p(_in(y, (n,))),
+                                     _p(_in(u, (n,))), _p(_in(v, (n,))), _p(out)))
+        return out
 
     # ------------------------------------------------------------ batched integration
     @staticmethod
