@@ -112,3 +112,33 @@ def test_fdetail_fields_match_oracle(cuda, oracle, case, tmp_path):
     write_fdetail(p, fd, LJ, LI, itr=1, ttime=1e-5)
     _, _, _, back = read_fdetail(p)
     assert np.allclose(back, fd, rtol=5.1e-7, atol=0)
+
+
+def test_restart_round_trip_resumes(cuda, oracle, case, tmp_path):
+    """A device state saved in the reference's restart layout and loaded into a fresh context
+    gives the same next sweep (to the 8 digits the file keeps)."""
+    g = case
+    n = LJ * LI
+    flow = dict(X=np.zeros(n), Y=g["yr"], U=g["u"], V=g["v"], W=np.zeros(n), P=np.zeros(n))
+    with cuda.UniChem(n) as u:
+        u.upload(g["tk"], g["rho"], g["y"])
+        u.sweep(1e-3, isor=3, tol=0.0)
+        u.save_restart(tmp_path / "FLAMEA", LJ, LI, flow, infuel=11, itr=1)
+        tk_s, rho_s, y_s, _, _ = u.download()
+        y_saved = (tk_s, rho_s, y_s)
+        u.sweep(1e-3, isor=3, tol=0.0)
+        _, _, y_a, _, _ = u.download()
+    with cuda.UniChem(n) as u2:
+        h, f = u2.load_restart(tmp_path / "FLAMEA")
+        assert (h["LJ"], h["LI"]) == (LJ, LI) and np.allclose(f["U"], g["u"], rtol=5.1e-8)
+        tk_l, rho_l, y_l, _, _ = u2.download()
+        assert np.allclose(tk_l, y_saved[0], rtol=5.1e-8, atol=0) and np.allclose(rho_l, y_saved[1], rtol=5.1e-8, atol=0)
+        assert np.allclose(y_l[:51], y_saved[2][:51], rtol=5.1e-8, atol=0)
+        u2.sweep(1e-3, isor=3, tol=0.0)
+        _, _, y_b, _, _ = u2.download()
+    # the continuation from the 8-digit state: almost every value to 1e-6 relative; values near
+    # zero can land on either side of the update's clip at 0, so the bound for all is absolute
+    big = y_a > 1e-10
+    rel = np.abs(y_b - y_a)[big] / y_a[big]
+    assert np.mean(rel <= 1e-6) > 0.999, np.mean(rel <= 1e-6)
+    assert np.abs(y_b - y_a).max() <= 1e-6

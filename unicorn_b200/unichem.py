@@ -312,6 +312,27 @@ class UniChem:
                                      _p(_in(u, (n,))), _p(_in(v, (n,))), _p(out)))
         return out
 
+    # ------------------------------------------------------------ restart files
+    def save_restart(self, path, lj: int, li: int, flow: dict, **header):
+        """Write the device state (RHO, FSP, TK, QDOT, STMF, STND) with the host's grid and flow
+        fields (flow: X, Y, U, V, W, P and, with iflow=2, AK, EPS) as a restart file."""
+        from .restart import write_restart
+        tk, rho, y, s1, s2 = self.download()
+        qd = np.zeros(self.n)
+        if self.lib.uc_download_outputs(self._h, None, _p(qd), None, None, None, None, None, None) != 0:
+            qd[:] = 0.0                      # no omega computed yet: QDOT is written as zero
+        f = dict(flow, RHO=rho, FSP=y, TK=tk, QDOT=qd, STMF=s1, STND=s2)
+        write_restart(path, f, self.scales, lj, li, **header)
+
+    def load_restart(self, path) -> tuple[dict, dict]:
+        """Read a restart file, upload its state (TK, RHO, FSP, STMF, STND); returns (header, fields)."""
+        from .restart import read_restart
+        h, f = read_restart(path)
+        if h["LI"] * h["LJ"] != self.n:
+            raise ValueError(f"restart grid {h['LJ']}x{h['LI']} does not match {self.n} cells")
+        self.upload(f["TK"], f["RHO"], f["FSP"], f["STMF"], f["STND"])
+        return h, f
+
     # ------------------------------------------------------------ batched integration
     @staticmethod
     def integrate_opts(dt: float, isor: int = 100, relx: float = 0.99, tol: float = 1e-8, c_tau: float = 1.0,
