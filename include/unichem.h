@@ -157,6 +157,55 @@ int uc_set_flow(uc_ctx *ctx, const double *u, const double *v, const double *tmu
 /* Assemble now (needs uc_props of the current state); e, w, n, s [51*n] host copies (may be NULL). */
 int uc_assemble_faces(uc_ctx *ctx, double dt, double *e, double *w, double *n, double *s);
 
+/* ---------------------------------------------------------------------------
+ * The enthalpy equation on the device.
+ * Replaces: CALL SOLVEH(ISOR2,RELXH,TOLRH,SIGSP,HNORM) at src/lib/spgsolv.f:1298
+ * (src/lib/solveh.f:34-1234) with the enthalpy coefficients of SPGSOLV
+ * (EKT spgsolv.f:174; ZE, ZW, ZN, ZS of spgsolv.f:240-1290) and the
+ * HT := FPZ copy and residual RESDH of spgsolv.f:1299-1415.
+ *
+ * uc_set_enthalpy uploads HT [n] (the reference's non-dimensional FPZ/HT) and
+ * the swirl velocity W [n] of the kinetic-energy term (NULL: none).
+ * uc_enthalpy_update runs, after a uc_sweep (whose species update leaves the
+ * rate plane of its start state, the properties and cp on the device) and on
+ * the grid and flow of uc_set_grid / uc_set_flow (SIGSP of the flow is the
+ * SIGSP of RDHSP):
+ *  - QDSP and QDOT from the start-state rates and the updated Y, overwriting
+ *    the context's omega as SOLVEH overwrites /DUMD/ and /HRLS/ (interior cells);
+ *  - RHSZ: species-enthalpy diffusion, radiation of CH4, CO2, CO, H2O and soot
+ *    (40%, with the soot mass fraction of the start of the update), RHO HT and
+ *    DT PROD; coefficients from EKT = REI (BETA2 VTC/TCP + TMU/SIGH);
+ *  - up to isor relaxation passes over the interior cells in the reference's
+ *    lexicographic Gauss-Seidel order (J outer, I inner: the same iterates),
+ *    until sum|dFPZ| / hnorm <= tol (hnorm <= 0 means lj*li, the reference's LE);
+ *  - T of the interior cells from FPZ less (U^2+V^2+W^2)/2 by the Newton of
+ *    solveh.f:1170-1234, then HT := FPZ.
+ * passes receives ISOR2 as the reference returns it (the converging pass, or
+ * isor + 1); resdh = sum|FPZ - HT| / hnorm. At most 1024 interior rows (lj - 2).
+ * Returns UC_E_NOCONV (not fatal) when a cell's Newton did not converge and
+ * UC_E_TIMEOUT when a bounded wait between passes gave up. */
+typedef struct {
+    double dt;      /* DT */
+    int isor;       /* ISOR2: passes at most */
+    double relx;    /* RELXH */
+    double tol;     /* TOLRH */
+    double hnorm;   /* HNORM (<= 0: lj*li) */
+    double sigh;    /* SIGH of EKT */
+} uc_enthalpy_opts;
+int uc_set_enthalpy(uc_ctx *ctx, const double *ht, const double *w);
+int uc_enthalpy_update(uc_ctx *ctx, const uc_enthalpy_opts *o, int *passes, double *resdh);
+/* HT [n] and the last update's RHSZ, ZE, ZW, ZN, ZS [n] to the host (NULL = skip). */
+int uc_enthalpy_get(uc_ctx *ctx, double *ht, double *rhsz, double *ze, double *zw, double *zn, double *zs);
+
+/* The relaxation alone, on host arrays of an lj x li grid (J fastest):
+ * fpz [lj*li] holds HT on entry and FPZ on return; rho, rhsz and the
+ * coefficients ze, zw, zn, zs are read on the interior cells. Same ordering,
+ * rounding and pass count as the loop of solveh.f:1146-1167.
+ * Replaces: src/lib/solveh.f:1146-1167. */
+int uc_enthalpy_relax(int device, int lj, int li, const double *rho, const double *rhsz, const double *ze,
+                      const double *zw, const double *zn, const double *zs, double *fpz, int isor, double relx,
+                      double tol, double hnorm, int *passes);
+
 /* FDETAIL fields of the current state on the cell corners of the lj x li grid
  * (the context's cells): out [218][n] in the order of the reference's record
  * z, r, RHO, v, u, T, QDOT, VMU, VTC, CP, then Y_k, D_k, QDSP_k, h_k per species,
@@ -181,7 +230,8 @@ int uc_download_outputs(uc_ctx *ctx, double *qdsp, double *qdot, double *domega_
 #define UC_K_CPH 3
 #define UC_K_TEMP 4
 #define UC_K_INTEGRATE 5   /* one uc_integrate graph launch */
-#define UC_K_COUNT 6
+#define UC_K_ENTHALPY 6    /* one uc_enthalpy_update (all its kernels) */
+#define UC_K_COUNT 7
 int uc_profile(uc_ctx *ctx, int on);
 int uc_profile_read(uc_ctx *ctx, double *ms, int *launches);
 

@@ -18,6 +18,10 @@ Translated pieces (reference paths relative to the UNICORN checkout):
 * ``src/lib/spgsolv.f:98-1290`` cp, EKT/EMU, face conductances and the
   E/W/N/S coefficients of the species equations    -> f77_spgsolv_coef
 * ``src/lib/stdata.f:26-118``   regular-grid fields, cp and h_k of FDETAIL -> f77_stdata_rg
+* ``src/lib/solveh.f:34-1145``  enthalpy-equation right-hand side (species
+  enthalpy diffusion, radiation, heat release)     -> f77_solveh_rhs
+* ``src/lib/solveh.f:34-1234``  the whole of SOLVEH: right-hand side, point
+  relaxation of FPZ and the temperature from it   -> f77_solveh_full
 * ``src/unicornd-mild-sd-5.f:84-113`` DATA WSP/CDIA/TLJ/CI11      -> f77_main_data
 * ``src/unicornd-mild-sd-5.f:327-483`` set-up of tables/scales    -> f77_main_setup
 * ``src/unicornd-mild-sd-5.f:821-1006`` Y clip + transport props   -> f77_main_props
@@ -74,6 +78,8 @@ def build(ref: str, lj: int, li: int, out: Path = OUT) -> Path:
         (spg, "f77_spgsolv_cp", [(98, 232)], None, probe_cp),
         (spg, "f77_spgsolv_coef", [(98, 1290)], None, None),
         (std, "f77_stdata_rg", [(26, 118)], None, None),
+        (sh, "f77_solveh_rhs", [(34, 1145)], None, None),
+        (sh, "f77_solveh_full", [(34, 1234)], None, None),
     ]
     code = translate(frags, [data, ckr, ssp, sh, spg, std, main])
     code = code.replace("#include <string.h>", f"#include <string.h>\ndouble F77P_TCP[{ncell}];", 1)

@@ -357,6 +357,55 @@ class Oracle:
                            ctypes.c_double(dt), ctypes.c_double(sigsp), *[_dptr(o) for o in out])
         return tuple(out)
 
+    def zfaces(self, lj, li, rho, tcp, vtc, tmu, u, v, yr, xxs, xxc, yys, yyc, isym=1, dt=1e-3, sigh=0.9):
+        """Enthalpy-equation coefficients (ze, zw, zn, zs) [lj*li] of the interior cells and EKT [lj*li]."""
+        ne = lj * li
+        out = [np.zeros(ne) for _ in range(5)]
+        self.lib.orc_zfaces(lj, li, *[_dptr(_c(a)) for a in (rho, tcp, vtc, tmu, u, v, yr, xxs, xxc, yys, yyc)],
+                            int(isym), ctypes.c_double(dt), ctypes.c_double(sigh), *[_dptr(o) for o in out])
+        return tuple(out[:4]), out[4]
+
+    def enthalpy_rhs(self, lj, li, tk, rho, y_new, ht, stmf, vdf, tmu, ekt, rc, yr, xxs, xxc, yys, yyc, isym=1,
+                     dt=1e-3, sigsp=0.9):
+        """Enthalpy right-hand side RHSZ [lj*li], QDSP [52][lj*li] and QDOT [lj*li] of the interior cells
+        (zero elsewhere); rc [544][lj*li] is the start-state rate table."""
+        ne = lj * li
+        rhsz, qdsp, qdot = np.zeros(ne), np.zeros((LSP, ne)), np.zeros(ne)
+        self.lib.orc_enthalpy_rhs(lj, li, *[_dptr(_c(a)) for a in (tk, rho, y_new, ht, stmf, vdf, tmu, ekt, rc, yr,
+                                                                    xxs, xxc, yys, yyc)],
+                                  int(isym), ctypes.c_double(dt), ctypes.c_double(sigsp), _dptr(rhsz), _dptr(qdsp),
+                                  _dptr(qdot))
+        return rhsz, qdsp, qdot
+
+    def enthalpy_relax(self, lj, li, rho, rhsz, z, ht, isor=100, relx=0.99, tol=1e-8, hnorm=None):
+        """FPZ after the point relaxation (starting from ht) and the pass count the reference reports."""
+        fpz = np.array(ht, dtype=np.float64, copy=True)
+        self.lib.orc_enthalpy_relax.restype = ctypes.c_int
+        passes = self.lib.orc_enthalpy_relax(lj, li, *[_dptr(_c(a)) for a in (rho, rhsz, *z)], _dptr(fpz), int(isor),
+                                             ctypes.c_double(relx), ctypes.c_double(tol),
+                                             ctypes.c_double(float(lj * li) if hnorm is None else hnorm))
+        return fpz, passes
+
+    def temperature_ke(self, lj, li, tk, y, fpz, u, v, w=None):
+        """Temperature of the interior cells from FPZ less the kinetic energy (guess: tk)."""
+        t = np.array(tk, dtype=np.float64, copy=True)
+        self.lib.orc_temperature_ke(lj, li, _dptr(t), _dptr(_c(y)), _dptr(_c(fpz)), _dptr(_c(u)), _dptr(_c(v)),
+                                    None if w is None else _dptr(_c(w)))
+        return t
+
+    def enthalpy_solve(self, lj, li, tk, rho, y_start, y_new, ht, stmf, vtc, vdf, u, v, tmu, yr, xxs, xxc, yys, yyc,
+                       w=None, isym=1, dt=1e-3, sigsp=0.9, sigh=0.9, isor=100, relx=0.99, tol=1e-8, hnorm=None):
+        """The whole enthalpy step (SPGSOLV's EKT and Z, SOLVEH): returns a dict with fpz, tk, passes,
+        rhsz, z, qdsp, qdot. Start state: tk, rho, y_start (rates, cp); y_new: after the species update."""
+        tcp = self.cp(tk, y_start)
+        z, ekt = self.zfaces(lj, li, rho, tcp, vtc, tmu, u, v, yr, xxs, xxc, yys, yyc, isym=isym, dt=dt, sigh=sigh)
+        rc, _ = self.rates(tk, rho, y_start)
+        rhsz, qdsp, qdot = self.enthalpy_rhs(lj, li, tk, rho, y_new, ht, stmf, vdf, tmu, ekt, rc, yr, xxs, xxc, yys,
+                                             yyc, isym=isym, dt=dt, sigsp=sigsp)
+        fpz, passes = self.enthalpy_relax(lj, li, rho, rhsz, z, ht, isor=isor, relx=relx, tol=tol, hnorm=hnorm)
+        tk_new = self.temperature_ke(lj, li, tk, y_new, fpz, u, v, w)
+        return dict(fpz=fpz, tk=tk_new, passes=passes, rhsz=rhsz, z=z, qdsp=qdsp, qdot=qdot, ekt=ekt)
+
     def fdetail(self, lj, li, x, y, rho, u, v, tk, qdot, vmu, vtc, fsp, vdf, qdsp):
         """FDETAIL fields [10 + 4*52, lj*li] (stdata.f:26-118)."""
         out = np.zeros((10 + 4 * LSP, lj * li))

@@ -356,3 +356,59 @@ class RefUnicorn:
             for A in (FR, VR, QR, EN):
                 rows.append(A[:, :, k].reshape(-1, order="F").copy())
         return np.stack(rows)
+
+    # -------------------------------------------------------------- SOLVEH enthalpy equation
+    def enthalpy_rhs(self, tk, rho, y_start, y_new, ht, stmf, vtc, vdf, u, v, tmu, xxs, xxc, yys, yyc, yr,
+                     isym=1, dt=1e-3, sigsp=0.9, sigh=0.9):
+        """SPGSOLV's assembly (spgsolv.f:98-1290: EKT, EMU and the enthalpy coefficients ZE..ZS),
+        CKRATES at the start state, then lib/solveh.f:34-1145 with SSP = y_new: returns
+        (rhsz, (ze, zw, zn, zs), qdsp [52], qdot) on the whole compile-time grid."""
+        n = self.LJ * self.LI
+        self.spgsolv_coefficients(tk, rho, y_start, vtc, vdf, u, v, tmu, np.zeros(n), xxs, xxc, yys, yyc, yr,
+                                  isym=isym, dt=dt, sigsp=sigsp, sigh=sigh)
+        z = tuple(self.var("SPGSOLV", nm).reshape(-1, order="F").copy() for nm in ("ZE", "ZW", "ZN", "ZS"))
+        self.lib.f77_ckrates()
+        H = "SOLVEH"
+        SSP = self.var(H, "SSP")
+        SSP[:, :] = np.asarray(y_new, dtype=np.float64).T
+        self.var(H, "HT")[:] = np.asarray(ht, dtype=np.float64).reshape(self.LJ, self.LI, order="F")
+        self.var(H, "STMF")[:] = np.asarray(stmf, dtype=np.float64).reshape(self.LJ, self.LI, order="F")
+        self.scalar(H, "RSOOT", 1.9e3)
+        self.var(H, "ISKIP")[:] = 0
+        ctypes.c_double.in_dll(self.lib, "F77A_SOLVEH_SIGSP").value = sigsp
+        self.lib.f77_solveh_rhs()
+        rhsz = self.var(H, "RHSZ").reshape(-1, order="F").copy()
+        q = self.var(H, "QDSP")
+        qdsp = np.stack([q[:, :, k].reshape(-1, order="F") for k in range(LSP)])
+        qdot = self.var(H, "QDOT").reshape(-1, order="F").copy()
+        return rhsz, z, qdsp, qdot
+
+    def enthalpy_solve(self, tk, rho, y_start, y_new, ht, stmf, vtc, vdf, u, v, tmu, xxs, xxc, yys, yyc, yr,
+                       w=None, isym=1, dt=1e-3, sigsp=0.9, sigh=0.9, isor=100, relx=0.99, tol=1e-8, hnorm=None):
+        """SPGSOLV's assembly with FPZ = HT (spgsolv.f:98-1290), CKRATES at the start state, then the
+        whole of SOLVEH (lib/solveh.f:34-1234) with SSP = y_new. Returns a dict with fpz, tk, passes
+        (ISOR2 on return), rhsz, qdsp, qdot on the whole compile-time grid."""
+        n = self.LJ * self.LI
+        sh = lambda a: np.asarray(a, dtype=np.float64).reshape(self.LJ, self.LI, order="F")
+        S = "SPGSOLV"
+        self.var(S, "HT")[:] = sh(ht)
+        self.var(S, "W")[:] = sh(np.zeros(n) if w is None else w)
+        self.spgsolv_coefficients(tk, rho, y_start, vtc, vdf, u, v, tmu, np.zeros(n), xxs, xxc, yys, yyc, yr,
+                                  isym=isym, dt=dt, sigsp=sigsp, sigh=sigh)
+        self.lib.f77_ckrates()
+        H = "SOLVEH"
+        self.var(H, "SSP")[:, :] = np.asarray(y_new, dtype=np.float64).T
+        self.var(H, "STMF")[:] = sh(stmf)
+        self.scalar(H, "RSOOT", 1.9e3)
+        self.var(H, "ISKIP")[:] = 0
+        ctypes.c_double.in_dll(self.lib, "F77A_SOLVEH_SIGSP").value = sigsp
+        ctypes.c_double.in_dll(self.lib, "F77A_SOLVEH_RELXH").value = relx
+        ctypes.c_double.in_dll(self.lib, "F77A_SOLVEH_TOLRH").value = tol
+        ctypes.c_double.in_dll(self.lib, "F77A_SOLVEH_HNORM").value = float(n) if hnorm is None else hnorm
+        ctypes.c_int.in_dll(self.lib, "F77A_SOLVEH_ISOR2").value = isor
+        self.lib.f77_solveh_full()
+        flat = lambda nm: self.var(H, nm).reshape(-1, order="F").copy()
+        q = self.var(H, "QDSP")
+        return dict(fpz=flat("FPZ"), tk=flat("TK"), passes=ctypes.c_int.in_dll(self.lib, "F77A_SOLVEH_ISOR2").value,
+                    rhsz=flat("RHSZ"), qdsp=np.stack([q[:, :, k].reshape(-1, order="F") for k in range(LSP)]),
+                    qdot=flat("QDOT"))

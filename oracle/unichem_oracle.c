@@ -1002,3 +1002,189 @@ void orc_fdetail(int lj, int li, const double *x, const double *y, const double 
     }
 #undef O
 }
+
+/* ------------------------------------------------------------- enthalpy equation */
+
+static inline double powi5(double x) { double t = x * x; double u = t * x; return u * t; }
+
+/* Enthalpy-equation coefficients ZE, ZW, ZN, ZS (spgsolv.f:233-348 and the
+ * Z lines of :350-1290) and EKT = REI (BETA2 VTC/TCP + TMU/SIGH)
+ * (spgsolv.f:174) of every cell; tcp is the mixture cp of orc_cp. */
+void orc_zfaces(int lj, int li, const double *rho, const double *tcp, const double *vtc, const double *tmu,
+                const double *u, const double *v, const double *yr, const double *xxs, const double *xxc,
+                const double *yys, const double *yyc, int isym, double dt, double sigh, double *ze, double *zw,
+                double *zn, double *zs, double *ekt)
+{
+    const size_t ne = (size_t)lj * li;
+    const double SYM = (double)isym;
+    for (size_t c = 0; c < ne; ++c) ekt[c] = S.REI * (S.BETA2 * vtc[c] / tcp[c] + tmu[c] / sigh);
+#define CI(j, i) ((size_t)(i) * lj + (j))
+    for (int i = 1; i < li - 1; ++i)
+        for (int j = 1; j < lj - 1; ++j) {
+            const size_t c = CI(j, i);
+            const double DTBRX = dt / xxc[i], DTBRY = dt / yyc[j];
+            const double RHOUE = 0.5 * (rho[CI(j, i + 1)] + rho[c]) * u[CI(j, i + 1)];
+            const double RHOUW = 0.5 * (rho[c] + rho[CI(j, i - 1)]) * u[c];
+            const double RHOVN = 0.5 * (rho[CI(j + 1, i)] + rho[c]) * v[CI(j + 1, i)];
+            const double RHOVS = 0.5 * (rho[c] + rho[CI(j - 1, i)]) * v[c];
+            const double SYMZ = SYM * dt * 0.5 * ekt[c] / yr[c];
+            const double DE = (ekt[CI(j, i + 1)] + ekt[c]) / xxs[i + 1];
+            const double DW = (ekt[c] + ekt[CI(j, i - 1)]) / xxs[i];
+            const double DN = (ekt[CI(j + 1, i)] + ekt[c]) / yys[j + 1];
+            const double DS = (ekt[c] + ekt[CI(j - 1, i)]) / yys[j];
+            double cv;
+            cv = fabs(RHOUE); if (DE >= cv) cv = DE;
+            ze[c] = DTBRX * 0.5 * (RHOUE - cv);
+            cv = fabs(RHOUW); if (DW >= cv) cv = DW;
+            zw[c] = DTBRX * 0.5 * (-RHOUW - cv);
+            cv = fabs(RHOVN); if (DN >= cv) cv = DN;
+            zn[c] = DTBRY * 0.5 * (RHOVN - cv) - SYMZ / yys[j + 1];
+            cv = fabs(RHOVS); if (DS >= cv) cv = DS;
+            zs[c] = DTBRY * 0.5 * (-RHOVS - cv) + SYMZ / yys[j];
+        }
+    (void)ne;
+}
+
+/* Right-hand side of the enthalpy equation (solveh.f:34-1145) for the
+ * interior cells: species-enthalpy diffusion (RDHSP of every cell), the
+ * radiation loss of CH4, CO2, CO, H2O and soot, RHO HT and the heat release
+ * DT PROD from RA = RC (start state) x Y (after the species update); also
+ * QDSP and QDOT of that state. y_new [52][n]; rc [544][n]. */
+void orc_enthalpy_rhs(int lj, int li, const double *tk, const double *rho, const double *y_new, const double *ht,
+                      const double *stmf, const double *vdf, const double *tmu, const double *ekt, const double *rc,
+                      const double *yr, const double *xxs, const double *xxc, const double *yys, const double *yyc,
+                      int isym, double dt, double sigsp, double *rhsz, double *qdsp, double *qdot)
+{
+    const size_t ne = (size_t)lj * li;
+    const double SYM = (double)isym, HCONVR = S.GASC / S.WMSTR / S.HSTR;
+    const double CRAD = S.ALSTR / S.RSTR / S.VSTR / S.VSTR / S.VSTR;
+    const double RCONV = S.VSTR / S.WMSTR / S.ALSTR * 1.0e-06;
+    const double RSOOT = 1.9000e+03;
+    double *RDHSP = (double *)malloc(ne * LSP * sizeof(double));
+    double *HENTH = (double *)malloc(ne * LSP * sizeof(double));
+    /* solveh.f:39-57 */
+    for (size_t c = 0; c < ne; ++c) {
+        const double TKD = tk[c] * S.TSTR;
+        const double TKD2 = TKD * TKD, TKD3 = TKD * TKD2, TKD4 = TKD * TKD3, TKD5 = TKD * TKD4;
+        const int ip = TKD > T.tpol1 ? 7 : 0;
+        const double EMU = S.REI * S.BETA3 * rho[c];
+        for (int k = 0; k < LSP; ++k) {
+            const double *a = T.poly + k * 14 + ip;
+            const double HSSP = (a[0] * TKD + a[1] * TKD2 / 2.0 + a[2] * TKD3 / 3.0 + a[3] * TKD4 / 4.0
+                                 + a[4] * TKD5 / 5.0) / S.WM[k] * HCONVR;
+            RDHSP[(size_t)k * ne + c] = (EMU * vdf[(size_t)k * ne + c] + S.REI * tmu[c] / sigsp - ekt[c]) * HSSP;
+            HENTH[(size_t)k * ne + c] = HSSP * S.WMSTR * S.HSTR + a[5] / S.WM[k] * S.GASC;
+        }
+    }
+#define CI(j, i) ((size_t)(i) * lj + (j))
+#define RD(k, p) RDHSP[(size_t)(k) * ne + (p)]
+#define YS(k, p) y_new[(size_t)(k) * ne + (p)]
+    /* solveh.f:59-115 */
+    for (int j = 1; j < lj - 1; ++j)
+        for (int i = 1; i < li - 1; ++i) {
+            const size_t c = CI(j, i), cE = c + lj, cW = c - lj, cN = c + 1, cS = c - 1;
+            double RDHE = 0.0, RDHW = 0.0, RDHN = 0.0, RDHS = 0.0, RDHP = 0.0, TMOLE = 0.0;
+            for (int k = 0; k < LSP; ++k) {
+                TMOLE = TMOLE + YS(k, c) / S.WM[k];
+                RDHE = RDHE + (RD(k, cE) + RD(k, c)) * (YS(k, cE) - YS(k, c));
+                RDHW = RDHW + (RD(k, c) + RD(k, cW)) * (YS(k, c) - YS(k, cW));
+                RDHN = RDHN + (RD(k, cN) + RD(k, c)) * (YS(k, cN) - YS(k, c));
+                RDHS = RDHS + (RD(k, c) + RD(k, cS)) * (YS(k, c) - YS(k, cS));
+                RDHP = RDHP + (RD(k, c)) * (YS(k, cN) - YS(k, cS));
+            }
+            const double TKD = tk[c] * S.TSTR;
+            const double TKDI = 1000.0 / TKD, TKDIS = TKDI * TKDI;
+            const double PLANK1 = F(6.6334) + TKD * (-3.5686e-03 + TKD * (1.6682e-08 + TKD * (2.5611e-10 - 2.6558e-14 * TKD)));
+            const double PLANK2 = 1.8741e+01 - TKDI * (1.2131e+02 - 2.7350e+02 * TKDI + 1.9405e+02 * TKDIS
+                                                      - 5.6310e+01 * TKDIS * TKDI + F(5.81690) * TKDIS * TKDIS);
+            double PLANK3;
+            if (TKD <= F(750.0))
+                PLANK3 = F(4.7869) + TKD * (-6.953e-02 + TKD * (2.95775e-04 + TKD * (-4.25732e-07 + 2.02894e-10 * TKD)));
+            else
+                PLANK3 = 1.009e+01 + TKD * (-1.183e-02 + TKD * (4.7753e-06 + TKD * (-5.87209e-10 - 2.5334e-14 * TKD)));
+            const double PLANK4 = -F(0.23093) - TKDI * (F(1.12390) - F(9.41530) * TKDI + F(2.99880) * TKDIS
+                                                       - F(0.51382) * TKDIS * TKDI + 1.86840e-05 * TKDIS * TKDIS);
+            const double PLANKC = (PLANK1 * YS(12, c) / S.WM[12] + PLANK2 * YS(9, c) / S.WM[9]
+                                   + PLANK3 * YS(8, c) / S.WM[8] + PLANK4 * YS(5, c) / S.WM[5]) / TMOLE;
+            const double QRAD = CRAD * F(0.4) * (F(4.0) * 5.669e-08 * PLANKC * (pow(TKD, F(4.0)) - 8.1e+09)
+                                                + 3.334e-04 * stmf[c] * (rho[c] / RSOOT) * powi5(TKD));
+            rhsz[c] = dt * F(0.5) * ((RDHE / xxs[i + 1] - RDHW / xxs[i]) / xxc[i]
+                                     + (RDHN / yys[j + 1] - RDHS / yys[j]) / yyc[j]
+                                     + SYM * RDHP / yr[c] / yyc[j]) - QRAD * dt;
+        }
+    /* solveh.f:117-1145 */
+    double RA[LRX], PRD[LSP], yc[LSP], rcc[LRX], so0[6] = {0, 0, 0, 0, 0, 0};
+    for (int j = 1; j < lj - 1; ++j)
+        for (int i = 1; i < li - 1; ++i) {
+            const size_t c = CI(j, i);
+            for (int k = 0; k < LSP; ++k) yc[k] = YS(k, c);
+            for (int r = 0; r < LRX; ++r) rcc[r] = rc[(size_t)r * ne + c];
+            for (int r = 0; r < LRX; ++r) {
+                if (!T.ra_has[r]) { RA[r] = 0.0; continue; }
+                double v = rcc[r];
+                for (int t = 0; t < T.ra_len[r]; ++t) v = v * yc[T.ra_sp[T.ra_off[r] + t]];
+                RA[r] = v;
+            }
+            double PROD = 0.0, HRR = 0.0;
+            for (int k = 0; k < LSP; ++k) {
+                PRD[k] = T.prd_has[k] ? S.WM[k] * S.HFO[k] * sum_terms(T.prd_off[k], T.prd_len[k], NULL, rcc, yc, NULL,
+                                                                       so0, RA) : 0.0;
+            }
+            for (int k = 0; k < LSP; ++k) {
+                PROD = PROD + PRD[k];
+                HRR = HRR + PRD[k] * HENTH[(size_t)k * ne + c] / S.HFO[k];
+                if (qdsp) qdsp[(size_t)k * ne + c] = -(RCONV * PRD[k] / S.HFO[k]);
+            }
+            rhsz[c] = rhsz[c] + rho[c] * ht[c] - dt * PROD;
+            if (qdot) qdot[c] = -(HRR * RCONV);
+        }
+#undef CI
+#undef RD
+#undef YS
+    free(RDHSP);
+    free(HENTH);
+}
+
+/* Point relaxation of the enthalpy equation (solveh.f:1146-1167): up to isor
+ * lexicographic Gauss-Seidel passes (J outer, I inner) over the interior
+ * cells, over-relaxed by relx, until sum|dFPZ| / hnorm <= tol. fpz [lj*li]
+ * holds HT on entry (boundary cells stay). Returns the pass count in the
+ * reference's convention (the converging pass, or isor + 1). */
+int orc_enthalpy_relax(int lj, int li, const double *rho, const double *rhsz, const double *ze, const double *zw,
+                       const double *zn, const double *zs, double *fpz, int isor, double relx, double tol,
+                       double hnorm)
+{
+    const double SOR1 = relx, SOR2 = F(1.0) - SOR1;
+    int p;
+    for (p = 1; p <= isor; ++p) {
+        double RSDZ = F(0.0);
+        for (int j = 1; j < lj - 1; ++j)
+            for (int i = 1; i < li - 1; ++i) {
+                const size_t c = (size_t)i * lj + j;
+                const double PPP = rho[c] - (ze[c] + zw[c] + zn[c] + zs[c]);
+                const double FNEW = SOR2 * fpz[c] + (rhsz[c] - zn[c] * fpz[c + 1] - zs[c] * fpz[c - 1]
+                                                     - ze[c] * fpz[c + lj] - zw[c] * fpz[c - lj]) * SOR1 / PPP;
+                RSDZ = RSDZ + fabs(fpz[c] - FNEW);
+                fpz[c] = FNEW;
+            }
+        if (RSDZ / hnorm <= tol) return p;
+    }
+    return p;
+}
+
+/* Temperature of the interior cells from FPZ less the kinetic energy
+ * (solveh.f:1170-1234): ENTH = (FPZ - (U^2 + V^2 + W^2)/2) HSTR + sum Y_k HFO_k HSTR.
+ * y [52][lj*li]; w may be NULL (no swirl). tk holds the guess on entry. */
+void orc_temperature_ke(int lj, int li, double *tk, const double *y, const double *fpz, const double *u,
+                        const double *v, const double *w)
+{
+    const size_t ne = (size_t)lj * li;
+    for (int i = 1; i < li - 1; ++i)
+        for (int j = 1; j < lj - 1; ++j) {
+            const size_t c = (size_t)i * lj + j;
+            const double wc = w ? w[c] : 0.0;
+            double ENTH = (fpz[c] - F(0.5) * (u[c] * u[c] + v[c] * v[c] + wc * wc)) * S.HSTR;
+            for (int k = 0; k < LSP; ++k) ENTH = ENTH + y[(size_t)k * ne + c] * S.HFO[k] * S.HSTR;
+            tk[c] = temperature_cell(tk[c], y + c, ne, ENTH);
+        }
+}

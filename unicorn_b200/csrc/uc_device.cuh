@@ -21,6 +21,7 @@ constexpr int ST_TMA_TIMEOUT = 1;
 constexpr int ST_NEWTON_NOCONV = 2;
 constexpr int ST_BAD_ORDER = 3;
 constexpr int ST_MMA_TIMEOUT = 4;
+constexpr int ST_RELAX_TIMEOUT = 5;
 
 // One reaction pair of the mechanism: forward slot 2p and reverse slot 2p+1
 // (0-based). Staged into shared memory by a bulk (TMA) copy at kernel start.

@@ -17,10 +17,29 @@
 #include "integrate_kernel.cuh"
 #include "faces_kernel.cuh"
 #include "fdetail_kernel.cuh"
+#include "enthalpy_kernel.cuh"
 #include "mlp_gemm.cuh"
 #include "mlp.cuh"
 
 using namespace uc;
+
+// Device buffers of the enthalpy relaxation, grown on demand: the ring of pass
+// results, the residual of each pass and the flags (progress [isor],
+// done [isor], stop pass, pass count, error word).
+struct RelaxBuffers {
+    double *ring = nullptr, *rsdz = nullptr;
+    int *flags = nullptr;
+    size_t ring_cap = 0, isor_cap = 0;
+    void release()
+    {
+        if (ring) cudaFree(ring);
+        if (rsdz) cudaFree(rsdz);
+        if (flags) cudaFree(flags);
+        ring = rsdz = nullptr;
+        flags = nullptr;
+        ring_cap = isor_cap = 0;
+    }
+};
 
 #define F32(x) ((double)(float)(x))
 
@@ -53,6 +72,13 @@ struct uc_ctx {
     uint8_t *hold = nullptr;
     bool have_grid = false, have_flow = false, faces_ready = false;
     double *fd_x = nullptr, *fd_y = nullptr, *fd_u = nullptr, *fd_v = nullptr, *fd_out = nullptr;
+    // enthalpy equation (SOLVEH)
+    bool rc_start = false;            // the RC plane belongs to the start state of the last species update
+    bool have_ht = false;
+    double *e_w = nullptr, *e_ekt = nullptr, *e_rdhsp = nullptr, *e_prod = nullptr, *e_fpz = nullptr;
+    double *e_ze = nullptr, *e_zw = nullptr, *e_zn = nullptr, *e_zs = nullptr, *e_rhsz = nullptr;
+    double *e_cf = nullptr, *e_f0s = nullptr, *e_part = nullptr;
+    RelaxBuffers e_rb;
     // batched integration
     double *pnd = nullptr, *enth = nullptr;
     int *nsub = nullptr, *order = nullptr, *hist = nullptr, *next_tile = nullptr, *cpasses = nullptr;
@@ -330,9 +356,12 @@ static void free_ctx(uc_ctx *c)
         if (c->pnd) cudaFree(c->pnd);
         if (c->enth) cudaFree(c->enth);
         void *fb[] = {c->g_xxs, c->g_xxc, c->g_yys, c->g_yyc, c->g_yr, c->f_u, c->f_v, c->f_tmu,
-                      c->fe, c->fw, c->fn, c->fs, c->hold, c->fd_x, c->fd_y, c->fd_u, c->fd_v, c->fd_out};
+                      c->fe, c->fw, c->fn, c->fs, c->hold, c->fd_x, c->fd_y, c->fd_u, c->fd_v, c->fd_out,
+                      c->e_w, c->e_ekt, c->e_rdhsp, c->e_prod, c->e_fpz, c->e_ze, c->e_zw, c->e_zn, c->e_zs,
+                      c->e_rhsz, c->e_cf, c->e_f0s, c->e_part};
         for (void *b : fb)
             if (b) cudaFree(b);
+        c->e_rb.release();
         if (c->int_exec) cudaGraphExecDestroy(c->int_exec);
         if (c->int_graph) cudaGraphDestroy(c->int_graph);
     }
@@ -512,6 +541,7 @@ extern "C" int uc_upload_fields(uc_ctx *ctx, const double *tk, const double *rho
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->have_fields = true;
     ctx->have_rc = false;
+    ctx->rc_start = false;
     return UC_OK;
 }
 
@@ -611,6 +641,7 @@ extern "C" int uc_rates(uc_ctx *ctx, int precision, double *rc)
     CK(cudaSetDevice(ctx->device));
     RET_IF(launch_chem(ctx, precision, true, false));
     ctx->have_rc = true;
+    ctx->rc_start = false;
     if (rc && precision == UC_FP64) {
         RET_IF(download_rows(ctx, rc, ctx->rc, LRX));
         CK(cudaStreamSynchronize(ctx->stream));
@@ -763,6 +794,7 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
         CK(cudaStreamSynchronize(ctx->stream));
     }
     ctx->have_rc = false;   // the RC plane belongs to the state before the update
+    ctx->rc_start = true;   // ... which the enthalpy equation uses (solveh.f:116-1145)
     return UC_OK;
 }
 
@@ -797,6 +829,7 @@ extern "C" int uc_sweep(uc_ctx *ctx, int precision, double dt, int isor, double 
     CK(cudaSetDevice(ctx->device));
     RET_IF(launch_chem(ctx, precision, true, true));
     ctx->have_rc = true;
+    ctx->rc_start = false;
     return uc_species_update(ctx, dt, isor, relx, tol, spnorm, face_sum, face_nbr, passes);
 }
 
@@ -976,6 +1009,284 @@ extern "C" int uc_assemble_faces(uc_ctx *ctx, double dt, double *e, double *w, d
         RET_IF(download_rows(ctx, s, ctx->fs, LSP - 1));
         CK(cudaStreamSynchronize(ctx->stream));
     }
+    return UC_OK;
+}
+
+// ------------------------------------------------------------------ enthalpy equation (SOLVEH)
+
+// Cells of the skewed plane of the relaxation: (ni + nj - 1) steps x nj rows.
+static __host__ __device__ size_t relax_plane(int lj, int li) { return (size_t)((li - 2) + (lj - 2) - 1) * (lj - 2); }
+
+// The relaxation on coefficients already in the skewed layout (cf, f0s) and
+// FPZ on entry f0 (natural layout). Writes fpz (natural layout) and the pass
+// count (device int); returns UC_E_* via err. isor >= 1.
+static int launch_relax(uc_ctx *ctx, cudaStream_t st, int nsm, RelaxBuffers &rb, int lj, int li, const double *cf,
+                        const double *f0, const double *f0s, int isor, double relx, double tol, double hnorm,
+                        double *fpz, int *status)
+{
+    const int nj = lj - 2, ni = li - 2;
+    const size_t plane = relax_plane(lj, li);
+    // ring of pass results: every pass when it fits in 1 GiB, else as many as fit (at least 2)
+    const size_t budget = (size_t)1 << 30;
+    int R = (int)std::min<size_t>((size_t)isor, std::max<size_t>(2, budget / (plane * sizeof(double))));
+    if (const char *e = getenv("UNICHEM_RELAX_RING")) {     // cap on the ring (memory); 2 is the least
+        const int cap = atoi(e);
+        if (cap >= 2) R = std::min(R, cap);
+    }
+    R = std::max(R, 2);
+    if ((size_t)R * plane > rb.ring_cap) {
+        if (rb.ring) cudaFree(rb.ring);
+        rb.ring = nullptr;
+        rb.ring_cap = 0;
+        if (cudaMalloc((void **)&rb.ring, (size_t)R * plane * sizeof(double)) != cudaSuccess)
+            return set_err(ctx, UC_E_NOMEM, "relaxation ring of %d x %zu doubles", R, plane);
+        rb.ring_cap = (size_t)R * plane;
+    }
+    if ((size_t)isor > rb.isor_cap) {
+        if (rb.rsdz) cudaFree(rb.rsdz);
+        if (rb.flags) cudaFree(rb.flags);
+        rb.rsdz = nullptr;
+        rb.flags = nullptr;
+        rb.isor_cap = 0;
+        if (cudaMalloc((void **)&rb.rsdz, (size_t)isor * sizeof(double)) != cudaSuccess ||
+            cudaMalloc((void **)&rb.flags, (2 * (size_t)isor + 2) * sizeof(int)) != cudaSuccess)
+            return set_err(ctx, UC_E_NOMEM, "relaxation flags");
+        rb.isor_cap = isor;
+    }
+    int *progress = rb.flags, *done = rb.flags + isor, *stop = rb.flags + 2 * isor, *passes = stop + 1;
+    CK(cudaMemsetAsync(rb.flags, 0, 2 * (size_t)isor * sizeof(int), st));
+    const int init[2] = {isor, 0};
+    CK(cudaMemcpyAsync(stop, init, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+    RelaxArgs a{};
+    a.lj = lj; a.li = li; a.nj = nj; a.ni = ni; a.nstep = ni + nj - 1;
+    a.cf = cf; a.f0 = f0; a.f0s = f0s; a.ring = rb.ring; a.rsdz = rb.rsdz;
+    a.progress = progress; a.done = done; a.stop_at = stop; a.status = status;
+    a.isor = isor; a.R = R;
+    a.sor1 = relx; a.sor2 = (double)1.0f - relx; a.tol = tol; a.hnorm = hnorm;
+    a.timeout_ns = 2000000000LL;
+    const int threads = (nj + 31) / 32 * 32;
+    const size_t smem = 3 * (size_t)nj * sizeof(double);
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, enth_relax_kernel, threads, smem));
+    if (per_sm < 1) return set_err(ctx, UC_E_CUDA, "relaxation kernel does not fit on an SM");
+    const int grid = std::min(isor, per_sm * nsm);
+    void *args[] = {&a};
+    CK(cudaLaunchCooperativeKernel((const void *)enth_relax_kernel, dim3(grid), dim3(threads), args, smem, st));
+    enth_relax_final_kernel<<<std::max(1, std::min((lj * li + 255) / 256, nsm * 4)), 256, 0, st>>>(a, fpz, passes);
+    CK(cudaGetLastError());
+    return UC_OK;
+}
+
+// skewed coefficient planes from natural-layout arrays: RHSZ, PPP = RHO - (ZE + ZW + ZN + ZS)
+// (solveh.f:1155), ZN, ZS, ZE, ZW, and the interior of FPZ on entry
+__global__ void enth_skew_kernel(int lj, int li, const double *rho, const double *rhsz, const double *ze,
+                                 const double *zw, const double *zn, const double *zs, const double *f0, double *cf,
+                                 double *f0s)
+{
+    const int nj = lj - 2;
+    const size_t plane = relax_plane(lj, li);
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < lj * li; idx += gridDim.x * blockDim.x) {
+        const int j = idx % lj, i = idx / lj;
+        if (j == 0 || j == lj - 1 || i == 0 || i == li - 1) continue;
+        const size_t k = skew_index(j - 1, i - 1, nj);
+        cf[CF_RHSZ * plane + k] = rhsz[idx];
+        cf[CF_PPP * plane + k] = rho[idx] - (ze[idx] + zw[idx] + zn[idx] + zs[idx]);
+        cf[CF_ZN * plane + k] = zn[idx];
+        cf[CF_ZS * plane + k] = zs[idx];
+        cf[CF_ZE * plane + k] = ze[idx];
+        cf[CF_ZW * plane + k] = zw[idx];
+        f0s[k] = f0[idx];
+    }
+}
+
+static int check_relax_grid(uc_ctx *ctx, int lj, int li)
+{
+    if (lj < 3 || li < 3) return set_err(ctx, UC_E_ARG, "enthalpy relaxation: lj, li >= 3");
+    if (lj - 2 > RELAX_MAX_ROWS)
+        return set_err(ctx, UC_E_ARG, "enthalpy relaxation: at most %d interior rows (lj - 2), got %d", RELAX_MAX_ROWS,
+                       lj - 2);
+    return UC_OK;
+}
+
+extern "C" int uc_enthalpy_relax(int device, int lj, int li, const double *rho, const double *rhsz, const double *ze,
+                                 const double *zw, const double *zn, const double *zs, double *fpz, int isor,
+                                 double relx, double tol, double hnorm, int *passes)
+{
+    if (!rho || !rhsz || !ze || !zw || !zn || !zs || !fpz) return UC_E_ARG;
+    RET_IF(check_relax_grid(nullptr, lj, li));
+    if (!(relx > 0.0)) return UC_E_ARG;
+    const size_t n = (size_t)lj * li, plane = relax_plane(lj, li);
+    if (isor < 1) {                   // zero-trip DO loop: FPZ unchanged, ISOR2 = 1 (solveh.f:1149-1167)
+        if (passes) *passes = 1;
+        return UC_OK;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return UC_E_CUDA;
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return UC_E_CUDA;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return UC_E_CUDA;
+    double *buf = nullptr;
+    int *status = nullptr;
+    RelaxBuffers rb;
+    int rc = UC_OK;
+    int hp[2] = {0, 0};
+    do {
+        if (cudaMalloc((void **)&buf, (8 * n + 7 * plane) * sizeof(double)) != cudaSuccess ||
+            cudaMalloc((void **)&status, 2 * sizeof(int)) != cudaSuccess) { rc = UC_E_NOMEM; break; }
+        double *d_rho = buf, *d_rhsz = d_rho + n, *d_ze = d_rhsz + n, *d_zw = d_ze + n, *d_zn = d_zw + n,
+               *d_zs = d_zn + n, *d_f0 = d_zs + n, *d_out = d_f0 + n, *d_cf = d_out + n, *d_f0s = d_cf + 6 * plane;
+        const double *src[7] = {rho, rhsz, ze, zw, zn, zs, fpz};
+        double *dst[7] = {d_rho, d_rhsz, d_ze, d_zw, d_zn, d_zs, d_f0};
+        bool ok = true;
+        for (int q = 0; q < 7 && ok; ++q)
+            ok = cudaMemcpyAsync(dst[q], src[q], n * sizeof(double), cudaMemcpyHostToDevice, st) == cudaSuccess;
+        if (!ok || cudaMemsetAsync(status, 0, 2 * sizeof(int), st) != cudaSuccess) { rc = UC_E_CUDA; break; }
+        enth_skew_kernel<<<std::max(1, std::min((int)((n + 255) / 256), nsm * 4)), 256, 0, st>>>(
+            lj, li, d_rho, d_rhsz, d_ze, d_zw, d_zn, d_zs, d_f0, d_cf, d_f0s);
+        if (cudaGetLastError() != cudaSuccess) { rc = UC_E_CUDA; break; }
+        rc = launch_relax(nullptr, st, nsm, rb, lj, li, d_cf, d_f0, d_f0s, isor, relx, tol,
+                          hnorm > 0.0 ? hnorm : (double)n, d_out, status);
+        if (rc != UC_OK) break;
+        if (cudaMemcpyAsync(fpz, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(hp, status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(hp + 1, rb.flags + 2 * isor + 1, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) { rc = UC_E_CUDA; break; }
+        if (hp[0] == ST_RELAX_TIMEOUT) { rc = UC_E_TIMEOUT; break; }
+        if (passes) *passes = hp[1];
+    } while (0);
+    cudaStreamSynchronize(st);
+    rb.release();
+    if (buf) cudaFree(buf);
+    if (status) cudaFree(status);
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+extern "C" int uc_set_enthalpy(uc_ctx *ctx, const double *ht, const double *w)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ht) return set_err(ctx, UC_E_ARG, "uc_set_enthalpy: ht is required");
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(dalloc(ctx, &ctx->ht, ctx->npad));
+    RET_IF(upload_rows(ctx, ctx->ht, ht, 1));
+    RET_IF(dalloc(ctx, &ctx->e_w, ctx->npad));
+    RET_IF(upload_rows(ctx, ctx->e_w, w, 1));       // NULL: no swirl (zeros)
+    ctx->have_ht = true;
+    return UC_OK;
+}
+
+extern "C" int uc_enthalpy_update(uc_ctx *ctx, const uc_enthalpy_opts *o, int *passes, double *resdh)
+{
+    if (!ctx || !o) return UC_E_ARG;
+    if (!ctx->have_grid || !ctx->have_flow) return set_err(ctx, UC_E_STATE, "uc_enthalpy_update: uc_set_grid and uc_set_flow first");
+    if (!ctx->have_ht) return set_err(ctx, UC_E_STATE, "uc_enthalpy_update: uc_set_enthalpy first");
+    if (!ctx->rc_start) return set_err(ctx, UC_E_STATE, "uc_enthalpy_update needs the rate plane of a species update (uc_sweep)");
+    if (!ctx->vtc || !ctx->vdf || !ctx->cp) return set_err(ctx, UC_E_STATE, "uc_enthalpy_update needs the properties and cp of uc_sweep");
+    if (!(o->dt >= 0.0) || !(o->relx > 0.0) || !(o->sigh > 0.0)) return set_err(ctx, UC_E_ARG, "invalid dt/relx/sigh");
+    RET_IF(check_relax_grid(ctx, ctx->lj, ctx->li));
+    CK(cudaSetDevice(ctx->device));
+    const size_t np = ctx->npad, plane = relax_plane(ctx->lj, ctx->li);
+    for (double **b : {&ctx->e_ekt, &ctx->e_prod, &ctx->e_fpz, &ctx->e_ze, &ctx->e_zw, &ctx->e_zn, &ctx->e_zs, &ctx->e_rhsz})
+        RET_IF(dalloc(ctx, b, np));
+    RET_IF(dalloc(ctx, &ctx->e_rdhsp, (size_t)LSP * np));
+    RET_IF(dalloc(ctx, &ctx->e_cf, CF_N * plane));
+    RET_IF(dalloc(ctx, &ctx->e_f0s, plane));
+    const int tgrid = ctx->nsm * 4;
+    RET_IF(dalloc(ctx, &ctx->e_part, tgrid));
+    int slot;
+    prof_begin(ctx, UC_K_ENTHALPY, slot);
+    // heat release of the start-state RC and the updated Y (solveh.f:116-1145)
+    {
+        EnthSrcArgs a{};
+        a.P = ctx->dP; a.rc = ctx->rc; a.rc32 = ctx->rc32; a.tile_flag = ctx->tile_flag;
+        a.tk = ctx->tk; a.y = ctx->y; a.hold = ctx->hold; a.qdsp = ctx->qdsp; a.qdot = ctx->qdot; a.prod = ctx->e_prod;
+        a.npad = ctx->npad; a.ntile = ctx->ntile;
+        const bool mixed = ctx->rc_prec == UC_MIXED;
+        const void *fn = mixed ? (const void *)enth_source_kernel<float> : (const void *)enth_source_kernel<double>;
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ENTH_SRC_SMEM));
+        if (mixed)
+            enth_source_kernel<float><<<std::min(ctx->ntile, ctx->nsm), CHEM_THREADS, ENTH_SRC_SMEM, ctx->stream>>>(a);
+        else
+            enth_source_kernel<double><<<std::min(ctx->ntile, ctx->nsm), CHEM_THREADS, ENTH_SRC_SMEM, ctx->stream>>>(a);
+        CK(cudaGetLastError());
+    }
+    // EKT and the species-enthalpy diffusion factors of every cell
+    {
+        EnthCoefArgs a{};
+        a.P = ctx->dP; a.tk = ctx->tk; a.rho = ctx->rho; a.cp = ctx->cp; a.vtc = ctx->vtc; a.vdf = ctx->vdf;
+        a.tmu = ctx->f_tmu; a.sigsp = ctx->sigsp; a.sigh = o->sigh; a.beta2 = ctx->sc.beta2;
+        a.ekt = ctx->e_ekt; a.rdhsp = ctx->e_rdhsp; a.n = ctx->n; a.npad = ctx->npad;
+        enth_coef_kernel<<<std::max(1, std::min((ctx->n + 127) / 128, ctx->nsm * 8)), 128, 0, ctx->stream>>>(a);
+        CK(cudaGetLastError());
+    }
+    // coefficients and right-hand side of the interior cells
+    {
+        EnthRhsArgs a{};
+        a.P = ctx->dP; a.lj = ctx->lj; a.li = ctx->li; a.npad = ctx->npad; a.isym = ctx->isym;
+        a.tk = ctx->tk; a.rho = ctx->rho; a.y = ctx->y; a.ht = ctx->ht; a.stmf = ctx->soot0; a.u = ctx->f_u; a.v = ctx->f_v;
+        a.ekt = ctx->e_ekt; a.rdhsp = ctx->e_rdhsp; a.prod = ctx->e_prod;
+        a.yr = ctx->g_yr; a.xxs = ctx->g_xxs; a.xxc = ctx->g_xxc; a.yys = ctx->g_yys; a.yyc = ctx->g_yyc;
+        a.dt = o->dt; a.crad = ctx->sc.alstr / ctx->sc.rstr / ctx->sc.vstr / ctx->sc.vstr / ctx->sc.vstr;
+        a.rsoot = 1.9000e+03;
+        a.ze = ctx->e_ze; a.zw = ctx->e_zw; a.zn = ctx->e_zn; a.zs = ctx->e_zs; a.rhsz = ctx->e_rhsz;
+        a.cf = ctx->e_cf; a.f0s = ctx->e_f0s;
+        enth_rhs_kernel<<<std::max(1, std::min((ctx->n + 127) / 128, ctx->nsm * 8)), 128, 0, ctx->stream>>>(a);
+        CK(cudaGetLastError());
+    }
+    // relaxation of FPZ (solveh.f:1146-1167)
+    const double hnorm = o->hnorm > 0.0 ? o->hnorm : (double)ctx->lj * ctx->li;
+    int hpass = 1;
+    if (o->isor >= 1) {
+        RET_IF(launch_relax(ctx, ctx->stream, ctx->nsm, ctx->e_rb, ctx->lj, ctx->li, ctx->e_cf, ctx->ht, ctx->e_f0s,
+                            o->isor, o->relx, o->tol, hnorm, ctx->e_fpz, ctx->status));
+    } else {
+        CK(cudaMemcpyAsync(ctx->e_fpz, ctx->ht, np * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    // T from FPZ, HT := FPZ (solveh.f:1170-1234, spgsolv.f:1304,1358)
+    {
+        EnthTempArgs a{};
+        a.P = ctx->dP; a.lj = ctx->lj; a.li = ctx->li; a.npad = ctx->npad;
+        a.y = ctx->y; a.fpz = ctx->e_fpz; a.u = ctx->f_u; a.v = ctx->f_v; a.w = ctx->e_w;
+        a.tk = ctx->tk; a.ht = ctx->ht; a.partial = ctx->e_part; a.status = ctx->status;
+        enth_temp_kernel<<<tgrid, 256, 0, ctx->stream>>>(a);
+        CK(cudaGetLastError());
+    }
+    prof_end(ctx, slot);
+    std::vector<double> part(tgrid);
+    int st = 0;
+    CK(cudaMemcpyAsync(part.data(), ctx->e_part, tgrid * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&st, ctx->status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (o->isor >= 1)
+        CK(cudaMemcpyAsync(&hpass, ctx->e_rb.flags + 2 * o->isor + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->rc_start = false;
+    if (st == ST_RELAX_TIMEOUT) {
+        CK(cudaMemsetAsync(ctx->status, 0, sizeof(int), ctx->stream));
+        return set_err(ctx, UC_E_TIMEOUT, "enthalpy relaxation: a wait between passes timed out on the device");
+    }
+    double r = 0.0;
+    for (double v : part) r += v;
+    if (passes) *passes = hpass;
+    if (resdh) *resdh = r / hnorm;
+    return check_status(ctx);
+}
+
+extern "C" int uc_enthalpy_get(uc_ctx *ctx, double *ht, double *rhsz, double *ze, double *zw, double *zn, double *zs)
+{
+    if (!ctx) return UC_E_ARG;
+    CK(cudaSetDevice(ctx->device));
+    if (ht) {
+        if (!ctx->have_ht) return set_err(ctx, UC_E_STATE, "no enthalpy field");
+        RET_IF(download_rows(ctx, ht, ctx->ht, 1));
+    }
+    const double *src[5] = {ctx->e_rhsz, ctx->e_ze, ctx->e_zw, ctx->e_zn, ctx->e_zs};
+    double *dst[5] = {rhsz, ze, zw, zn, zs};
+    for (int q = 0; q < 5; ++q) {
+        if (!dst[q]) continue;
+        if (!src[q]) return set_err(ctx, UC_E_STATE, "no enthalpy update yet");
+        RET_IF(download_rows(ctx, dst[q], src[q], 1));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
     return UC_OK;
 }
 
@@ -1180,6 +1491,7 @@ static int integrate_prepare(uc_ctx *ctx, int precision, const uc_integrate_opts
 extern "C" int uc_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts *o)
 {
     RET_IF(integrate_prepare(ctx, precision, o));
+    ctx->rc_start = false;
     const bool fresh = ctx->int_exec && ctx->int_prec == precision && ctx->int_gwarps == ctx->int_warps &&
                        ctx->int_gsorted == ctx->int_sorted && same_opts(ctx->int_opts, *o);
     if (!fresh) {

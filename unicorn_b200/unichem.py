@@ -70,6 +70,12 @@ class IntegrateOpts(ctypes.Structure):
                 ("c_tau", ctypes.c_double), ("y_tau", ctypes.c_double), ("nsub_max", ctypes.c_int)]
 
 
+class EnthalpyOpts(ctypes.Structure):
+    """uc_enthalpy_opts: settings of the enthalpy equation (SOLVEH)."""
+    _fields_ = [("dt", ctypes.c_double), ("isor", ctypes.c_int), ("relx", ctypes.c_double), ("tol", ctypes.c_double),
+                ("hnorm", ctypes.c_double), ("sigh", ctypes.c_double)]
+
+
 def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     """Load libunichem.so; raises if it is missing (no CPU fallback exists)."""
     global _lib
@@ -113,6 +119,11 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.uc_integrate.argtypes = [vp, ctypes.c_int, ctypes.POINTER(IntegrateOpts)]
     lib.uc_integrate_tune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(IntegrateOpts)]
     lib.uc_integrate_counts.argtypes = [vp, IP, IP]
+    lib.uc_set_enthalpy.argtypes = [vp, P, P]
+    lib.uc_enthalpy_update.argtypes = [vp, ctypes.POINTER(EnthalpyOpts), IP, P]
+    lib.uc_enthalpy_get.argtypes = [vp, P, P, P, P, P, P]
+    lib.uc_enthalpy_relax.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, P, P, P, P, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double, IP]
     _lib = lib
     return lib
 
@@ -277,10 +288,10 @@ class UniChem:
 
     def profile_read(self) -> dict:
         """Device time (ms) and launches per kernel kind since the last read."""
-        ms = np.zeros(6)
-        cnt = (ctypes.c_int * 6)()
+        ms = np.zeros(7)
+        cnt = (ctypes.c_int * 7)()
         self._ck(self.lib.uc_profile_read(self._h, _p(ms), cnt))
-        names = ["chem", "update", "props", "cp_h", "temperature", "integrate"]
+        names = ["chem", "update", "props", "cp_h", "temperature", "integrate", "enthalpy"]
         return {nm: (float(ms[i]), int(cnt[i])) for i, nm in enumerate(names)}
 
     # ------------------------------------------------------------ species-equation faces
@@ -311,6 +322,28 @@ class UniChem:
         self._ck(self.lib.uc_fdetail(self._h, int(lj), int(li), _p(_in(x, (n,))), _p(_in(y, (n,))),
                                      _p(_in(u, (n,))), _p(_in(v, (n,))), _p(out)))
         return out
+
+    # ------------------------------------------------------------ enthalpy equation
+    def set_enthalpy(self, ht, w=None):
+        """HT [n] (non-dimensional FPZ) and the swirl velocity W [n] (None: no swirl)."""
+        n = self.n
+        self._ck(self.lib.uc_set_enthalpy(self._h, _p(_in(ht, (n,))), _p(_in(w, (n,)))))
+
+    def enthalpy_update(self, dt: float, isor: int = 100, relx: float = 0.99, tol: float = 1e-8,
+                        hnorm: float = 0.0, sigh: float = 0.9):
+        """SOLVEH after a uc_sweep: returns (passes as ISOR2 reports it, RESDH). T and HT are updated
+        on the device; QDSP/QDOT of the interior cells become SOLVEH's."""
+        o = EnthalpyOpts(float(dt), int(isor), float(relx), float(tol), float(hnorm), float(sigh))
+        passes = ctypes.c_int(0)
+        resdh = np.zeros(1)
+        self._ck_warn(self.lib.uc_enthalpy_update(self._h, ctypes.byref(o), ctypes.byref(passes), _p(resdh)))
+        return passes.value, float(resdh[0])
+
+    def enthalpy_get(self):
+        """(HT, RHSZ, ZE, ZW, ZN, ZS) [n] each, after an enthalpy update."""
+        out = [np.empty(self.n) for _ in range(6)]
+        self._ck(self.lib.uc_enthalpy_get(self._h, *[_p(o) for o in out]))
+        return tuple(out)
 
     # ------------------------------------------------------------ restart files
     def save_restart(self, path, lj: int, li: int, flow: dict, **header):
@@ -381,3 +414,18 @@ class UniChem:
             warnings.warn(self.lib.uc_last_error(self._h).decode())
         else:
             self._ck(rc)
+
+
+def enthalpy_relax(lj: int, li: int, rho, rhsz, z, ht, isor: int = 100, relx: float = 0.99, tol: float = 1e-8,
+                   hnorm: float = 0.0, device: int = 0):
+    """The relaxation of solveh.f:1146-1167 alone on the device: z = (ze, zw, zn, zs); returns (FPZ, passes)."""
+    lib = load_library()
+    n = lj * li
+    fpz = np.array(ht, dtype=np.float64, copy=True).reshape(n)
+    passes = ctypes.c_int(0)
+    arrs = [_in(a, (n,)) for a in (rho, rhsz, *z)]
+    rc = lib.uc_enthalpy_relax(int(device), int(lj), int(li), *[_p(a) for a in arrs], _p(fpz), int(isor),
+                               float(relx), float(tol), float(hnorm), ctypes.byref(passes))
+    if rc != 0:
+        raise RuntimeError(f"uc_enthalpy_relax failed ({rc})")
+    return fpz, passes.value
