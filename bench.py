@@ -651,6 +651,117 @@ def main_c5(args):
     print(json.dumps(line), flush=True)
 
 
+def cpu_baseline_enthalpy(u, fl, ht, ncols=61):
+    """The oracle's enthalpy step (rates, EKT/Z, RHSZ, Gauss-Seidel relaxation, T) on one host core for
+    the first ncols columns of the device's current field, as a bounded sample."""
+    from oracle.oracle import Oracle
+    o = Oracle()
+    tk, rho, y, s1, _ = u.download()
+    nr = fl["lj"]
+    m = nr * ncols
+    sl = slice(0, m)
+    yc, _, vtc, vdf, _ = o.props(tk[sl], np.ascontiguousarray(y[:, sl]))
+    t0 = time.perf_counter()
+    r = o.enthalpy_solve(nr, ncols, tk[sl], rho[sl], yc, yc, ht[sl], s1[sl], vtc, vdf, fl["u"][sl], fl["v"][sl],
+                         fl["tmu"][sl], fl["yr"][sl], fl["xxs"][:ncols], fl["xxc"][:ncols], fl["yys"], fl["yyc"],
+                         dt=DT, isor=ISOR, relx=RELX, tol=TOL)
+    dt = time.perf_counter() - t0
+    return {"value": m / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"enthalpy step only (oracle/unichem_oracle.c, -O2, 1 thread) on the first {ncols} columns "
+                      f"({m} cells) of the field after the pre-sweeps, {r['passes']} relaxation passes, {dt:.2f} s"}
+
+
+def main_c5_live(args):
+    """In-loop sweeps with live transport: the species faces assembled on the device from the state of
+    each sweep (SPGSOLV's coefficients), then the enthalpy equation (SOLVEH: heat release, species
+    enthalpy diffusion, radiation, Gauss-Seidel relaxation, T from FPZ) and the density at PBACK."""
+    import torch
+    from unicorn_b200 import unichem
+    from unicorn_b200.fields import jet_field, jet_flow, nondimensional, sensible_enthalpy
+    f = jet_field(NZ, NR, fuel=FUEL, t_peak=TPEAK, seed=0)
+    fl = jet_flow(NZ, NR, seed=0)
+    n = f.n
+    prec = unichem.MIXED if args.precision == "mixed" else unichem.FP64
+    u = unichem.UniChem(n)
+    sc = u.scales
+    tk, rho = nondimensional(f, sc, u.wm)
+    u.upload(tk, rho, f.y)
+    u.set_grid(fl["lj"], fl["li"], fl["xxs"], fl["xxc"], fl["yys"], fl["yyc"], fl["yr"], isym=1)
+    u.set_flow(fl["u"], fl["v"], fl["tmu"], 0.9)
+    with open(Path(__file__).resolve().parent / "unicorn_b200" / "mech" / "sandiego52.json") as fh:
+        poly = np.array(json.load(fh)["poly"])
+    ht = sensible_enthalpy(f.T, f.y, poly, u.wm, u.hfo, sc) + 0.5 * (fl["u"] ** 2 + fl["v"] ** 2)
+    # the generator puts radicals (1e-10..1e-3) into cold cells as well; species-only sweeps at held
+    # enthalpy first let the chemistry consume them, as the frozen in-loop run does, before the
+    # enthalpy equation couples the heat release to T
+    import warnings
+    if args.presweeps > 0:
+        u.set_pressure(f.p / sc["PSTR"])
+        u.hold_enthalpy()
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            for _ in range(args.presweeps):
+                u.sweep(DT, precision=prec, isor=ISOR, relx=RELX, tol=TOL)
+                u.temperature_from_held()
+        tk0, _, y0, _, _ = u.download()
+        T0 = tk0 * sc["TSTR"]
+        ht = sensible_enthalpy(T0, y0, poly, u.wm, u.hfo, sc) + 0.5 * (fl["u"] ** 2 + fl["v"] ** 2)
+    else:
+        T0 = f.T
+    u.set_enthalpy(ht)
+    cpu = None if args.no_cpu_baseline else cpu_baseline_enthalpy(u, fl, ht)
+    view = unichem_view(u)
+    ext = torch.cuda.ExternalStream(view["stream"])
+    sweeps = args.sweeps
+    sp_passes, h_passes, resdh = [], [], []
+    ms, ms_split = 0.0, {}
+    for sw in range(args.warmup + sweeps):
+        timed = sw >= args.warmup
+        if timed:
+            u.profile(True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            p1 = u.sweep(DT, precision=prec, isor=ISOR, relx=RELX, tol=TOL)
+            p2, r = u.enthalpy_update(DT, isor=ISOR, relx=RELX, tol=TOL, sigh=0.9)
+        u.density()
+        if timed:
+            e1.record(ext)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            for k, (t, c) in u.profile_read().items():
+                ms_split[k] = ms_split.get(k, 0.0) + t
+            u.profile(False)
+            sp_passes.append(p1)
+            h_passes.append(p2)
+            resdh.append(r)
+    tk1, rho1, y1, s1, _ = u.download()
+    T1 = tk1 * sc["TSTR"]
+    inner = np.zeros((NZ, NR), dtype=bool)
+    inner[1:-1, 1:-1] = True
+    inner = inner.reshape(-1)
+    report = {"peak_T": round(float(T1.max()), 3), "mean_T": round(float(T1[inner].mean()), 3),
+              "mean_T_start": round(float(T0[inner].mean()), 3), "presweeps": args.presweeps,
+              "cells_at_5000K": int((T1 >= 5000.0 - 1e-6).sum()), "cells_at_TKDMIN": int((T1 <= sc["TSTR"] - 1 + 1e-6).sum()),
+              "sumY_drift_max": float(np.abs(y1.sum(0) + s1 - 1.0).max()),
+              "rho_range": [float(rho1.min()), float(rho1.max())],
+              "species_passes": sp_passes[:5] + sp_passes[-3:], "enthalpy_passes": h_passes[:5] + h_passes[-3:],
+              "resdh_first_last": [resdh[0], resdh[-1]] if resdh else None,
+              "ms_per_sweep_by_kind": {k: round(v / max(sweeps, 1), 3) for k, v in ms_split.items() if v > 0}}
+    u.close()
+    line = {"metric": "in-loop sweeps with live transport and the enthalpy equation", "value": round(n * sweeps / (ms / 1e3), 1),
+            "unit": UNIT, "n_gpus": 1, "steps": sweeps, "warmup": args.warmup, "ms_per_step": round(ms / sweeps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
+            "data": "synthetic (seeded C2 generator and jet flow)",
+            "config": {"workload": f"C5 with live transport: 601x301 heptane field, {sweeps} sweeps of dt=1e-5 s; "
+                                   "each sweep = uc_sweep (faces assembled on the device) + uc_enthalpy_update "
+                                   "(SOLVEH) + uc_density", "report": report}}
+    if cpu is not None:
+        line["cpu_baseline_enthalpy_step"] = cpu
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -661,10 +772,12 @@ def main():
     ap.add_argument("--cells", type=int, default=0, help="use only the first N cells (profiling runs)")
     ap.add_argument("--isor", type=int, default=ISOR, help="update passes cap (profiling runs)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "c5-live"],
                     help="c2: the species sweep of the 601x301 heptane field (headline); c3: batched stiff "
-                         "integration; c4: learned surrogate with fallback; c5: in-loop sweeps")
+                         "integration; c4: learned surrogate with fallback; c5: in-loop sweeps; c5-live: in-loop "
+                         "sweeps with live transport faces and the enthalpy equation")
     ap.add_argument("--sweeps", type=int, default=1000, help="c5: sweeps")
+    ap.add_argument("--presweeps", type=int, default=200, help="c5-live: species-only sweeps before the live ones")
     ap.add_argument("--train-steps", type=int, default=2000, help="c4: Adam steps")
     args = ap.parse_args()
     if args.workload == "c3":
@@ -673,6 +786,8 @@ def main():
         main_c4(args)
     elif args.workload == "c5":
         main_c5(args)
+    elif args.workload == "c5-live":
+        main_c5_live(args)
     elif args.impl == "reference":
         main_reference(args)
     else:

@@ -197,6 +197,14 @@ int uc_enthalpy_update(uc_ctx *ctx, const uc_enthalpy_opts *o, int *passes, doub
 /* HT [n] and the last update's RHSZ, ZE, ZW, ZN, ZS [n] to the host (NULL = skip). */
 int uc_enthalpy_get(uc_ctx *ctx, double *ht, double *rhsz, double *ze, double *zw, double *zn, double *zs);
 
+/* Density of every cell from the gas law at the back pressure PBACK,
+ * RHO = PBACK / (BETA1 TK sum Y_k/W_k), with the reference's edge rules (last
+ * column extrapolated linearly, first row copied from the second); needs the
+ * grid of uc_set_grid. The reference stores this as RHONP and makes it RHO in
+ * steady runs (ISTDY = 1).
+ * Replaces: src/unicornd-mild-sd-5.f:1056-1073. */
+int uc_density(uc_ctx *ctx);
+
 /* The relaxation alone, on host arrays of an lj x li grid (J fastest):
  * fpz [lj*li] holds HT on entry and FPZ on return; rho, rhsz and the
  * coefficients ze, zw, zn, zs are read on the interior cells. Same ordering,

@@ -22,6 +22,7 @@ Translated pieces (reference paths relative to the UNICORN checkout):
   enthalpy diffusion, radiation, heat release)     -> f77_solveh_rhs
 * ``src/lib/solveh.f:34-1234``  the whole of SOLVEH: right-hand side, point
   relaxation of FPZ and the temperature from it   -> f77_solveh_full
+* ``src/unicornd-mild-sd-5.f:1056-1068`` density from the gas law at PBACK -> f77_main_density
 * ``src/unicornd-mild-sd-5.f:84-113`` DATA WSP/CDIA/TLJ/CI11      -> f77_main_data
 * ``src/unicornd-mild-sd-5.f:327-483`` set-up of tables/scales    -> f77_main_setup
 * ``src/unicornd-mild-sd-5.f:821-1006`` Y clip + transport props   -> f77_main_props
@@ -80,6 +81,7 @@ def build(ref: str, lj: int, li: int, out: Path = OUT) -> Path:
         (std, "f77_stdata_rg", [(26, 118)], None, None),
         (sh, "f77_solveh_rhs", [(34, 1145)], None, None),
         (sh, "f77_solveh_full", [(34, 1234)], None, None),
+        (main, "f77_main_density", [(1056, 1068)], "MAIN_", None),
     ]
     code = translate(frags, [data, ckr, ssp, sh, spg, std, main])
     code = code.replace("#include <string.h>", f"#include <string.h>\ndouble F77P_TCP[{ncell}];", 1)

@@ -406,6 +406,12 @@ class Oracle:
         tk_new = self.temperature_ke(lj, li, tk, y_new, fpz, u, v, w)
         return dict(fpz=fpz, tk=tk_new, passes=passes, rhsz=rhsz, z=z, qdsp=qdsp, qdot=qdot, ekt=ekt)
 
+    def density(self, lj, li, tk, y):
+        """RHONP [lj*li] of the gas law at PBACK with the grid's edge rules (main:1056-1068)."""
+        out = np.empty(lj * li)
+        self.lib.orc_density(lj, li, _dptr(_c(tk)), _dptr(_c(y)), _dptr(out))
+        return out
+
     def fdetail(self, lj, li, x, y, rho, u, v, tk, qdot, vmu, vtc, fsp, vdf, qdsp):
         """FDETAIL fields [10 + 4*52, lj*li] (stdata.f:26-118)."""
         out = np.zeros((10 + 4 * LSP, lj * li))

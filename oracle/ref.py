@@ -412,3 +412,14 @@ class RefUnicorn:
         return dict(fpz=flat("FPZ"), tk=flat("TK"), passes=ctypes.c_int.in_dll(self.lib, "F77A_SOLVEH_ISOR2").value,
                     rhsz=flat("RHSZ"), qdsp=np.stack([q[:, :, k].reshape(-1, order="F") for k in range(LSP)]),
                     qdot=flat("QDOT"))
+
+    # -------------------------------------------------------------- density after SPGSOLV
+    def density(self, tk, y):
+        """main:1056-1068 on the whole compile-time grid: RHONP = PBACK/(BETA1 TK RBAR), the last
+        column extrapolated linearly, the first row copied from the second. Returns RHONP [LJ*LI]."""
+        M = "UNICORN"
+        n = self.LJ * self.LI
+        self.var(M, "TK")[:] = np.asarray(tk, dtype=np.float64)          # main's view: TK(LE), FSP(LE,LSP)
+        self.var(M, "FSP")[:, :] = np.asarray(y, dtype=np.float64).T
+        self.lib.f77_main_density()
+        return self.var(M, "RHONP").reshape(-1, order="F").copy()

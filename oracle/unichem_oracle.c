@@ -1188,3 +1188,19 @@ void orc_temperature_ke(int lj, int li, double *tk, const double *y, const doubl
             tk[c] = temperature_cell(tk[c], y + c, ne, ENTH);
         }
 }
+
+/* Density from the gas law at the back pressure (src/unicornd-mild-sd-5.f:1056-1068):
+ * RHONP = PBACK / (BETA1 TK RBAR), RBAR = sum Y_k / W_k, on every cell of the
+ * lj x li grid; the last column (I = LI) extrapolated linearly from the two
+ * before it, then the first row (J = 1) copied from the second. y [52][lj*li]. */
+void orc_density(int lj, int li, const double *tk, const double *y, double *rho)
+{
+    const size_t ne = (size_t)lj * li;
+    for (size_t c = 0; c < ne; ++c) {
+        double RBAR = F(0.0);
+        for (int k = 0; k < LSP; ++k) RBAR = RBAR + y[(size_t)k * ne + c] / S.WM[k];
+        rho[c] = S.PBACK / (S.BETA1 * tk[c] * RBAR);
+    }
+    for (size_t c = ne - lj; c < ne; ++c) rho[c] = F(2.0) * rho[c - lj] - rho[c - 2 * (size_t)lj];
+    for (size_t c = 0; c < ne; c += lj) rho[c] = rho[c + 1];
+}

@@ -75,3 +75,14 @@ def test_enthalpy_solve_bitwise_vs_reference(oracle, ref, isym, seed, isor, tol)
     assert np.abs(o["fpz"] - g["ht"])[inner].max() > 1e-6
     assert np.abs(o["tk"] - g["tk"])[inner].max() > 1e-6
     assert np.all(np.isfinite(o["fpz"])) and np.all(np.isfinite(o["tk"]))
+
+
+def test_density_bitwise_vs_reference(oracle, ref):
+    """RHONP of main:1056-1068 (gas law at PBACK, last-column extrapolation, first-row copy)."""
+    LJ, LI = ref.LJ, ref.LI
+    g = enthalpy_case(oracle, LJ, LI, 11)
+    r = ref.density(g["tk"], g["y_new"])
+    o = oracle.density(LJ, LI, g["tk"], g["y_new"])
+    assert np.array_equal(r, o)
+    J = np.arange(LJ * LI) % LJ
+    assert np.array_equal(o[J == 0], o[np.nonzero(J == 0)[0] + 1])

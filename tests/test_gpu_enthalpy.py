@@ -174,3 +174,15 @@ def test_enthalpy_update_needs_a_sweep(cuda, oracle):
         u.enthalpy_update(1e-3, isor=5)
         with pytest.raises(RuntimeError):        # the rate plane belongs to the state before the update
             u.enthalpy_update(1e-3, isor=5)
+
+
+def test_density_matches_oracle(cuda, oracle):
+    g = enthalpy_case(oracle, LJ, LI, 12)
+    n = LJ * LI
+    with cuda.UniChem(n) as u:
+        u.upload(g["tk"], g["rho"], g["y_new"])
+        u.set_grid(LJ, LI, g["xxs"], g["xxc"], g["yys"], g["yyc"], g["yr"], isym=1)
+        u.density()
+        _, rho_g, _, _, _ = u.download()
+    rho_o = oracle.density(LJ, LI, g["tk"], g["y_new"])
+    assert np.array_equal(rho_g, rho_o)

@@ -440,6 +440,7 @@ struct EnthTempArgs {
     double *tk, *ht;                     // tk: guess in, T out; ht := fpz on the interior
     double *partial;                     // [gridDim.x] partial sums of |FPZ - HT|
     int *status;
+    const int *relax_status;             // error word of the relaxation: when set, nothing is changed
 };
 
 __global__ void __launch_bounds__(256) enth_temp_kernel(const EnthTempArgs a)
@@ -448,7 +449,8 @@ __global__ void __launch_bounds__(256) enth_temp_kernel(const EnthTempArgs a)
     const int lj = a.lj, li = a.li;
     __shared__ double s_part[256];
     double res = 0.0;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < lj * li; idx += gridDim.x * blockDim.x) {
+    const bool skip = a.relax_status && *a.relax_status != ST_OK;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; !skip && idx < lj * li; idx += gridDim.x * blockDim.x) {
         const int j = idx % lj, i = idx / lj;
         if (j == 0 || j == lj - 1 || i == 0 || i == li - 1) continue;
         const size_t c = idx;
@@ -468,6 +470,31 @@ __global__ void __launch_bounds__(256) enth_temp_kernel(const EnthTempArgs a)
         for (int t = 0; t < (int)blockDim.x; ++t) b += s_part[t];
         a.partial[blockIdx.x] = b;
     }
+}
+
+// ------------------------------------------------------------------ density
+
+// RHONP = PBACK / (BETA1 TK RBAR), RBAR = sum Y_k / W_k (src/unicornd-mild-sd-5.f:1056-1062)
+__global__ void density_kernel(const DevParams *Pp, double pback, int n, int npad, const double *tk, const double *y,
+                               double *rho)
+{
+    const DevParams &P = *Pp;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        double rbar = 0.0;
+        for (int k = 0; k < LSP; ++k) rbar = rbar + y[(size_t)k * npad + c] / P.WM[k];
+        rho[c] = pback / (P.BETA1 * tk[c] * rbar);
+    }
+}
+
+// edge rules of src/unicornd-mild-sd-5.f:1063-1068 (one CTA): the last column
+// extrapolated linearly, then the first row copied from the second
+__global__ void density_edges_kernel(int lj, int li, double *rho)
+{
+    const size_t last = (size_t)(li - 1) * lj;
+    for (int j = threadIdx.x; j < lj; j += blockDim.x)
+        rho[last + j] = 2.0 * rho[last + j - lj] - rho[last + j - 2 * (size_t)lj];
+    __syncthreads();
+    for (int i = threadIdx.x; i < li; i += blockDim.x) rho[(size_t)i * lj] = rho[(size_t)i * lj + 1];
 }
 
 }  // namespace uc

@@ -1018,11 +1018,11 @@ extern "C" int uc_assemble_faces(uc_ctx *ctx, double dt, double *e, double *w, d
 static __host__ __device__ size_t relax_plane(int lj, int li) { return (size_t)((li - 2) + (lj - 2) - 1) * (lj - 2); }
 
 // The relaxation on coefficients already in the skewed layout (cf, f0s) and
-// FPZ on entry f0 (natural layout). Writes fpz (natural layout) and the pass
-// count (device int); returns UC_E_* via err. isor >= 1.
+// FPZ on entry f0 (natural layout). Writes fpz (natural layout), the pass
+// count and its own error word (rb.flags[2 isor + 1], [2 isor + 2]); isor >= 1.
 static int launch_relax(uc_ctx *ctx, cudaStream_t st, int nsm, RelaxBuffers &rb, int lj, int li, const double *cf,
                         const double *f0, const double *f0s, int isor, double relx, double tol, double hnorm,
-                        double *fpz, int *status)
+                        double *fpz)
 {
     const int nj = lj - 2, ni = li - 2;
     const size_t plane = relax_plane(lj, li);
@@ -1049,14 +1049,14 @@ static int launch_relax(uc_ctx *ctx, cudaStream_t st, int nsm, RelaxBuffers &rb,
         rb.flags = nullptr;
         rb.isor_cap = 0;
         if (cudaMalloc((void **)&rb.rsdz, (size_t)isor * sizeof(double)) != cudaSuccess ||
-            cudaMalloc((void **)&rb.flags, (2 * (size_t)isor + 2) * sizeof(int)) != cudaSuccess)
+            cudaMalloc((void **)&rb.flags, (2 * (size_t)isor + 3) * sizeof(int)) != cudaSuccess)
             return set_err(ctx, UC_E_NOMEM, "relaxation flags");
         rb.isor_cap = isor;
     }
-    int *progress = rb.flags, *done = rb.flags + isor, *stop = rb.flags + 2 * isor, *passes = stop + 1;
+    int *progress = rb.flags, *done = rb.flags + isor, *stop = rb.flags + 2 * isor, *passes = stop + 1, *status = stop + 2;
     CK(cudaMemsetAsync(rb.flags, 0, 2 * (size_t)isor * sizeof(int), st));
-    const int init[2] = {isor, 0};
-    CK(cudaMemcpyAsync(stop, init, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(passes, 0, 2 * sizeof(int), st));
+    CK(cudaMemcpyAsync(stop, &isor, sizeof(int), cudaMemcpyHostToDevice, st));
     RelaxArgs a{};
     a.lj = lj; a.li = li; a.nj = nj; a.ni = ni; a.nstep = ni + nj - 1;
     a.cf = cf; a.f0 = f0; a.f0s = f0s; a.ring = rb.ring; a.rsdz = rb.rsdz;
@@ -1126,13 +1126,11 @@ extern "C" int uc_enthalpy_relax(int device, int lj, int li, const double *rho, 
     cudaStream_t st = nullptr;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return UC_E_CUDA;
     double *buf = nullptr;
-    int *status = nullptr;
     RelaxBuffers rb;
     int rc = UC_OK;
     int hp[2] = {0, 0};
     do {
-        if (cudaMalloc((void **)&buf, (8 * n + 7 * plane) * sizeof(double)) != cudaSuccess ||
-            cudaMalloc((void **)&status, 2 * sizeof(int)) != cudaSuccess) { rc = UC_E_NOMEM; break; }
+        if (cudaMalloc((void **)&buf, (8 * n + 7 * plane) * sizeof(double)) != cudaSuccess) { rc = UC_E_NOMEM; break; }
         double *d_rho = buf, *d_rhsz = d_rho + n, *d_ze = d_rhsz + n, *d_zw = d_ze + n, *d_zn = d_zw + n,
                *d_zs = d_zn + n, *d_f0 = d_zs + n, *d_out = d_f0 + n, *d_cf = d_out + n, *d_f0s = d_cf + 6 * plane;
         const double *src[7] = {rho, rhsz, ze, zw, zn, zs, fpz};
@@ -1140,24 +1138,25 @@ extern "C" int uc_enthalpy_relax(int device, int lj, int li, const double *rho, 
         bool ok = true;
         for (int q = 0; q < 7 && ok; ++q)
             ok = cudaMemcpyAsync(dst[q], src[q], n * sizeof(double), cudaMemcpyHostToDevice, st) == cudaSuccess;
-        if (!ok || cudaMemsetAsync(status, 0, 2 * sizeof(int), st) != cudaSuccess) { rc = UC_E_CUDA; break; }
+        if (!ok) { rc = UC_E_CUDA; break; }
         enth_skew_kernel<<<std::max(1, std::min((int)((n + 255) / 256), nsm * 4)), 256, 0, st>>>(
             lj, li, d_rho, d_rhsz, d_ze, d_zw, d_zn, d_zs, d_f0, d_cf, d_f0s);
         if (cudaGetLastError() != cudaSuccess) { rc = UC_E_CUDA; break; }
         rc = launch_relax(nullptr, st, nsm, rb, lj, li, d_cf, d_f0, d_f0s, isor, relx, tol,
-                          hnorm > 0.0 ? hnorm : (double)n, d_out, status);
+                          hnorm > 0.0 ? hnorm : (double)n, d_out);
         if (rc != UC_OK) break;
-        if (cudaMemcpyAsync(fpz, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-            cudaMemcpyAsync(hp, status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        if (cudaMemcpyAsync(hp, rb.flags + 2 * isor + 2, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaMemcpyAsync(hp + 1, rb.flags + 2 * isor + 1, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess) { rc = UC_E_CUDA; break; }
+        if (hp[0] == ST_OK &&
+            (cudaMemcpyAsync(fpz, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+             cudaStreamSynchronize(st) != cudaSuccess)) { rc = UC_E_CUDA; break; }
         if (hp[0] == ST_RELAX_TIMEOUT) { rc = UC_E_TIMEOUT; break; }
         if (passes) *passes = hp[1];
     } while (0);
     cudaStreamSynchronize(st);
     rb.release();
     if (buf) cudaFree(buf);
-    if (status) cudaFree(status);
     cudaStreamDestroy(st);
     return rc;
 }
@@ -1238,7 +1237,7 @@ extern "C" int uc_enthalpy_update(uc_ctx *ctx, const uc_enthalpy_opts *o, int *p
     int hpass = 1;
     if (o->isor >= 1) {
         RET_IF(launch_relax(ctx, ctx->stream, ctx->nsm, ctx->e_rb, ctx->lj, ctx->li, ctx->e_cf, ctx->ht, ctx->e_f0s,
-                            o->isor, o->relx, o->tol, hnorm, ctx->e_fpz, ctx->status));
+                            o->isor, o->relx, o->tol, hnorm, ctx->e_fpz));
     } else {
         CK(cudaMemcpyAsync(ctx->e_fpz, ctx->ht, np * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     }
@@ -1248,6 +1247,7 @@ extern "C" int uc_enthalpy_update(uc_ctx *ctx, const uc_enthalpy_opts *o, int *p
         a.P = ctx->dP; a.lj = ctx->lj; a.li = ctx->li; a.npad = ctx->npad;
         a.y = ctx->y; a.fpz = ctx->e_fpz; a.u = ctx->f_u; a.v = ctx->f_v; a.w = ctx->e_w;
         a.tk = ctx->tk; a.ht = ctx->ht; a.partial = ctx->e_part; a.status = ctx->status;
+        a.relax_status = o->isor >= 1 ? ctx->e_rb.flags + 2 * o->isor + 2 : nullptr;
         enth_temp_kernel<<<tgrid, 256, 0, ctx->stream>>>(a);
         CK(cudaGetLastError());
     }
@@ -1255,20 +1255,34 @@ extern "C" int uc_enthalpy_update(uc_ctx *ctx, const uc_enthalpy_opts *o, int *p
     std::vector<double> part(tgrid);
     int st = 0;
     CK(cudaMemcpyAsync(part.data(), ctx->e_part, tgrid * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(&st, ctx->status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    if (o->isor >= 1)
+    if (o->isor >= 1) {
         CK(cudaMemcpyAsync(&hpass, ctx->e_rb.flags + 2 * o->isor + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(&st, ctx->e_rb.flags + 2 * o->isor + 2, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    }
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->rc_start = false;
-    if (st == ST_RELAX_TIMEOUT) {
-        CK(cudaMemsetAsync(ctx->status, 0, sizeof(int), ctx->stream));
+    if (st != ST_OK)          // T and HT were left as they were
         return set_err(ctx, UC_E_TIMEOUT, "enthalpy relaxation: a wait between passes timed out on the device");
-    }
     double r = 0.0;
     for (double v : part) r += v;
     if (passes) *passes = hpass;
     if (resdh) *resdh = r / hnorm;
     return check_status(ctx);
+}
+
+extern "C" int uc_density(uc_ctx *ctx)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "no fields uploaded");
+    if (!ctx->have_grid || ctx->li < 3) return set_err(ctx, UC_E_STATE, "uc_density needs the grid of uc_set_grid (li >= 3)");
+    CK(cudaSetDevice(ctx->device));
+    density_kernel<<<std::max(1, std::min((ctx->n + 255) / 256, ctx->nsm * 4)), 256, 0, ctx->stream>>>(
+        ctx->dP, ctx->sc.pback, ctx->n, ctx->npad, ctx->tk, ctx->y, ctx->rho);
+    density_edges_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->lj, ctx->li, ctx->rho);
+    CK(cudaGetLastError());
+    ctx->have_rc = false;
+    ctx->rc_start = false;
+    return UC_OK;
 }
 
 extern "C" int uc_enthalpy_get(uc_ctx *ctx, double *ht, double *rhsz, double *ze, double *zw, double *zn, double *zs)

@@ -12,6 +12,9 @@ The reference ships no benchmark data, so the workloads are generated:
   (4) the other 47 species log-uniform in [1e-10, 1e-3]; then all 52 are
       renormalised so that sum Y = 1.
   Cells are ordered like the reference's arrays: r (J) fastest.
+* ``jet_flow(nz, nr, seed)``: geometry and a synthetic flow for that grid
+  (uniform spacing 1/(nr-1), cell-centre radius, a spreading round jet with
+  co-flow, seeded radial noise, an eddy viscosity that follows the jet).
 * ``batch_cells(n, seed)``: n independent cells with compositions of the
   heptane generator, T ~ U[300, 2400] K and p ~ U[0.8, 1.2] atm.
 
@@ -109,3 +112,19 @@ def sensible_enthalpy(T: np.ndarray, y: np.ndarray, poly: np.ndarray, wm: np.nda
         hk = a[:, 0] * t + a[:, 1] * t ** 2 / 2 + a[:, 2] * t ** 3 / 3 + a[:, 3] * t ** 4 / 4 + a[:, 4] * t ** 5 / 5 + a[:, 5]
         out[sel] = (y[:, sel] / wm[:, None] * hk).sum(axis=0) * scales["GASC"] / scales["WMSTR"]
     return out / scales["HSTR"] - (y * hfo[:, None]).sum(axis=0)
+
+
+def jet_flow(nz: int, nr: int, seed: int = 0, u_jet: float = 1.0, tmu: float = 1e-3) -> dict:
+    """Geometry and flow of the (z, r) grid of ``jet_field`` (r fastest, LJ = nr rows, LI = nz columns),
+    non-dimensional: spacing 1/(nr-1) in both directions (XXS, XXC, YYS, YYC), radius of the cell
+    centres (j + 1/2)/(nr-1), axial velocity u = u_jet exp(-(r/(0.2+0.02 z))^2) + 0.05 (r, z in grid
+    units, the spreading of the mixture fraction), radial velocity N(0, 0.01^2), eddy viscosity
+    tmu (0.1 + u/u_jet)."""
+    rng = np.random.default_rng(seed)
+    d = 1.0 / (nr - 1)
+    z = np.arange(nz, dtype=np.float64)[:, None]
+    r = np.arange(nr, dtype=np.float64)[None, :]
+    u = (u_jet * np.exp(-(r / (0.2 + 0.02 * z)) ** 2) + 0.05).reshape(-1)
+    v = rng.normal(0.0, 0.01, size=nz * nr)
+    return dict(lj=nr, li=nz, xxs=np.full(nz, d), xxc=np.full(nz, d), yys=np.full(nr, d), yyc=np.full(nr, d),
+                yr=np.tile((np.arange(nr) + 0.5) * d, nz), u=u, v=v, tmu=tmu * (0.1 + u / u_jet))

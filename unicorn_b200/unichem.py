@@ -122,6 +122,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.uc_set_enthalpy.argtypes = [vp, P, P]
     lib.uc_enthalpy_update.argtypes = [vp, ctypes.POINTER(EnthalpyOpts), IP, P]
     lib.uc_enthalpy_get.argtypes = [vp, P, P, P, P, P, P]
+    lib.uc_density.argtypes = [vp]
     lib.uc_enthalpy_relax.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, P, P, P, P, ctypes.c_int,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, IP]
     _lib = lib
@@ -338,6 +339,10 @@ class UniChem:
         resdh = np.zeros(1)
         self._ck_warn(self.lib.uc_enthalpy_update(self._h, ctypes.byref(o), ctypes.byref(passes), _p(resdh)))
         return passes.value, float(resdh[0])
+
+    def density(self):
+        """RHO of every cell from the gas law at PBACK with the grid's edge rules (main:1056-1073)."""
+        self._ck(self.lib.uc_density(self._h))
 
     def enthalpy_get(self):
         """(HT, RHSZ, ZE, ZW, ZN, ZS) [n] each, after an enthalpy update."""
