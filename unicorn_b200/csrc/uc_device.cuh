@@ -99,50 +99,6 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
         : "memory");
 }
 
-// Wall clock of the device (ns).
-__device__ __forceinline__ long long uc_gtimer()
-{
-    long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// One test of phase `parity` of the mbarrier (may suspend the thread briefly).
-__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
-{
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return done != 0;
-}
-
-// One non-blocking test of phase `parity` of the mbarrier.
-__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity)
-{
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return done != 0;
-}
-
-// Wait on phase `parity` for at most limit_ns of wall clock, spinning on the
-// non-blocking test (no suspension): false if it gave up.
-__device__ __forceinline__ bool mbar_wait_ns(uint64_t *bar, uint32_t parity, long long limit_ns)
-{
-    if (mbar_test(bar, parity)) return true;
-    const long long t0 = uc_gtimer();
-    for (int it = 0;; ++it) {
-        if (mbar_test(bar, parity)) return true;
-        if ((it & 255) == 255 && uc_gtimer() - t0 > limit_ns) return false;
-    }
-}
-
 // Bounded wait on phase `parity` of the mbarrier: returns false if it gave up.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int max_tries)
 {

@@ -14,7 +14,6 @@
 #include "chem_mixed_kernel.cuh"
 #include "props_kernel.cuh"
 #include "update_kernel.cuh"
-#include "update_staged_kernel.cuh"
 #include "integrate_kernel.cuh"
 #include "faces_kernel.cuh"
 #include "fdetail_kernel.cuh"
@@ -64,7 +63,6 @@ struct uc_ctx {
     int *status = nullptr, *passes = nullptr;
     bool have_fields = false, have_rc = false;
     int upd_grid = 0;
-    int upd_staged = 0, stg_grid = 0;  // FP64 update through the shared-memory RC ring (update_staged_kernel)
     // species-equation faces assembled on the device (grid, flow, coefficients)
     int lj = 0, li = 0, isym = 0;
     double sigsp = 0.0;
@@ -506,13 +504,6 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
         if (per_sm < 1) per_sm = 1;
         ctx->upd_grid = std::min(per_sm * ctx->nsm, std::max(1, (ctx->ntile + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32)));
         if ((rc = dalloc(ctx, &ctx->partial, 2 * (size_t)per_sm * ctx->nsm))) break;
-        e = cudaFuncSetAttribute(update_staged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)STG_SMEM);
-        if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "smem attribute: %s", cudaGetErrorString(e)); break; }
-        int stg_per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&stg_per_sm, update_staged_kernel, STG_THREADS, STG_SMEM);
-        stg_per_sm = std::max(1, std::min(stg_per_sm, per_sm * UPD_THREADS / STG_THREADS));
-        ctx->stg_grid = std::min(stg_per_sm * ctx->nsm, std::max(1, (ctx->ntile + STG_WARPS - 1) / STG_WARPS));
-        if (const char *k = getenv("UNICHEM_UPDATE")) ctx->upd_staged = !strcmp(k, "staged");
         e = cudaDeviceSynchronize();
         if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "init: %s", cudaGetErrorString(e)); break; }
     } while (0);
@@ -790,26 +781,17 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
     a.face_sum = fs; a.face_nbr = fn; a.y = ctx->y; a.soot = ctx->soot; a.partial = ctx->partial;
     a.hold = hold;
     a.passes = ctx->passes;
-    a.status = ctx->status;
     a.dt = dt; a.sor1 = relx; a.tol = tol; a.spnorm = spnorm > 0.0 ? spnorm : (double)ctx->n * (LSP - 1);
     a.isor = isor; a.n = ctx->n; a.npad = ctx->npad; a.ntile = ctx->ntile;
     void *args[] = {&a};
     int slot;
     prof_begin(ctx, UC_K_UPDATE, slot);
-    if (ctx->rc_prec != UC_MIXED && ctx->upd_staged) {
-        CK(cudaLaunchCooperativeKernel((const void *)update_staged_kernel, dim3(ctx->stg_grid), dim3(STG_THREADS), args,
-                                       STG_SMEM, ctx->stream));
-    } else {
-        const void *kfn = ctx->rc_prec == UC_MIXED ? (const void *)update_kernel<float> : (const void *)update_kernel<double>;
-        CK(cudaLaunchCooperativeKernel(kfn, dim3(ctx->upd_grid), dim3(UPD_THREADS), args, UPD_SMEM, ctx->stream));
-    }
+    const void *kfn = ctx->rc_prec == UC_MIXED ? (const void *)update_kernel<float> : (const void *)update_kernel<double>;
+    CK(cudaLaunchCooperativeKernel(kfn, dim3(ctx->upd_grid), dim3(UPD_THREADS), args, UPD_SMEM, ctx->stream));
     prof_end(ctx, slot);
     if (passes) {
-        int st = ST_OK;
         CK(cudaMemcpyAsync(passes, ctx->passes, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(&st, ctx->status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
-        if (st == ST_TMA_TIMEOUT) return check_status(ctx);
     }
     ctx->have_rc = false;   // the RC plane belongs to the state before the update
     ctx->rc_start = true;   // ... which the enthalpy equation uses (solveh.f:116-1145)
@@ -897,7 +879,6 @@ extern "C" int uc_stat(uc_ctx *ctx, const char *name, double *value)
     if (!ctx || !name || !value) return UC_E_ARG;
     if (!strcmp(name, "tiles")) { *value = ctx->ntile; return UC_OK; }
     if (!strcmp(name, "int_warps")) { *value = ctx->int_warps; return UC_OK; }
-    if (!strcmp(name, "update_staged")) { *value = ctx->upd_staged; return UC_OK; }
     if (!strcmp(name, "int_sorted")) { *value = ctx->int_sorted; return UC_OK; }
     if (!strcmp(name, "int_tune_best_ms")) { *value = ctx->tune_best; return UC_OK; }
     if (!strcmp(name, "int_tune_worst_ms")) { *value = ctx->tune_worst; return UC_OK; }

@@ -36,7 +36,6 @@ struct UpdArgs {
     int *passes;                                 // out: pass count as ISOR1 reports it
     double dt, sor1, tol, spnorm;
     int isor, n, npad, ntile;
-    int *status;                                 // error word (update_staged_kernel: a chunk never landed)
 };
 
 #ifndef UC_UPD_WARPS

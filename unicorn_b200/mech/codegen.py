@@ -38,7 +38,7 @@ class Leaf:
         if self.kind == "RC":
             return ctx.rc(self.idx)
         if self.kind == "yo":
-            return ctx.yo(self.idx) if hasattr(ctx, "yo") else f"YO({self.idx})"
+            return f"YO({self.idx})"
         if self.kind == "yn":
             return f"YN({self.idx})"
         if self.kind == "y0":
@@ -210,116 +210,6 @@ def gen_update_program(mech: dict) -> str:
     L.append("// RC rows read by each species block (first-use order): rows [off[b], off[b+1]).")
     L.append(f"static __device__ const int16_t uc_upd_row_off[{len(offs)}] = {{{', '.join(map(str, offs))}}};")
     L.append(f"static __device__ const int16_t uc_upd_rows[{len(rows)}] = {{{', '.join(map(str, rows))}}};")
-    L.append("#endif")
-    return "\n".join(L) + "\n\n" + gen_staged_program(blocks)
-
-
-# ------------------------------------------------------------------ staged update program
-
-STG_C = 16      # RC rows per chunk of the staged program
-STG_NR = 5      # chunks resident in a warp's ring
-
-
-class _StagedCtx:
-    """Emission context of the staged program: every RC use gets a position in
-    the warp's row stream (the rows a pass copies into shared memory, in use
-    order). A row already in the stream is reused while its chunk is at most
-    STG_NR - 2 chunks behind the newest one (still resident); otherwise it is
-    appended again."""
-
-    def __init__(self, C: int, NR: int):
-        self.C, self.NR = C, NR
-        self.L: list[int] = []
-        self.pos_of: dict[int, int] = {}
-        self.cur: list[int] = []
-        self.updated: set[int] = set()
-        self.shadow: list[int] = []
-
-    def yo(self, k: int) -> str:
-        """Start-of-pass value of species k: in place (YO) until k is updated, then from the
-        shadow copy the tile keeps for the few species read at their old value afterwards."""
-        if k not in self.updated:
-            return f"YO({k})"
-        if k not in self.shadow:
-            self.shadow.append(k)
-        return f"YOS({self.shadow.index(k)})"
-
-    def rc(self, r0: int) -> str:
-        newest = (len(self.L) - 1) // self.C if self.L else 0
-        p = self.pos_of.get(r0)
-        if p is None or p // self.C < newest - (self.NR - 2):
-            p = len(self.L)
-            self.L.append(r0)
-            self.pos_of[r0] = p
-        self.cur.append(p)
-        return f"RCS({p})"
-
-
-def gen_staged_program(blocks, C: int = STG_C, NR: int = STG_NR) -> str:
-    ctx = _StagedCtx(C, NR)
-    stmts: list[tuple[str, list[int]]] = []
-
-    def add_sum(terms, acc):
-        for i, (sgn, t) in enumerate(terms):
-            ctx.cur = []
-            v = t.c(ctx)
-            txt = f"{acc} = {'' if sgn > 0 else '-'}{v};" if i == 0 else f"{acc} = {acc} {'+' if sgn > 0 else '-'} {v};"
-            stmts.append((txt, sorted({p // C for p in ctx.cur})))
-
-    for b in blocks:
-        k = b["species"]
-        ctx.updated = {x["species"] for x in blocks[:blocks.index(b)]}
-        if b["prod"] is not None:
-            add_sum(b["prod"], "prod")
-        add_sum(b["extra"], "extra")
-        stmts.append((f"rhs1 = rho * Y0({k}) + dt * WM({k}) * (prod + extra);", []))
-        if b["loss"] is None:
-            stmts.append(("rhs2 = 0.0;", []))
-        else:
-            add_sum(b["loss"], "loss")
-            stmts.append((f"rhs2 = -(dt * WM({k}) * loss);", []))
-        stmts.append((f"ppp = rho - FACE_SUM({k});", []))
-        stmts.append((f"fnew = sor2 * YO({k}) + (rhs1 - FACE_NBR({k})) * sor1 / (ppp - rhs2);", []))
-        stmts.append((f"rsd += fabs(YO({k}) - fnew);", []))
-        stmts.append((f"UC_UPDATE_TAIL({k});", []))
-    M = len(ctx.L)
-    nc = (M + C - 1) // C
-    ncp = (nc + NR - 1) // NR * NR
-    first, last = {}, {}
-    for si, (_, chs) in enumerate(stmts):
-        for c in chs:
-            first.setdefault(c, si)
-            last[c] = si
-    for c in range(nc - NR):
-        assert last[c] < first[c + NR], f"chunk {c} is still read after chunk {c + NR} is needed"
-    out = []
-    waited = -1
-    for si, (txt, chs) in enumerate(stmts):
-        for c in chs:
-            while waited < c:
-                waited += 1
-                out.append(f"UC_RC_WAIT({waited});")
-        out.append(txt)
-        for c in sorted(c for c in chs if last[c] == si):
-            out.append(f"UC_RC_RELEASE({c});")
-    for c in range(nc, ncp):
-        out += [f"UC_RC_WAIT({c});", f"UC_RC_RELEASE({c});"]
-    rows = ctx.L + [-1] * (ncp * C - M)
-    L = ["// Staged form of the same program: RCS(i) reads position i of the warp's",
-         f"// row stream from shared memory ({M} rows per pass in chunks of {C}, {NR} chunks",
-         "// resident); UC_RC_WAIT(c) waits for chunk c, UC_RC_RELEASE(c) hands its",
-         "// slot to chunk c + UC_STG_NR. Rows are read in the order of uc_stg_rows (-1: none).",
-         "// YOS(m): start-of-pass value of species uc_stg_shadow[m], read after that species' update.",
-         f"#define UC_STG_C {C}", f"#define UC_STG_NR {NR}", f"#define UC_STG_ROWS {M}", f"#define UC_STG_NCHUNK {ncp}",
-         f"#define UC_STG_NSHADOW {len(ctx.shadow)}",
-         "#define UC_UPDATE_PROGRAM_STAGED() do { \\",
-         "    double prod = 0.0, extra, loss, rhs1, rhs2, ppp, fnew; \\"]
-    L.extend("    " + x + " \\" for x in out)
-    L.append("} while (0)")
-    L.append("#ifdef __CUDACC__")
-    L.append(f"static __constant__ int16_t uc_stg_rows[{len(rows)}] = {{{', '.join(map(str, rows))}}};")
-    L.append(f"static __device__ const int8_t uc_stg_shadow[{max(1, len(ctx.shadow))}] = "
-             f"{{{', '.join(map(str, ctx.shadow or [0]))}}};")
     L.append("#endif")
     return "\n".join(L) + "\n"
 
