@@ -229,9 +229,13 @@ def roofline(res, n, steps):
     npad = (n + 31) // 32 * 32
     passes = sum(res["passes"][-steps:]) / max(1, steps)
     # algorithmic bytes per launch (per-cell figures x cells)
+    traffic = None
     if name == "update":
         per_cell = passes * (544 + 52 + 52 + 6 + 2 + 2) * 8 + (52 + 2) * 8
         unit_note = f"per cell and launch: {passes:.1f} passes x (RC 544 + Y 52 in + 52 out + SOUR 6 + soot 4) x 8 B"
+        # DRAM read + write of one update_kernel<double> launch under ncu (65,536 C2 cells, 5 passes:
+        # 2.468 GB + 0.130 GB), per cell and pass, scaled to this launch by cells x passes run
+        traffic = round(7928.0 * n * min(passes, ISOR))
     elif name == "chem":
         per_cell = (52 + 4) * 8 + (544 + 52 + 52 + 1 + 6) * 8
         unit_note = "per cell: read T, rho, soot, Y (56 x 8 B); write RC 544, QDSP 52, dw/dY 52, QDOT, SOUR 6"
@@ -241,7 +245,7 @@ def roofline(res, n, steps):
     bytes_per_launch = per_cell * n
     achieved = bytes_per_launch / (ms / cnt / 1e3) / 1e9
     return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "peak_source": src,
-            "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None, "bytes_per_launch": bytes_per_launch,
+            "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": traffic, "bytes_per_launch": bytes_per_launch,
             "avg_launch_ms": ms / cnt, "bytes_rule": unit_note}
 
 
