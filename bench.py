@@ -233,9 +233,10 @@ def roofline(res, n, steps):
     if name == "update":
         per_cell = passes * (544 + 52 + 52 + 6 + 2 + 2) * 8 + (52 + 2) * 8
         unit_note = f"per cell and launch: {passes:.1f} passes x (RC 544 + Y 52 in + 52 out + SOUR 6 + soot 4) x 8 B"
-        # DRAM read + write of one update_kernel<double> launch under ncu (65,536 C2 cells, 5 passes:
-        # 2.468 GB + 0.130 GB), per cell and pass, scaled to this launch by cells x passes run
-        traffic = round(7928.0 * n * min(passes, ISOR))
+        # DRAM read + write of one launch of the FP64 update (Y in place, 14 warps per SM) under ncu
+        # (65,536 C2 cells, 5 passes: 3.723 GB + 0.193 GB), per cell and pass, scaled to this launch
+        # by cells x passes run
+        traffic = round(11951.0 * n * min(passes, ISOR))
     elif name == "chem":
         per_cell = (52 + 4) * 8 + (544 + 52 + 52 + 1 + 6) * 8
         unit_note = "per cell: read T, rho, soot, Y (56 x 8 B); write RC 544, QDSP 52, dw/dY 52, QDOT, SOUR 6"

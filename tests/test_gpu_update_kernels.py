@@ -1,0 +1,70 @@
+"""The two FP64 species-update kernels against each other and the oracle: the
+default one with Y in place (update_kernel<double, 14, true>, 14 warps per SM)
+and the two-Y-set one (8 warps per SM, UNICHEM_UPDATE=twoset at uc_init).
+Same pass counts, Y within 1e-9 of the oracle (the tolerance of the FP64
+update tests), on the C1 field, a many-tile batch that runs several rounds per
+warp, and frozen transport terms."""
+import numpy as np
+import pytest
+
+from test_gpu_parity import assert_rel, c1  # noqa: F401  (c1: the 101x61 CH4 field)
+from unicorn_b200.fields import batch_cells, nondimensional
+
+pytestmark = pytest.mark.gpu
+KINDS = ["inplace", "twoset"]
+
+
+@pytest.fixture(scope="module")
+def cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("a GPU test ran without a CUDA device")
+    from unicorn_b200 import unichem
+    return unichem
+
+
+def run_update(cuda, monkeypatch, kind, tk, rho, y, **kw):
+    monkeypatch.setenv("UNICHEM_UPDATE", kind)
+    with cuda.UniChem(len(tk)) as u:
+        assert u.stat("update_ip_warps") == (0.0 if kind == "twoset" else 14.0)
+        u.upload(tk, rho, y)
+        u.ckrates()
+        passes = u.solvesp(1e-3, **kw)
+        _, _, yg, s1, _ = u.download()
+    return passes, yg, s1
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("isor,tol", [(1, 1e-8), (5, 0.0)])
+def test_inplace_matches_oracle(cuda, oracle, monkeypatch, c1, kind, isor, tol):
+    tk, rho, y = c1
+    passes, yg, s1 = run_update(cuda, monkeypatch, kind, tk, rho, y, isor=isor, relx=0.99, tol=tol)
+    rc, sour = oracle.rates(tk, rho, y)
+    yo, so, po = oracle.species_update(rho, y, rc, sour, 1e-3, isor=isor, tol=tol)
+    assert passes == po
+    assert_rel(yg, yo, 1e-9, 1e-18, "Y after update")
+    assert_rel(s1, so[0], 1e-9, 1e-30, "soot mass fraction")
+
+
+def test_inplace_many_rounds_matches_twoset(cuda, oracle, monkeypatch):
+    """65,536 cells: 2,048 tiles, several rounds per warp, converged passes."""
+    f = batch_cells(65536, seed=5)
+    tk, rho = nondimensional(f, oracle.scales, oracle.wm)
+    pa, ya, _ = run_update(cuda, monkeypatch, "twoset", tk, rho, f.y, isor=100, relx=0.99, tol=1e-8)
+    pb, yb, _ = run_update(cuda, monkeypatch, "inplace", tk, rho, f.y, isor=100, relx=0.99, tol=1e-8)
+    assert pa == pb and pa > 3
+    assert_rel(yb, ya, 1e-9, 1e-18, "Y in place vs two Y sets")
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_inplace_frozen_transport(cuda, oracle, monkeypatch, c1, kind):
+    tk, rho, y = c1
+    n = len(tk)
+    rng = np.random.default_rng(4)
+    fs = rng.uniform(-0.02, 0.0, (51, n)) * rho
+    fn = fs * y[:51] * rng.uniform(0.9, 1.1, (51, n))
+    passes, yg, _ = run_update(cuda, monkeypatch, kind, tk, rho, y, isor=3, tol=0.0, face_sum=fs, face_nbr=fn)
+    rc, sour = oracle.rates(tk, rho, y)
+    yo, _, po = oracle.species_update(rho, y, rc, sour, 1e-3, isor=3, tol=0.0, face_sum=fs, face_nbr=fn)
+    assert passes == po
+    assert_rel(yg, yo, 1e-9, 1e-18, "Y with frozen transport")

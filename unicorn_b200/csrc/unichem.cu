@@ -63,6 +63,7 @@ struct uc_ctx {
     int *status = nullptr, *passes = nullptr;
     bool have_fields = false, have_rc = false;
     int upd_grid = 0;
+    int upd_ip = 0, ip_grid = 0;       // FP64 update with Y in place: warps per CTA (0: two Y sets, 8 warps)
     // species-equation faces assembled on the device (grid, flow, coefficients)
     int lj = 0, li = 0, isym = 0;
     double sigsp = 0.0;
@@ -435,6 +436,17 @@ static int check_status(uc_ctx *ctx)
     return UC_OK;
 }
 
+// FP64 update with Y in place: 14 warps per CTA (one CTA per SM). Measured on
+// the C2 sweep against the two-Y-set kernel at 8 warps: 0.56 against 0.65 ms
+// per pass; 12, 16 and 17 warps gave 0.62, 0.57 and 0.66 (fewer registers per
+// thread as the warps grow: 168, 128, 96).
+constexpr int UPD_IP_WARPS = 14;
+static void ip_kernel(const void **fn, size_t *sm)
+{
+    *fn = (const void *)update_kernel<double, UPD_IP_WARPS, true>;
+    *sm = upd_smem<UPD_IP_WARPS, true>();
+}
+
 #define RET_IF(x)                 \
     do {                          \
         int r_ = (x);             \
@@ -504,6 +516,18 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
         if (per_sm < 1) per_sm = 1;
         ctx->upd_grid = std::min(per_sm * ctx->nsm, std::max(1, (ctx->ntile + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32)));
         if ((rc = dalloc(ctx, &ctx->partial, 2 * (size_t)per_sm * ctx->nsm))) break;
+        ctx->upd_ip = UPD_IP_WARPS;        // UNICHEM_UPDATE=twoset selects the two-Y-set kernel instead
+        if (const char *k = getenv("UNICHEM_UPDATE")) if (!strcmp(k, "twoset")) ctx->upd_ip = 0;
+        if (ctx->upd_ip) {
+            const void *fn; size_t sm;
+            ip_kernel(&fn, &sm);
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "smem attribute: %s", cudaGetErrorString(e)); break; }
+            int ip_per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ip_per_sm, fn, ctx->upd_ip * 32, sm);
+            ip_per_sm = std::max(1, std::min(ip_per_sm, per_sm));
+            ctx->ip_grid = std::min(ip_per_sm * ctx->nsm, std::max(1, (ctx->ntile + ctx->upd_ip - 1) / ctx->upd_ip));
+        }
         e = cudaDeviceSynchronize();
         if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "init: %s", cudaGetErrorString(e)); break; }
     } while (0);
@@ -786,8 +810,14 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
     void *args[] = {&a};
     int slot;
     prof_begin(ctx, UC_K_UPDATE, slot);
-    const void *kfn = ctx->rc_prec == UC_MIXED ? (const void *)update_kernel<float> : (const void *)update_kernel<double>;
-    CK(cudaLaunchCooperativeKernel(kfn, dim3(ctx->upd_grid), dim3(UPD_THREADS), args, UPD_SMEM, ctx->stream));
+    if (ctx->rc_prec != UC_MIXED && ctx->upd_ip) {
+        const void *fn; size_t sm;
+        ip_kernel(&fn, &sm);
+        CK(cudaLaunchCooperativeKernel(fn, dim3(ctx->ip_grid), dim3(ctx->upd_ip * 32), args, sm, ctx->stream));
+    } else {
+        const void *kfn = ctx->rc_prec == UC_MIXED ? (const void *)update_kernel<float> : (const void *)update_kernel<double>;
+        CK(cudaLaunchCooperativeKernel(kfn, dim3(ctx->upd_grid), dim3(UPD_THREADS), args, UPD_SMEM, ctx->stream));
+    }
     prof_end(ctx, slot);
     if (passes) {
         CK(cudaMemcpyAsync(passes, ctx->passes, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -879,6 +909,7 @@ extern "C" int uc_stat(uc_ctx *ctx, const char *name, double *value)
     if (!ctx || !name || !value) return UC_E_ARG;
     if (!strcmp(name, "tiles")) { *value = ctx->ntile; return UC_OK; }
     if (!strcmp(name, "int_warps")) { *value = ctx->int_warps; return UC_OK; }
+    if (!strcmp(name, "update_ip_warps")) { *value = ctx->upd_ip; return UC_OK; }
     if (!strcmp(name, "int_sorted")) { *value = ctx->int_sorted; return UC_OK; }
     if (!strcmp(name, "int_tune_best_ms")) { *value = ctx->tune_best; return UC_OK; }
     if (!strcmp(name, "int_tune_worst_ms")) { *value = ctx->tune_worst; return UC_OK; }

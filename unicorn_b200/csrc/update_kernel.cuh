@@ -5,7 +5,12 @@
 // reference's statement sequence with its A-terms resolved into products of
 // RC, the pass-start Y (YO) and the freshly updated Y (YN). Both Y sets live
 // in shared memory ([52][32] per warp each), so registers go to keeping RC
-// loads in flight. The warps of a CTA can run the program in lockstep (a
+// loads in flight. The in-place form (IP, the FP64 default) keeps one set
+// ([51][32] per warp: each species is overwritten by its own update), so 14
+// warps fit per SM instead of 8; the eight species whose start-of-pass value
+// the program still reads after their update (through A-terms built before
+// it) are read from the tile's Y rows in global memory, which hold the
+// start-of-pass values until the tile's program has ended. The warps of a CTA can run the program in lockstep (a
 // barrier after every species) so that the instruction cache holds only the code of
 // the current species (optional, see UC_LOCKSTEP); RC (the plane written by
 // the rate kernel, [544][npad]) is read with loads that do not allocate in L1
@@ -110,25 +115,38 @@ __device__ __forceinline__ void prefetch_block_rows(int b, const RCT *tile_base,
     }
 }
 
+// Shared memory of a CTA of NW warps: two Y sets [52][32] per warp, or with
+// IP (in place) one set of the 51 updated species. In place, the few species
+// the program reads at their start-of-pass value after their own update are
+// read from the Y rows in global memory, which keep the start-of-pass values
+// until the tile's program ends.
+template <int NW, bool IP>
+constexpr size_t upd_smem()
+{
+    return (size_t)NW * (IP ? (LSP - 1) : 2 * LSP) * TILE * sizeof(double);
+}
+
 // RCT: storage type of the RC plane (double for the FP64 form, float for the
-// mixed form); the update itself is FP64 in both.
-template <typename RCT>
-__global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
+// mixed form); the update itself is FP64 in both. NW warps per CTA; IP: Y in
+// place (one array per warp), so that more warps fit per SM.
+template <typename RCT, int NW = UPD_WARPS, bool IP = false>
+__global__ void __launch_bounds__(NW * 32, 1) update_kernel(const UpdArgs a)
 {
     // the plane is addressed through the kernel parameter itself (not a local
     // pointer copy): ptxas then rebuilds addresses from the parameter bank and
     // the generated program fits in registers (a local copy spilled 5 KB/thread)
+    static_assert(!IP || sizeof(RCT) == 8, "the in-place form reads the FP64 plane");
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
     extern __shared__ __align__(128) double s_upd[];
-    __shared__ double s_part[UPD_WARPS];
+    __shared__ double s_part[NW];
     __shared__ double s_wm[LSP];
     const DevParams &P = *a.P;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double *syo = s_upd + (size_t)wib * 2 * LSP * TILE + lane;   // YO(k) = syo[k*32]
-    double *syn = syo + LSP * TILE;                              // YN(k) = syn[k*32]
-    const int nwarp = gridDim.x * UPD_WARPS;
-    const int gwarp = blockIdx.x * UPD_WARPS + wib;
+    double *syo = s_upd + (size_t)wib * (IP ? LSP - 1 : 2 * LSP) * TILE + lane;   // YO(k) = syo[k*32]
+    double *syn = IP ? syo : syo + LSP * TILE;                   // YN(k) = syn[k*32]
+    const int nwarp = gridDim.x * NW;
+    const int gwarp = blockIdx.x * NW + wib;
     const int rounds = (a.ntile + nwarp - 1) / nwarp;            // same trip count for every warp of the grid
     const double sor1 = a.sor1, sor2 = 1.0 - a.sor1, dt = a.dt;
     const size_t np = a.npad;
@@ -166,7 +184,14 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
 #define UC_UPDATE_SYNC() do { } while (0)
 #endif
 #define UC_UPDATE_BLOCK_BEGIN(b) do { } while (0)
-                if (sizeof(RCT) == 4 && a.tile_flag && a.tile_flag[tile]) {
+#define YOS(m) __ldcg(a.y + (size_t)uc_ip_shadow[m] * np + cell)
+                if constexpr (IP) {
+#define RC(r) ld_hint(a.rc + (size_t)(r) * np + cell, keep)
+#define RC_LAST(r) ld_hint(a.rc + (size_t)(r) * np + cell, drop)
+                    UC_UPDATE_PROGRAM_IP();
+#undef RC
+#undef RC_LAST
+                } else if (sizeof(RCT) == 4 && a.tile_flag && a.tile_flag[tile]) {
                     // a tile the mixed rate kernel sent to FP64: its RC is in the FP64 plane
 #define RC(r) ld_hint(a.rc + (size_t)(r) * np + cell, keep)
 #define RC_LAST(r) ld_hint(a.rc + (size_t)(r) * np + cell, drop)
@@ -192,6 +217,7 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
 #undef UC_UPDATE_TAIL
 #undef UC_UPDATE_SYNC
 #undef UC_UPDATE_BLOCK_BEGIN
+#undef YOS
                 // soot mass fraction and number density (solvesp.f:2807-2832)
                 const double s1 = a.soot[cell], s2 = a.soot[np + cell];
                 const double so0 = so[0], so1 = so[1], so2 = so[2], so3 = so[3], so4 = so[4], so5 = so[5];
@@ -220,7 +246,7 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
         __syncthreads();
         if (threadIdx.x == 0) {
             double b = 0.0;
-            for (int w = 0; w < UPD_WARPS; ++w) b += s_part[w];
+            for (int w = 0; w < NW; ++w) b += s_part[w];
             a.partial[(pass & 1) * gridDim.x + blockIdx.x] = b;
         }
         grid.sync();
@@ -230,8 +256,8 @@ __global__ void __launch_bounds__(UPD_THREADS, 1) update_kernel(const UpdArgs a)
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *a.passes = pass;   // ISOR1+1 if not converged
     // N2 closure and renormalisation (solvesp.f:2839-2915)
-    for (size_t cell = (size_t)blockIdx.x * UPD_THREADS + threadIdx.x; cell < (size_t)a.n;
-         cell += (size_t)gridDim.x * UPD_THREADS) {
+    for (size_t cell = (size_t)blockIdx.x * (NW * 32) + threadIdx.x; cell < (size_t)a.n;
+         cell += (size_t)gridDim.x * (NW * 32)) {
         if (a.hold && a.hold[cell]) continue;
         double ft = a.y[cell];
         for (int k = 1; k < LSP - 1; ++k) ft = ft + a.y[k * np + cell];

@@ -38,7 +38,7 @@ class Leaf:
         if self.kind == "RC":
             return ctx.rc(self.idx)
         if self.kind == "yo":
-            return f"YO({self.idx})"
+            return ctx.yo(self.idx) if hasattr(ctx, "yo") else f"YO({self.idx})"
         if self.kind == "yn":
             return f"YN({self.idx})"
         if self.kind == "y0":
@@ -210,6 +210,61 @@ def gen_update_program(mech: dict) -> str:
     L.append("// RC rows read by each species block (first-use order): rows [off[b], off[b+1]).")
     L.append(f"static __device__ const int16_t uc_upd_row_off[{len(offs)}] = {{{', '.join(map(str, offs))}}};")
     L.append(f"static __device__ const int16_t uc_upd_rows[{len(rows)}] = {{{', '.join(map(str, rows))}}};")
+    L.append("#endif")
+    return "\n".join(L) + "\n\n" + gen_inplace_program(blocks, uses)
+
+
+# ------------------------------------------------------------------ in-place form
+
+class _InPlaceCtx(_Ctx):
+    """Emission context of the in-place program: one Y array per tile, each
+    species overwritten by its own update. A species' start-of-pass value read
+    after its update (through an A-term built before it) comes from a shadow
+    copy YOS(m) the tile keeps for those few species."""
+
+    def __init__(self, last_use: dict):
+        super().__init__(last_use)
+        self.updated: set[int] = set()
+        self.shadow: list[int] = []
+
+    def yo(self, k: int) -> str:
+        if k not in self.updated:
+            return f"YO({k})"
+        if k not in self.shadow:
+            self.shadow.append(k)
+        return f"YOS({self.shadow.index(k)})"
+
+
+def gen_inplace_program(blocks, uses: dict) -> str:
+    ctx = _InPlaceCtx(uses)
+    body = []
+    for b in blocks:
+        k = b["species"]
+        if b["prod"] is not None:
+            body += emit_sum(b["prod"], ctx, "prod")
+        body += emit_sum(b["extra"], ctx, "extra")
+        body.append(f"rhs1 = rho * Y0({k}) + dt * WM({k}) * (prod + extra);")
+        if b["loss"] is None:
+            body.append("rhs2 = 0.0;")
+        else:
+            body += emit_sum(b["loss"], ctx, "loss")
+            body.append(f"rhs2 = -(dt * WM({k}) * loss);")
+        body.append(f"ppp = rho - FACE_SUM({k});")
+        body.append(f"fnew = sor2 * YO({k}) + (rhs1 - FACE_NBR({k})) * sor1 / (ppp - rhs2);")
+        body.append(f"rsd += fabs(YO({k}) - fnew);")
+        body.append(f"UC_UPDATE_TAIL({k});")
+        ctx.updated.add(k)
+    L = ["// In-place form of the same program: YO(k) and YN(k) name one array; YOS(m)",
+         "// is the start-of-pass value of species uc_ip_shadow[m], read after that",
+         "// species' own update.",
+         f"#define UC_IP_NSHADOW {len(ctx.shadow)}",
+         "#define UC_UPDATE_PROGRAM_IP() do { \\",
+         "    double prod = 0.0, extra, loss, rhs1, rhs2, ppp, fnew; \\"]
+    L.extend("    " + x + " \\" for x in body)
+    L.append("} while (0)")
+    L.append("#ifdef __CUDACC__")
+    L.append(f"static __constant__ int8_t uc_ip_shadow[{max(1, len(ctx.shadow))}] = "
+             f"{{{', '.join(map(str, ctx.shadow or [0]))}}};")
     L.append("#endif")
     return "\n".join(L) + "\n"
 
