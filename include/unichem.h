@@ -247,7 +247,7 @@ int uc_profile_read(uc_ctx *ctx, double *ms, int *launches);
  *   "tiles"               32-cell tiles of the context
  *   "mixed_fp64_tiles"    tiles the last UC_MIXED rate call sent to FP64 because a
  *                         rate left the FP32 range
- *   "update_ip_warps"     warps per CTA of the FP64 species update with Y in place
+ *   "update_ip_warps"     warps per CTA of the species update with Y in place
  *                         (14); 0 when UNICHEM_UPDATE=twoset was set at uc_init and
  *                         the two-Y-set kernel (8 warps) runs instead
  * Returns UC_E_ARG for an unknown name. */

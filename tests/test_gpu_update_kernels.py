@@ -68,3 +68,18 @@ def test_inplace_frozen_transport(cuda, oracle, monkeypatch, c1, kind):
     yo, _, po = oracle.species_update(rho, y, rc, sour, 1e-3, isor=3, tol=0.0, face_sum=fs, face_nbr=fn)
     assert passes == po
     assert_rel(yg, yo, 1e-9, 1e-18, "Y with frozen transport")
+
+
+def test_inplace_mixed_matches_twoset(cuda, oracle, monkeypatch, c1):
+    """The mixed form (FP32 RC plane, flagged tiles from the FP64 plane) through both kernels."""
+    tk, rho, y = c1
+    out = {}
+    for kind in ("twoset", "inplace"):
+        monkeypatch.setenv("UNICHEM_UPDATE", kind)
+        with cuda.UniChem(len(tk)) as u:
+            u.upload(tk, rho, y)
+            passes = u.sweep(1e-3, precision=cuda.MIXED, isor=100, relx=0.99, tol=1e-8)
+            assert u.stat("mixed_fp64_tiles") > 0            # both planes are read
+            out[kind] = (passes, u.download()[2])
+    assert out["twoset"][0] == out["inplace"][0]
+    assert_rel(out["inplace"][1], out["twoset"][1], 1e-9, 1e-18, "mixed Y in place vs two Y sets")

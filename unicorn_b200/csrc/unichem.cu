@@ -441,9 +441,10 @@ static int check_status(uc_ctx *ctx)
 // per pass; 12, 16 and 17 warps gave 0.62, 0.57 and 0.66 (fewer registers per
 // thread as the warps grow: 168, 128, 96).
 constexpr int UPD_IP_WARPS = 14;
-static void ip_kernel(const void **fn, size_t *sm)
+static void ip_kernel(bool mixed, const void **fn, size_t *sm)
 {
-    *fn = (const void *)update_kernel<double, UPD_IP_WARPS, true>;
+    *fn = mixed ? (const void *)update_kernel<float, UPD_IP_WARPS, true>
+                : (const void *)update_kernel<double, UPD_IP_WARPS, true>;
     *sm = upd_smem<UPD_IP_WARPS, true>();
 }
 
@@ -519,13 +520,17 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
         ctx->upd_ip = UPD_IP_WARPS;        // UNICHEM_UPDATE=twoset selects the two-Y-set kernel instead
         if (const char *k = getenv("UNICHEM_UPDATE")) if (!strcmp(k, "twoset")) ctx->upd_ip = 0;
         if (ctx->upd_ip) {
-            const void *fn; size_t sm;
-            ip_kernel(&fn, &sm);
+            const void *fn, *fnm; size_t sm;
+            ip_kernel(true, &fnm, &sm);
+            e = cudaFuncSetAttribute(fnm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "smem attribute: %s", cudaGetErrorString(e)); break; }
+            ip_kernel(false, &fn, &sm);
             e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "smem attribute: %s", cudaGetErrorString(e)); break; }
-            int ip_per_sm = 0;
+            int ip_per_sm = 0, ipm_per_sm = 0;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ip_per_sm, fn, ctx->upd_ip * 32, sm);
-            ip_per_sm = std::max(1, std::min(ip_per_sm, per_sm));
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ipm_per_sm, fnm, ctx->upd_ip * 32, sm);
+            ip_per_sm = std::max(1, std::min(std::min(ip_per_sm, ipm_per_sm), per_sm));
             ctx->ip_grid = std::min(ip_per_sm * ctx->nsm, std::max(1, (ctx->ntile + ctx->upd_ip - 1) / ctx->upd_ip));
         }
         e = cudaDeviceSynchronize();
@@ -810,9 +815,9 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
     void *args[] = {&a};
     int slot;
     prof_begin(ctx, UC_K_UPDATE, slot);
-    if (ctx->rc_prec != UC_MIXED && ctx->upd_ip) {
+    if (ctx->upd_ip) {
         const void *fn; size_t sm;
-        ip_kernel(&fn, &sm);
+        ip_kernel(ctx->rc_prec == UC_MIXED, &fn, &sm);
         CK(cudaLaunchCooperativeKernel(fn, dim3(ctx->ip_grid), dim3(ctx->upd_ip * 32), args, sm, ctx->stream));
     } else {
         const void *kfn = ctx->rc_prec == UC_MIXED ? (const void *)update_kernel<float> : (const void *)update_kernel<double>;

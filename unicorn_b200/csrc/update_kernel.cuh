@@ -135,7 +135,6 @@ __global__ void __launch_bounds__(NW * 32, 1) update_kernel(const UpdArgs a)
     // the plane is addressed through the kernel parameter itself (not a local
     // pointer copy): ptxas then rebuilds addresses from the parameter bank and
     // the generated program fits in registers (a local copy spilled 5 KB/thread)
-    static_assert(!IP || sizeof(RCT) == 8, "the in-place form reads the FP64 plane");
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
     extern __shared__ __align__(128) double s_upd[];
@@ -186,11 +185,21 @@ __global__ void __launch_bounds__(NW * 32, 1) update_kernel(const UpdArgs a)
 #define UC_UPDATE_BLOCK_BEGIN(b) do { } while (0)
 #define YOS(m) __ldcg(a.y + (size_t)uc_ip_shadow[m] * np + cell)
                 if constexpr (IP) {
+                    if (sizeof(RCT) == 4 && a.tile_flag && a.tile_flag[tile]) {
 #define RC(r) ld_hint(a.rc + (size_t)(r) * np + cell, keep)
 #define RC_LAST(r) ld_hint(a.rc + (size_t)(r) * np + cell, drop)
-                    UC_UPDATE_PROGRAM_IP();
+                        UC_UPDATE_PROGRAM_IP();
 #undef RC
 #undef RC_LAST
+                    } else {
+#define UC_RCP (sizeof(RCT) == 4 ? reinterpret_cast<const RCT *>(a.rc32) : reinterpret_cast<const RCT *>(a.rc))
+#define RC(r) ld_hint(UC_RCP + (size_t)(r) * np + cell, keep)
+#define RC_LAST(r) ld_hint(UC_RCP + (size_t)(r) * np + cell, drop)
+                        UC_UPDATE_PROGRAM_IP();
+#undef RC
+#undef RC_LAST
+#undef UC_RCP
+                    }
                 } else if (sizeof(RCT) == 4 && a.tile_flag && a.tile_flag[tile]) {
                     // a tile the mixed rate kernel sent to FP64: its RC is in the FP64 plane
 #define RC(r) ld_hint(a.rc + (size_t)(r) * np + cell, keep)
