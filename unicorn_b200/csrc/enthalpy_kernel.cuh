@@ -5,6 +5,7 @@
 //   enth_source_kernel  heat release of the start-state rate coefficients and
 //                       the updated mass fractions: RA = RC * prod(Y), PRD,
 //                       PROD = sum PRD, QDSP, QDOT          (solveh.f:116-1145)
+//                       (two 16-warp CTAs per SM, RC read through L1)
 //   enth_coef_kernel    EKT, EMU and the species-enthalpy diffusion factors
 //                       RDHSP_k of every cell      (spgsolv.f:174, solveh.f:39-57)
 //   enth_rhs_kernel     interior cells: coefficients ZE, ZW, ZN, ZS (hybrid
@@ -53,14 +54,19 @@ struct EnthSrcArgs {
     int npad, ntile;
 };
 
-constexpr size_t ENTH_SRC_SMEM = (size_t)(LRX + 3 * LSP + 1) * TILE * sizeof(double);
+constexpr size_t ENTH_SRC_SMEM = (size_t)(3 * LSP + 1) * TILE * sizeof(double);
 
+// RC is read straight from the plane (through L1: a row of the tile is read by
+// the PRD lists of several species), so that shared memory holds only the
+// tile's Y and the species sums and two CTAs share an SM: the loads of one
+// overlap the arithmetic of the other. (Staging the tile's RC block [544][32]
+// in shared memory allowed one CTA per SM: 2.98 ms for the C2 field, 3.7 % of
+// DRAM bandwidth, stalled on the barriers between its load and species phases.)
 template <typename RCT>
-__global__ void __launch_bounds__(CHEM_THREADS, 1) enth_source_kernel(const EnthSrcArgs a)
+__global__ void __launch_bounds__(CHEM_THREADS, 2) enth_source_kernel(const EnthSrcArgs a)
 {
     extern __shared__ __align__(16) double esm[];
-    double *sRC = esm;                 // [544][32]
-    double *sY = sRC + LRX * TILE;     // [52][32]
+    double *sY = esm;                  // [52][32]
     double *sP = sY + LSP * TILE;      // [52][32] PRD
     double *sH = sP + LSP * TILE;      // [52][32] PRD * HENTH / HFO
     double *sT = sH + LSP * TILE;      // [32] TKD
@@ -70,12 +76,6 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) enth_source_kernel(const Enth
     for (int tile = blockIdx.x; tile < a.ntile; tile += gridDim.x) {
         const size_t cell = (size_t)tile * TILE + lane;
         const bool f64 = sizeof(RCT) == 8 || (a.tile_flag && a.tile_flag[tile]);
-        if (f64) {
-            for (int r = warp; r < LRX; r += CHEM_WARPS) sRC[r * TILE + lane] = __ldcs(a.rc + (size_t)r * np + cell);
-        } else {
-            for (int r = warp; r < LRX; r += CHEM_WARPS)
-                sRC[r * TILE + lane] = (double)__ldcs(a.rc32 + (size_t)r * np + cell);
-        }
         for (int k = warp; k < LSP; k += CHEM_WARPS) sY[k * TILE + lane] = a.y[(size_t)k * np + cell];
         if (warp == 0) sT[lane] = a.tk[cell] * P.TSTR;
         __syncthreads();
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) enth_source_kernel(const Enth
                         const int r = code & 0x1FFF;
                         double v = 0.0;
                         if (!(code & 0x2000)) {           // SRA terms are zero (solveh.f:671-676)
-                            v = sRC[r * TILE + lane];
+                            v = f64 ? __ldg(a.rc + (size_t)r * np + cell) : (double)__ldg(a.rc32 + (size_t)r * np + cell);
                             for (int q = 0; q < P.ra_len[r]; ++q) v = v * sY[P.ra_sp[r * 3 + q] * TILE + lane];
                             if (code & 0x4000) v = P.prd_coef[off + t] * v;
                         }

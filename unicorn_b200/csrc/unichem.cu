@@ -1240,9 +1240,9 @@ extern "C" int uc_enthalpy_update(uc_ctx *ctx, const uc_enthalpy_opts *o, int *p
         const void *fn = mixed ? (const void *)enth_source_kernel<float> : (const void *)enth_source_kernel<double>;
         CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ENTH_SRC_SMEM));
         if (mixed)
-            enth_source_kernel<float><<<std::min(ctx->ntile, ctx->nsm), CHEM_THREADS, ENTH_SRC_SMEM, ctx->stream>>>(a);
+            enth_source_kernel<float><<<std::min(ctx->ntile, 2 * ctx->nsm), CHEM_THREADS, ENTH_SRC_SMEM, ctx->stream>>>(a);
         else
-            enth_source_kernel<double><<<std::min(ctx->ntile, ctx->nsm), CHEM_THREADS, ENTH_SRC_SMEM, ctx->stream>>>(a);
+            enth_source_kernel<double><<<std::min(ctx->ntile, 2 * ctx->nsm), CHEM_THREADS, ENTH_SRC_SMEM, ctx->stream>>>(a);
         CK(cudaGetLastError());
     }
     // EKT and the species-enthalpy diffusion factors of every cell
