@@ -436,10 +436,12 @@ static int check_status(uc_ctx *ctx)
     return UC_OK;
 }
 
-// FP64 update with Y in place: 14 warps per CTA (one CTA per SM). Measured on
+// Species update with Y in place: 14 warps per CTA (one CTA per SM). Measured on
 // the C2 sweep against the two-Y-set kernel at 8 warps: 0.56 against 0.65 ms
 // per pass; 12, 16 and 17 warps gave 0.62, 0.57 and 0.66 (fewer registers per
-// thread as the warps grow: 168, 128, 96).
+// thread as the warps grow: 168, 128, 96). 14 warps stay at 128 registers: each
+// of the SM's four schedulers holds four of them in its 16K-register share, so
+// a 144-register build has no resident CTA and cannot be launched.
 constexpr int UPD_IP_WARPS = 14;
 static void ip_kernel(bool mixed, const void **fn, size_t *sm)
 {
