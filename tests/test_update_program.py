@@ -50,3 +50,20 @@ def test_generated_programs_match_oracle(oracle, harness, isor):
     y1 = np.ascontiguousarray(y.copy())
     p1 = harness.harness_update(*args(y1))
     assert p1 == po and np.array_equal(_closure(y1), yo)
+
+
+@pytest.mark.parametrize("isor", [1, 3])
+def test_inplace_program_equals_two_set_program(oracle, harness, isor):
+    """The in-place form of the program (one Y array, eight species read at their start-of-pass
+    value from the cell's Y row) gives bit for bit what the two-array form gives."""
+    tk, rho, y = random_state(oracle, 300, 22)
+    rc, sour = oracle.rates(tk, rho, y)
+    sour[:] = 0.0
+    P = lambda a: np.ascontiguousarray(a).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    args = lambda yy: (len(tk), P(rho), P(y), P(yy), P(rc), P(sour), P(oracle.wm), ctypes.c_double(1e-3), isor,
+                       ctypes.c_double(0.99), ctypes.c_double(1e-8), ctypes.c_double(len(tk) * 51.0))
+    y1, y2 = np.ascontiguousarray(y.copy()), np.ascontiguousarray(y.copy())
+    p1 = harness.harness_update(*args(y1))
+    p2 = harness.harness_update_ip(*args(y2))
+    assert p1 == p2 and np.array_equal(y1, y2)
+    assert np.abs(y1 - y).max() > 1e-8            # the update moved Y

@@ -40,3 +40,36 @@ extern "C" int harness_update(int n, const double *rho_a, const double *y0_a, do
     }
     return pass;
 }
+
+// The in-place form (UC_UPDATE_PROGRAM_IP): one Y array per cell, overwritten
+// species by species; the species read at their start-of-pass value after
+// their own update come from the cell's row in y_a, which still holds the
+// start-of-pass values while the program runs (as on the device).
+extern "C" int harness_update_ip(int n, const double *rho_a, const double *y0_a, double *y_a,
+                                 const double *rc_a, const double *sour_a, const double *wm,
+                                 double dt, int isor, double relx, double tol, double spnorm)
+{
+    const double sor1 = relx, sor2 = 1.0 - relx;
+    static const int shadow[UC_IP_NSHADOW] = UC_IP_SHADOW_LIST;
+    double y[LSP], y0[LSP], sour[6];
+    int pass;
+    for (pass = 1; pass <= isor; ++pass) {
+        double rsd = 0.0;
+        for (int c = 0; c < n; ++c) {
+            for (int k = 0; k < LSP; ++k) { y[k] = y_a[k * n + c]; y0[k] = y0_a[k * n + c]; }
+            for (int m = 0; m < 6; ++m) sour[m] = sour_a[m * n + c];
+            const double rho = rho_a[c];
+#undef YO
+#undef YN
+#undef UC_UPDATE_TAIL
+#define YO(k) y[k]
+#define YN(k) y[k]
+#define YOS(m) y_a[shadow[m] * n + c]
+#define UC_UPDATE_TAIL(k) do { if (fnew < 0.0) fnew = 0.0; y[k] = fnew; } while (0)
+            UC_UPDATE_PROGRAM_IP();
+            for (int k = 0; k < LSP - 1; ++k) y_a[k * n + c] = y[k];
+        }
+        if (rsd / spnorm <= tol) break;
+    }
+    return pass;
+}

@@ -258,13 +258,13 @@ def gen_inplace_program(blocks, uses: dict) -> str:
          "// is the start-of-pass value of species uc_ip_shadow[m], read after that",
          "// species' own update.",
          f"#define UC_IP_NSHADOW {len(ctx.shadow)}",
+         f"#define UC_IP_SHADOW_LIST {{{', '.join(map(str, ctx.shadow or [0]))}}}",
          "#define UC_UPDATE_PROGRAM_IP() do { \\",
          "    double prod = 0.0, extra, loss, rhs1, rhs2, ppp, fnew; \\"]
     L.extend("    " + x + " \\" for x in body)
     L.append("} while (0)")
     L.append("#ifdef __CUDACC__")
-    L.append(f"static __constant__ int8_t uc_ip_shadow[{max(1, len(ctx.shadow))}] = "
-             f"{{{', '.join(map(str, ctx.shadow or [0]))}}};")
+    L.append(f"static __constant__ int8_t uc_ip_shadow[{max(1, len(ctx.shadow))}] = UC_IP_SHADOW_LIST;")
     L.append("#endif")
     return "\n".join(L) + "\n"
 
