@@ -6,7 +6,9 @@ the oracle's restatement, itself pinned bit for bit to the reference's SOLVEH
   the same pass count (the device runs the reference's lexicographic
   Gauss-Seidel order and rounds every operation as written), converged or
   not, with the ring of pass buffers full and capped at 2 and 3 slots, on the
-  C1 grid and on the reference's 131 x 711 grid.
+  C1 grid, on the reference's 131 x 711 grid, and on edge grids (one interior
+  row, one interior column, one interior cell, 1024 interior rows); more
+  rows than one pass takes are refused.
 * The whole update after a sweep, against the oracle given the device's rate
   plane, properties and cp of the start state (their own parity is covered by
   tests/test_gpu_parity.py): ZE..ZS to 1e-12 of the cell's largest
@@ -186,3 +188,23 @@ def test_density_matches_oracle(cuda, oracle):
         _, rho_g, _, _, _ = u.download()
     rho_o = oracle.density(LJ, LI, g["tk"], g["y_new"])
     assert np.array_equal(rho_g, rho_o)
+
+
+@pytest.mark.parametrize("lj,li", [(3, 9), (9, 3), (3, 3), (1026, 5)])
+def test_relax_edge_grids(cuda, oracle, lj, li):
+    """One interior row, one interior column, a single interior cell, and the most rows one pass
+    takes (1024 interior rows, one thread each): bit for bit with the oracle."""
+    g, o = oracle_coefficients(oracle, lj, li, 13)
+    fpz_o, passes_o = oracle.enthalpy_relax(lj, li, g["rho"], o["rhsz"], o["z"], g["ht"], isor=30, tol=1e-10)
+    fpz_g, passes_g = cuda.enthalpy_relax(lj, li, g["rho"], o["rhsz"], o["z"], g["ht"], isor=30, tol=1e-10)
+    assert passes_g == passes_o
+    assert np.array_equal(fpz_g, fpz_o)
+
+
+def test_relax_rejects_too_many_rows(cuda, oracle):
+    """1025 interior rows exceed one thread per row: a clear error, no launch."""
+    lj, li = 1027, 4
+    n = lj * li
+    z = tuple(np.zeros(n) for _ in range(4))
+    with pytest.raises(RuntimeError):
+        cuda.enthalpy_relax(lj, li, np.ones(n), np.zeros(n), z, np.zeros(n), isor=3)
