@@ -16,7 +16,9 @@ the oracle's restatement, itself pinned bit for bit to the reference's SOLVEH
   diffusion sums, the radiation, DT times the gross heat release); QDSP and
   QDOT to 1e-10 of their gross sizes; FPZ bit for bit against the oracle's
   relaxation of the device's coefficients; T to 2e-3 K (the Newton step
-  tolerance of solveh.f:1211 is 1e-3 K)."""
+  tolerance of solveh.f:1211 is 1e-3 K). The same after a mixed-precision
+  sweep, whose FP32 rate plane (with FP64 tiles for the cold cells) the
+  heat release reads."""
 import numpy as np
 import pytest
 
@@ -208,3 +210,47 @@ def test_relax_rejects_too_many_rows(cuda, oracle):
     z = tuple(np.zeros(n) for _ in range(4))
     with pytest.raises(RuntimeError):
         cuda.enthalpy_relax(lj, li, np.ones(n), np.zeros(n), z, np.zeros(n), isor=3)
+
+
+def test_enthalpy_update_after_mixed_sweep(cuda, oracle):
+    """The heat release read from the mixed form's rate plane (FP32, with the tiles sent to FP64 read
+    from the FP64 plane): against the oracle given that same plane and the sweep's own properties."""
+    from test_gpu_parity import gross
+    g = enthalpy_case(oracle, LJ, LI, 14)
+    n = LJ * LI
+    g["tk"][:10 * LJ] = 300.0 / oracle.scales["TSTR"]      # cold columns: their rates leave the FP32 range
+    ht = consistent_ht(oracle, g)
+    dt = 1e-7
+    inner = interior(LJ, LI)
+    with cuda.UniChem(n) as u:
+        u.upload(g["tk"], g["rho"], g["y"], stmf=g["stmf"])
+        u.set_grid(LJ, LI, g["xxs"], g["xxc"], g["yys"], g["yyc"], g["yr"], isym=1)
+        u.set_flow(g["u"], g["v"], g["tmu"], 0.9)
+        u.set_enthalpy(ht)
+        u.sweep(dt, precision=cuda.MIXED, isor=4, tol=0.0)
+        _, _, y_new, _, _ = u.download()
+        start = u.download_outputs()                        # properties and cp of the start state
+        u.enthalpy_update(dt, isor=100, relx=0.99, tol=1e-8, sigh=0.9)
+        ht_g, rhsz_g, ze_g, zw_g, zn_g, zs_g = u.enthalpy_get()
+        out = u.download_outputs()
+    with cuda.UniChem(n) as u2:
+        u2.upload(g["tk"], g["rho"], g["y"], stmf=g["stmf"])
+        u2.props()
+        rc = u2.ckrates(precision=cuda.MIXED, return_rc=True)
+        assert u2.stat("mixed_fp64_tiles") > 0
+    z_o, ekt = oracle.zfaces(LJ, LI, g["rho"], start["cp"], start["vtc"], g["tmu"], g["u"], g["v"], g["yr"], g["xxs"],
+                             g["xxc"], g["yys"], g["yyc"], isym=1, dt=dt, sigh=0.9)
+    zmax = np.max(np.abs(np.stack(z_o)), axis=0)
+    for a, b in zip((ze_g, zw_g, zn_g, zs_g), z_o):
+        assert np.all(np.abs(a - b)[inner] <= 1e-12 * zmax[inner] + 1e-300)
+    rhsz_o, qdsp_o, qdot_o = oracle.enthalpy_rhs(LJ, LI, g["tk"], g["rho"], y_new, ht, g["stmf"], start["vdf"],
+                                                 g["tmu"], ekt, rc, g["yr"], g["xxs"], g["xxc"], g["yys"], g["yyc"],
+                                                 isym=1, dt=dt, sigsp=0.9)
+    gq = gross(oracle, g["tk"], g["rho"], y_new)
+    sc = oracle.scales
+    rconv = sc["VSTR"] / sc["WMSTR"] / sc["ALSTR"] * 1e-6
+    scale = np.abs(g["rho"] * ht) + np.abs(rhsz_o) + dt * (gq * np.abs(oracle.hfo)[:, None]).sum(0) / rconv + 1e-300
+    assert (np.abs(rhsz_g - rhsz_o)[inner] / scale[inner]).max() <= 1e-10
+    assert np.all(np.abs(out["qdsp"] - qdsp_o)[:, inner] <= 1e-10 * gq[:, inner] + 1e-300)
+    fpz_o, _ = oracle.enthalpy_relax(LJ, LI, g["rho"], rhsz_g, (ze_g, zw_g, zn_g, zs_g), ht, isor=100, tol=1e-8)
+    assert np.array_equal(ht_g[inner], fpz_o[inner])
