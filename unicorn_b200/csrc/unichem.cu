@@ -439,10 +439,14 @@ static int check_status(uc_ctx *ctx)
 // Species update with Y in place: 14 warps per CTA (one CTA per SM). Measured on
 // the C2 sweep against the two-Y-set kernel at 8 warps: 0.56 against 0.65 ms
 // per pass; 12, 16 and 17 warps gave 0.62, 0.57 and 0.66 (fewer registers per
-// thread as the warps grow: 168, 128, 96). 14 warps stay at 128 registers: each
+// thread as the warps grow: 168, 128, 96); over 5 sweeps 13, 14 and 15 warps
+// took 257.3, 257.2 and 250.8 ms of update time. 14 warps stay at 128 registers: each
 // of the SM's four schedulers holds four of them in its 16K-register share, so
 // a 144-register build has no resident CTA and cannot be launched.
-constexpr int UPD_IP_WARPS = 14;
+#ifndef UC_UPD_IP_WARPS
+#define UC_UPD_IP_WARPS 14
+#endif
+constexpr int UPD_IP_WARPS = UC_UPD_IP_WARPS;
 static void ip_kernel(bool mixed, const void **fn, size_t *sm)
 {
     *fn = mixed ? (const void *)update_kernel<float, UPD_IP_WARPS, true>
