@@ -220,7 +220,7 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def roofline(res, n, steps):
+def roofline(res, n, steps, mixed=False):
     """Dominant kernel of the step and its achieved rate against the measured HBM copy bandwidth."""
     kt = res["kernel_ms"]
     name = max(kt, key=lambda k: kt[k][0])
@@ -228,9 +228,13 @@ def roofline(res, n, steps):
     hbm, src = peaks()
     npad = (n + 31) // 32 * 32
     passes = sum(res["passes"][-steps:]) / max(1, steps)
-    # algorithmic bytes per launch (per-cell figures x cells)
+    # algorithmic bytes per launch: per-cell figures x cells
     traffic = None
-    if name == "update":
+    if name == "update" and mixed:
+        per_cell = passes * (544 * 4 + (52 + 52 + 6 + 2 + 2) * 8) + (52 + 2) * 8
+        unit_note = (f"per cell and launch: {passes:.1f} passes x (RC 544 x 4 B of the FP32 plane + (Y 52 in + 52 out "
+                     "+ SOUR 6 + soot 4) x 8 B)")
+    elif name == "update":
         per_cell = passes * (544 + 52 + 52 + 6 + 2 + 2) * 8 + (52 + 2) * 8
         unit_note = f"per cell and launch: {passes:.1f} passes x (RC 544 + Y 52 in + 52 out + SOUR 6 + soot 4) x 8 B"
         # DRAM read + write of one launch of the FP64 update (Y in place, 14 warps per SM) under ncu
@@ -272,7 +276,7 @@ def main_ours(args):
                 "config": workload_config(world, {"update_passes_per_step": res["passes"][-args.steps:],
                                                   "precision": args.precision}),
                 "e2e": res["e2e"], "gpu_launches": res["gpu_launches"] * world, "clocks": res["clocks"],
-                "roofline": roofline(res, res["n"], args.steps),
+                "roofline": roofline(res, res["n"], args.steps, args.precision == "mixed"),
                 "kernel_ms": {k: round(v[0], 3) for k, v in res["kernel_ms"].items()}}
         if cpu is not None:
             line["cpu_baseline"] = cpu
