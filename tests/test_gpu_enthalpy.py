@@ -7,8 +7,9 @@ the oracle's restatement, itself pinned bit for bit to the reference's SOLVEH
   Gauss-Seidel order and rounds every operation as written), converged or
   not, with the ring of pass buffers full and capped at 2 and 3 slots, on the
   C1 grid, on the reference's 131 x 711 grid, and on edge grids (one interior
-  row, one interior column, one interior cell, 1024 interior rows); more
-  rows than one pass takes are refused.
+  row, one interior column, one interior cell, 1024 interior rows) and the
+  whole C2 grid (301 x 601), where the converged FPZ also satisfies the
+  discrete enthalpy equation; more rows than one pass takes are refused.
 * The whole update after a sweep, against the oracle given the device's rate
   plane, properties and cp of the start state (their own parity is covered by
   tests/test_gpu_parity.py): ZE..ZS to 1e-12 of the cell's largest
@@ -254,3 +255,23 @@ def test_enthalpy_update_after_mixed_sweep(cuda, oracle):
     assert np.all(np.abs(out["qdsp"] - qdsp_o)[:, inner] <= 1e-10 * gq[:, inner] + 1e-300)
     fpz_o, _ = oracle.enthalpy_relax(LJ, LI, g["rho"], rhsz_g, (ze_g, zw_g, zn_g, zs_g), ht, isor=100, tol=1e-8)
     assert np.array_equal(ht_g[inner], fpz_o[inner])
+
+
+def test_relax_full_c2_grid(cuda, oracle):
+    """The C2 grid (301 rows x 601 columns, 180,901 cells): bit for bit with the oracle, and the
+    converged FPZ satisfies the discrete enthalpy equation PPP F = RHSZ - (ZE F_E + ZW F_W + ZN F_N
+    + ZS F_S) on the interior to the relaxation's tolerance."""
+    lj, li = 301, 601
+    g, o = oracle_coefficients(oracle, lj, li, 15)
+    fpz_o, passes_o = oracle.enthalpy_relax(lj, li, g["rho"], o["rhsz"], o["z"], g["ht"], isor=100, tol=1e-10)
+    fpz_g, passes_g = cuda.enthalpy_relax(lj, li, g["rho"], o["rhsz"], o["z"], g["ht"], isor=100, tol=1e-10)
+    assert passes_g == passes_o and passes_g <= 100
+    assert np.array_equal(fpz_g, fpz_o)
+    F = fpz_g.reshape(li, lj)
+    ze, zw, zn, zs = (z.reshape(li, lj) for z in o["z"])
+    rho, rhsz = g["rho"].reshape(li, lj), o["rhsz"].reshape(li, lj)
+    c = (slice(1, -1), slice(1, -1))
+    ppp = rho[c] - (ze[c] + zw[c] + zn[c] + zs[c])
+    nb = ze[c] * F[2:, 1:-1] + zw[c] * F[:-2, 1:-1] + zn[c] * F[1:-1, 2:] + zs[c] * F[1:-1, :-2]
+    res = np.abs(ppp * F[c] - (rhsz[c] - nb)) / (np.abs(rhsz[c]) + np.abs(ppp * F[c]) + 1e-300)
+    assert np.median(res) < 1e-9 and res.max() < 1e-6, (np.median(res), res.max())
