@@ -1,7 +1,7 @@
 /*
  * unichem: B200 (sm_100a) implementation of UNICORN's per-cell chemistry and
  * property hot path, behind a C ABI that a Fortran host binds with
- * ISO_C_BINDING (see INTEGRATION.md for the interface module).
+ * ISO_C_BINDING.
  *
  * Data layout: the host's COMMON arrays as they are. A field of n cells is
  * passed as Fortran arrays over the (J,I) grid flattened column-major, i.e.
@@ -391,8 +391,18 @@ void uc_mlp_destroy(uc_mlp *mlp);
  *    contents; nothing in it has to start at zero (every partial sum is written
  *    before it is read). Calls that overlap on the GPU, from any context or
  *    stream, race on it: serialise them.
+ *  - The update runs on the context's stream (uc_device_view_get().stream),
+ *    which is created non-blocking: writes to the input arrays made on other
+ *    streams must be complete, or ordered before the call (an event the
+ *    caller records and makes that stream wait on), when the call is made.
  *  - passes (host pointer, may be NULL) receives the pass count; giving it
- *    makes the call wait for the update to finish.
+ *    makes the call wait for the update to finish. With passes == NULL the
+ *    call returns once the update is queued: synchronise (uc_sync, or a wait
+ *    on the context's stream) before reading y or soot.
+ *  - It runs the two-Y-set form of the update kernel (8 warps per block, the
+ *    kernel UNICHEM_UPDATE=twoset selects for uc_species_update), whose only
+ *    scratch is the per-block partial sums; its results are bit for bit those
+ *    of uc_species_update.
  */
 #define UC_NOALLOC_MAX_BLOCKS 1024
 typedef struct {

@@ -32,7 +32,8 @@ The grid size is a compile-time PARAMETER in the reference (LI=711, LJ=131,
 LI=66: a 32x64 = 2048-cell interior) and the driver in ``oracle/ref.py``
 processes larger fields in chunks of that size.
 
-Usage: python oracle/build_ref.py [--ref /root/reference] [--lj 34 --li 66]
+Usage: python oracle/build_ref.py [--ref <reference checkout>] [--lj 34 --li 66]
+(default: $UNICORN_REF, else ``reference`` beside this repository)
 """
 from __future__ import annotations
 
@@ -111,7 +112,8 @@ def build(ref: str, lj: int, li: int, out: Path = OUT) -> Path:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("UNICORN_REF", "/root/reference"))
+    from unicorn_b200.refsrc import reference_root
+    ap.add_argument("--ref", default=str(reference_root()))
     ap.add_argument("--lj", type=int, default=34)
     ap.add_argument("--li", type=int, default=66)
     a = ap.parse_args()

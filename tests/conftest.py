@@ -24,7 +24,8 @@ def ref():
     """The reference's own routines, translated to C (oracle/_ref)."""
     from oracle import ref as R
     if not R.available():
-        src = os.environ.get("UNICORN_REF", "/root/reference")
+        from unicorn_b200.refsrc import reference_root
+        src = str(reference_root())
         if Path(src).exists():
             from oracle.build_ref import build
             build(src, 34, 66)

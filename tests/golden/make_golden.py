@@ -30,6 +30,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT))
+from unicorn_b200.refsrc import reference_root  # noqa: E402
 
 
 def states(scales, wm, n, seed, tlo, thi):
@@ -48,7 +49,7 @@ def states(scales, wm, n, seed, tlo, thi):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-src", default="/root/reference")
+    ap.add_argument("--ref-src", default=str(reference_root()))
     args = ap.parse_args()
     from oracle import ref as R
     if not R.available():

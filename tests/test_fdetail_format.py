@@ -1,6 +1,5 @@
 """The FDETAIL writer (unicorn_b200/fdetail.py): the Fortran edit descriptors
 of stdata.f:120-175 and the variable line of its FORMAT 105."""
-import os
 import re
 from pathlib import Path
 
@@ -8,8 +7,9 @@ import numpy as np
 import pytest
 
 from unicorn_b200.fdetail import e15_7e3, read_fdetail, variables_line, write_fdetail
+from unicorn_b200.refsrc import reference_root
 
-REF = Path(os.environ.get("UNICORN_REF", "/root/reference"))
+REF = reference_root()
 
 
 @pytest.mark.parametrize("v,s", [(0.0, " 0.0000000E+000"), (1.0, " 0.1000000E+001"), (-123.4567, "-0.1234567E+003"),

@@ -24,7 +24,8 @@ def sample(lj, li, seed=0):
     return f
 
 
-@pytest.mark.parametrize("iflow,bodies", [(1, None), (2, [[3, 4, 6, 8]])])
+@pytest.mark.parametrize("iflow,bodies", [(1, None), (2, [[3, 4, 6, 8]]),
+                                          (1, [[b + 1, b + 2, b + 3, b + 4] for b in range(7)])])
 def test_round_trip(tmp_path, iflow, bodies):
     lj, li = 7, 5
     f = sample(lj, li)

@@ -67,6 +67,9 @@ def test_noalloc_update_matches_regular_entry_point():
         d_soot = d_soot0.clone()
         arr = UpdateArrays(n, npad, d_rc.data_ptr(), d_sour.data_ptr(), d_rho.data_ptr(), d_y0.data_ptr(),
                            d_soot0.data_ptr(), None, None, d_y.data_ptr(), d_soot.data_ptr())
+        # the arrays were filled on torch's stream; the call runs on the context's own
+        # stream, which is not ordered after it
+        torch.cuda.synchronize()
         passes = ctypes.c_int(-1)
         rc = lib.uc_species_update_noalloc(u._h, ctypes.byref(arr), 1e-3, isor, 0.99, tol, 0.0,
                                            ctypes.byref(passes))

@@ -22,7 +22,8 @@ Every product is a left-to-right chain of factors and every sum a
 left-to-right list of signed terms, in the reference's statement order, so
 that evaluators can reproduce the reference's rounding.
 
-Usage: python -m unicorn_b200.mech.extract [--ref /root/reference]
+Usage: python -m unicorn_b200.mech.extract [--ref <reference checkout>]
+(default: $UNICORN_REF, else ``reference`` beside this repository)
 """
 from __future__ import annotations
 
@@ -36,6 +37,7 @@ from pathlib import Path
 import numpy as np
 
 from unicorn_b200.fortran.parser import Bin, Name, Num, Ref, Un, build_units
+from unicorn_b200.refsrc import reference_root
 
 LSP, LRX = 52, 544
 HERE = Path(__file__).resolve().parent
@@ -412,7 +414,7 @@ def extract(ref: Path) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("UNICORN_REF", "/root/reference"))
+    ap.add_argument("--ref", default=str(reference_root()))
     ap.add_argument("--out", default=str(OUT))
     a = ap.parse_args()
     mech = extract(Path(a.ref))

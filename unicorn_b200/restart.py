@@ -50,7 +50,9 @@ def write_restart(path, f: dict, scales: dict, lj: int, li: int, infuel: int = 1
              "".join(f"{v:6d}" for v in (li, lj, isym, iflow, iswrl, ithrm, ichem, igrav, 0, itr)) + f"{dt:12.10f}"]
     lines += _records([scales[k] for k in SCALES])
     if bodies:
-        lines.append("".join(f"{v:6d}" for v in [len(bodies)] + [c for b in bodies for c in b]))
+        ints = [len(bodies)] + [c for b in bodies for c in b]
+        # FORMAT(21I6): 21 integers per record, the list continues on further records
+        lines += ["".join(f"{v:6d}" for v in ints[i:i + 21]) for i in range(0, len(ints), 21)]
     body = [f["X"], f["Y"], f["RHO"]] + [f["FSP"][k] for k in range(51)] + [f["U"], f["V"], f["W"], f["P"],
                                                                            f["QDOT"], f["TK"]]
     lines += _records(np.concatenate([np.asarray(a, dtype=np.float64).reshape(n) for a in body]))
@@ -99,9 +101,14 @@ def read_restart(path) -> tuple[dict, dict]:
     h["scales"] = dict(zip(SCALES, sc))
     if iflame >= 100000:
         iflame -= 100000
+        # NBODY and the corners of each body under FORMAT(21I6): 21 per record
         nn = int(lines[pos][:6])
-        h["bodies"] = [[int(lines[pos][6 + 6 * (4 * b + q):12 + 6 * (4 * b + q)]) for q in range(4)] for b in range(nn)]
-        pos += 1
+        ints = []
+        while len(ints) < 1 + 4 * nn:
+            l = lines[pos]
+            pos += 1
+            ints += [int(l[6 * i:6 * i + 6]) for i in range(min(21, len(l) // 6))]
+        h["bodies"] = [ints[1 + 4 * b:5 + 4 * b] for b in range(nn)]
     lsp = iflame // 100
     h["INFUEL"] = iflame % 100
     n = h["LI"] * h["LJ"]
