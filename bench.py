@@ -1,18 +1,26 @@
-"""Benchmark: chem+property cell-updates/s of UNICORN's species sweep on B200.
+"""Benchmark: chem+property cell-updates/s of UNICORN's species sweep on B200,
+FP64 against the mixed-precision form and the learned surrogate with fallback.
 
-One step = one species sweep over the 601x301 (180,901-cell) heptane field
-(fuel=11, T peak 2300 K, seed 0): Y clip + mixture-averaged transport, cp and
-h, the 544 rate coefficients, omega_k and d(omega_k)/dY_k, then the
-point-implicit update of SOLVESP with the reference's input-card settings
-(up to 100 passes, relaxation 0.99, tolerance 1e-8) at dt = 1e-5 s.
-A cell-update = one cell through one such sweep.
+Headline workload (default): the 1M-cell heptane field -- 1,048,576 cells of
+the heptane generator (fuel=11) with T ~ U[300, 2400] K and p ~ U[0.8, 1.2]
+atm, seed 7. One step = one species sweep of the field from its seeded state:
+Y clip + mixture-averaged transport, cp and h, the 544 rate coefficients,
+omega_k and d(omega_k)/dY_k, then the point-implicit update of SOLVESP with
+the reference's input-card settings (up to 100 passes, relaxation 0.99,
+tolerance 1e-8) at dt = 1e-5 s. A cell-update = one cell through one such
+sweep. Every step starts from the same seeded state (a device-to-device copy
+inside the step), so every step does the same work, and the reference arm
+runs the same sweep on chunks of the same field.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-``value`` is device-resident throughput (fields already on the GPU);
+``value`` is device-resident FP64 throughput (fields already on the GPU);
 ``e2e`` is the same sweep through the C ABI with the step's inputs copied
 from pinned host memory and its outputs copied back, inside the timed
-region. ``--impl reference`` times the reference's own routines (translated
+region. ``forms`` compares, on the same field, the FP64 form with the mixed
+form and with the learned surrogate plus per-cell fallback, with the error
+of each against FP64; ``c2`` is the FP64 sweep of the 601x301 heptane jet
+field. ``--impl reference`` times the reference's own routines (translated
 to C, oracle/_ref) on the host cores.
 """
 from __future__ import annotations
@@ -36,13 +44,23 @@ UNIT = "cell-updates/s"
 DT = 1e-3            # non-dimensional: 1e-5 s / TMSTR (0.01 s)
 ISOR, RELX, TOL = 100, 0.99, 1e-8     # docs/input.uni:25-27
 NZ, NR, FUEL, TPEAK = 601, 301, 11, 2300.0
+HEAD_CELLS, HEAD_SEED = 1 << 20, 7
+TRAIN_STATES, TRAIN_STEPS = 4 << 20, 6000
+MLP_TOLS = (1e-3, 1e-2, 1e-1)
 
 
-def workload_config(n_gpus, extra=None):
-    c = {"workload": "C2: 601x301 heptane jet field (fuel=11, T_peak 2300 K, seed 0), one species sweep per step "
-                     "(props, cp/h, rates, omega, domega/dY, point-implicit update isor=100 relx=0.99 tol=1e-8, dt=1e-5 s)",
-         "cells": NZ * NR, "precision": "fp64", "l2": "working set > L2 (RC plane 787 MB written and read every step)",
-         "parallelism": f"cell-sharded x{n_gpus} (independent fields per rank)"}
+def head_field(n=HEAD_CELLS, seed=HEAD_SEED):
+    from unicorn_b200.fields import batch_cells
+    return batch_cells(n, seed=seed)
+
+
+def head_config(n, n_gpus, extra=None):
+    c = {"workload": f"{n}-cell heptane field (fuel=11, T~U[300,2400] K, p~U[0.8,1.2] atm, seed {HEAD_SEED}), one "
+                     "species sweep per step from the seeded state (props, cp/h, rates, omega, domega/dY, "
+                     "point-implicit update isor=100 relx=0.99 tol=1e-8, dt=1e-5 s)",
+         "cells": n, "precision": "fp64",
+         "l2": "inputs larger than L2 (state 453 MB, RC plane 4.6 GB at 1M cells)",
+         "parallelism": f"cell-sharded x{n_gpus} (an independent field per rank)"}
     if extra:
         c.update(extra)
     return c
@@ -90,105 +108,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-# ---------------------------------------------------------------- our arm
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        pass
+
+
+# ---------------------------------------------------------------- helpers
 def peaks():
+    """Measured HBM copy bandwidth and bf16 tensor throughput of this pool's B200s."""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
-
-
-def cpu_baseline_port(f, scales_src):
-    """The oracle (a faithful FP64 C restatement) on one host core, bounded sample."""
-    from oracle.oracle import Oracle
-    from unicorn_b200.fields import nondimensional
-    o = Oracle()
-    ns = 1024
-    tk, rho = nondimensional(f, o.scales, o.wm)
-    tk, rho, y = tk[:ns].copy(), rho[:ns].copy(), np.ascontiguousarray(f.y[:, :ns])
-    t0 = time.perf_counter()
-    yc, mu, lam, dk, _ = o.props(tk, y)
-    cp = o.cp(tk, yc)
-    h = o.enthalpy(tk, yc)
-    q = o.omega(tk, rho, yc)
-    rc, sour = o.rates(tk, rho, yc)
-    yn, s, passes = o.species_update(rho, yc, rc, sour, DT, isor=ISOR, relx=RELX, tol=TOL)
-    dt = time.perf_counter() - t0
-    return {"value": ns / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"first {ns} cells of the C2 field, one full sweep (oracle/unichem_oracle.c, -O2, 1 thread; "
-                      f"{passes} update passes), {dt:.2f} s"}
-
-
-def run_ours(args, rank, world, dev):
-    import torch
-    from unicorn_b200 import unichem
-    from unicorn_b200.fields import jet_field, nondimensional
-    f = jet_field(NZ, NR, fuel=FUEL, t_peak=TPEAK, seed=rank)
-    if args.cells:
-        f.T, f.p, f.y = f.T[:args.cells].copy(), f.p[:args.cells].copy(), np.ascontiguousarray(f.y[:, :args.cells])
-    n = f.n
-    u = unichem.UniChem(n, device=dev)
-    tk, rho = nondimensional(f, u.scales, u.wm)
-    view = unichem_view(u)
-    ext = torch.cuda.ExternalStream(view["stream"], device=dev)
-    # pinned host buffers for the end-to-end path
-    pin = lambda *s: torch.empty(s, dtype=torch.float64, pin_memory=True).numpy()
-    h_tk, h_rho, h_y = pin(n), pin(n), pin(52, n)
-    h_tk[:], h_rho[:], h_y[:] = tk, rho, f.y
-    outs = dict(qdsp=pin(52, n), qdot=pin(n), domega_dy=pin(52, n), vmu=pin(n), vtc=pin(n), vdf=pin(52, n),
-                cp=pin(n), h=pin(n))
-    h_yout = pin(52, n)
-
-    def reset():
-        u.upload(h_tk, h_rho, h_y)
-
-    prec = unichem.MIXED if args.precision == "mixed" else unichem.FP64
-
-    def step_device():
-        return u.sweep(DT, precision=prec, isor=args.isor, relx=RELX, tol=TOL)
-
-    passes_seen = []
-    reset()
-    for _ in range(args.warmup):
-        passes_seen.append(step_device())
-    # ---------------- device-resident timing
-    reset()
-    torch.cuda.synchronize(dev)
-    barrier(world)
-    u.profile(True)
-    with torch.cuda.stream(ext):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with ClockSampler(dev if world == 1 else dev) as clk:
-            e0.record(ext)
-            for _ in range(args.steps):
-                passes_seen.append(step_device())
-            e1.record(ext)
-            torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1)
-    kt = u.profile_read()
-    u.profile(False)
-    ms = max_over_ranks(ms, world)
-    # ---------------- end-to-end through the C ABI (host buffers)
-    torch.cuda.synchronize(dev)
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        u.upload(h_tk, h_rho, h_y)
-        u.sweep(DT, precision=prec, isor=args.isor, relx=RELX, tol=TOL)
-        u.download_outputs(outs)
-        u.lib.uc_download_fields(u._h, None, None, unichem._p(h_yout), None, None)
-    u.sync()
-    e2e_s = max_over_ranks((time.perf_counter() - t0) * 1e3, world) / 1e3
-    h2d = (2 + 52) * 8 * n
-    d2h = (52 * 4 + 5) * 8 * n
-    res = {"ms_per_step": ms / args.steps, "value": world * n * args.steps / (ms / 1e3),
-           "e2e": {"value": world * n * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                   "d2h_bytes_per_step": d2h},
-           "kernel_ms": kt, "passes": passes_seen, "clocks": clk.summary(), "n": n,
-           "gpu_launches": sum(c for _, c in kt.values())}
-    u.close()
-    return res, f
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "bf16_tflops_sustained": float(d.get("bf16_tflops_sustained", d["bf16_tflops"])),
+                "source": "measured (MEASURED_PEAKS.json)"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+            "source": "fallback (no MEASURED_PEAKS.json)"}
 
 
 def unichem_view(u):
@@ -220,77 +158,119 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def roofline(res, n, steps, mixed=False, isor=ISOR):
-    """Dominant kernel of the step and its achieved rate against the measured HBM copy bandwidth."""
-    kt = res["kernel_ms"]
+def omega_rel_error(q, exact, y):
+    """Relative error of QDSP per (cell, species) on species above 1e-8 mass fraction, with a floor of
+    1e-6 x the cell's largest |omega| (a stated near-zero net); the flat array of those pairs."""
+    wmax = np.abs(exact).max(axis=0)
+    r = np.abs(q - exact) / np.maximum(np.abs(exact), 1e-6 * wmax + 1e-300)
+    return r[y > 1e-8]
+
+
+def err_summary(r, tol=1e-3):
+    return {"p50": float(np.median(r)), "p99": float(np.quantile(r, 0.99)), "max": float(r.max()),
+            "frac_le_1e-3": round(float((r <= tol).mean()), 6)}
+
+
+class DeviceState:
+    """The seeded state of a field kept on the device; restore() loads it into a context (asynchronous,
+    on the context's stream)."""
+
+    def __init__(self, u, tk, rho, y, dev):
+        import torch
+        self.t = {"tk": torch.from_numpy(np.ascontiguousarray(tk)).to(dev),
+                  "rho": torch.from_numpy(np.ascontiguousarray(rho)).to(dev),
+                  "y": torch.from_numpy(np.ascontiguousarray(y)).to(dev)}
+        torch.cuda.synchronize(dev)
+        self.u = u
+
+    def restore(self):
+        t = self.t
+        self.u.upload_device(t["tk"].data_ptr(), t["rho"].data_ptr(), t["y"].data_ptr(), None, None, self.u.n)
+
+
+def time_sweeps(u, st, ext, prec, steps, warmup, isor=ISOR, clocks=None):
+    """K sweeps, each from the seeded state, bracketed by CUDA events on the context's stream."""
+    import torch
+    for _ in range(warmup):
+        st.restore()
+        u.sweep(DT, precision=prec, isor=isor, relx=RELX, tol=TOL)
+    u.sync()
+    u.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    passes = []
+    with (clocks if clocks is not None else _Null()):
+        e0.record(ext)
+        for _ in range(steps):
+            st.restore()
+            passes.append(u.sweep(DT, precision=prec, isor=isor, relx=RELX, tol=TOL))
+        e1.record(ext)
+        e1.synchronize()
+    kt = u.profile_read()
+    u.profile(False)
+    return e0.elapsed_time(e1), passes, kt
+
+
+def time_calls(fn, ext, reps, warmup):
+    """Mean device time (ms) of fn() over reps calls after warmup calls."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(reps):
+        fn()
+    e1.record(ext)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def roofline(kt, n, passes_run, pk):
+    """Dominant kernel of the FP64 sweep and its achieved rate against the measured HBM copy bandwidth."""
     name = max(kt, key=lambda k: kt[k][0])
     ms, cnt = kt[name]
-    hbm, src = peaks()
-    npad = (n + 31) // 32 * 32
-    # passes run per step (the reported count is isor + 1 when the tolerance was not met)
-    passes = sum(min(p, isor) for p in res["passes"][-steps:]) / max(1, steps)
-    # algorithmic bytes per launch: per-cell figures x cells
     traffic = None
-    if name == "update" and mixed:
-        per_cell = passes * (544 * 4 + (52 + 52 + 6 + 2 + 2) * 8) + (52 + 2) * 8
-        unit_note = (f"per cell and launch: {passes:.1f} passes x (RC 544 x 4 B of the FP32 plane + (Y 52 in + 52 out "
-                     "+ SOUR 6 + soot 4) x 8 B)")
-    elif name == "update":
-        per_cell = passes * (544 + 52 + 52 + 6 + 2 + 2) * 8 + (52 + 2) * 8
-        unit_note = f"per cell and launch: {passes:.1f} passes x (RC 544 + Y 52 in + 52 out + SOUR 6 + soot 4) x 8 B"
-        # DRAM read + write of one launch of the FP64 update (Y in place, 14 warps per SM) under ncu
-        # (65,536 C2 cells, 5 passes: 3.723 GB + 0.193 GB), per cell and pass, scaled to this launch
-        # by cells x passes run
-        traffic = round(11951.0 * n * passes)
+    if name == "update":
+        per_cell = passes_run * (544 + 52 + 52 + 6 + 2 + 2) * 8 + (52 + 2) * 8
+        rule = (f"per cell and launch: {passes_run:.1f} passes x (RC 544 + Y 52 in + 52 out + SOUR 6 + soot 4) x 8 B "
+                "+ the closure's 54 x 8 B")
+        # DRAM read + write of one launch of the FP64 update under ncu (65,536 C2 cells, 5 passes:
+        # 3.723 GB + 0.193 GB), per cell and pass, scaled to this launch by cells x passes run
+        traffic = round(11951.0 * n * passes_run)
     elif name == "chem":
         per_cell = (52 + 4) * 8 + (544 + 52 + 52 + 1 + 6) * 8
-        unit_note = "per cell: read T, rho, soot, Y (56 x 8 B); write RC 544, QDSP 52, dw/dY 52, QDOT, SOUR 6"
+        rule = "per cell: read T, rho, soot, Y (56 x 8 B); write RC 544, QDSP 52, dw/dY 52, QDOT, SOUR 6"
     else:
         per_cell = (54 + 54) * 8
-        unit_note = "per cell: 54 inputs + 54 outputs x 8 B"
-    bytes_per_launch = per_cell * n
-    achieved = bytes_per_launch / (ms / cnt / 1e3) / 1e9
-    return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "peak_source": src,
-            "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": traffic, "bytes_per_launch": bytes_per_launch,
-            "avg_launch_ms": ms / cnt, "bytes_rule": unit_note}
+        rule = "per cell: 54 inputs + 54 outputs x 8 B"
+    achieved = per_cell * n / (ms / cnt / 1e3) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
+            "peak_source": pk["source"], "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
+            "traffic": traffic, "bytes_per_launch": per_cell * n, "avg_launch_ms": round(ms / cnt, 4),
+            "bytes_rule": rule}
 
 
-def main_ours(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    res, f = run_ours(args, rank, world, local)
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_port(f, None)
-    if rank == 0:
-        line = {"metric": METRIC, "value": round(res["value"], 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": round(res["ms_per_step"], 4), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded C2 generator; the reference ships no benchmark data)",
-                "config": workload_config(world, {"update_passes_per_step": res["passes"][-args.steps:],
-                                                  "precision": args.precision}),
-                "e2e": res["e2e"], "gpu_launches": res["gpu_launches"] * world, "clocks": res["clocks"],
-                "roofline": roofline(res, res["n"], args.steps, args.precision == "mixed", args.isor),
-                "kernel_ms": {k: round(v[0], 3) for k, v in res["kernel_ms"].items()}}
-        if cpu is not None:
-            line["cpu_baseline"] = cpu
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-        dist.destroy_process_group()
+# ---------------------------------------------------------------- CPU baselines
+def cpu_baseline_port(tk, rho, y, ns=1024):
+    """The oracle (a faithful FP64 C restatement) on one host core, bounded sample."""
+    from oracle.oracle import Oracle
+    o = Oracle()
+    tk, rho, y = tk[:ns].copy(), rho[:ns].copy(), np.ascontiguousarray(y[:, :ns])
+    t0 = time.perf_counter()
+    yc, mu, lam, dk, _ = o.props(tk, y)
+    o.cp(tk, yc)
+    o.enthalpy(tk, yc)
+    o.omega(tk, rho, yc)
+    rc, sour = o.rates(tk, rho, yc)
+    yn, s, passes = o.species_update(rho, yc, rc, sour, DT, isor=ISOR, relx=RELX, tol=TOL)
+    dt = time.perf_counter() - t0
+    return {"value": round(ns / dt, 1), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"first {ns} cells of the field, one full sweep (oracle/unichem_oracle.c, -O2, 1 thread; "
+                      f"{passes} update passes), {dt:.2f} s"}
 
 
-# ---------------------------------------------------------------- reference arm
 def _ref_worker(args_tuple):
-    """One host process: the reference's own routines on a chunk of cells."""
+    """One host process: the reference's own routines on a chunk of cells (one full sweep)."""
     tk, rho, y, isor = args_tuple
     from oracle.ref import RefUnicorn
     r = _ref_worker.r if hasattr(_ref_worker, "r") else None
@@ -298,12 +278,248 @@ def _ref_worker(args_tuple):
         r = _ref_worker.r = RefUnicorn()
     t0 = time.perf_counter()
     yc, mu, lam, vdf = r.props(tk, y)
-    cp = r.cp(tk, yc)
-    q = r.omega(tk, rho, yc)
+    r.cp(tk, yc)
+    r.omega(tk, rho, yc)
     yn, s1, s2, passes = r.species_update(tk, rho, yc, DT, isor=isor, relx=RELX, tol=TOL)
     return len(tk), time.perf_counter() - t0, passes
 
 
+def reference_steps(tk, rho, y, steps, warmup, cores=None):
+    """The reference's routines on all host cores, one process per core, each step one chunk per core
+    (consecutive chunks of the field); returns (cells, seconds, passes per chunk)."""
+    import multiprocessing as mp
+    from oracle import ref as R
+    chunk = R.RefUnicorn().chunk
+    cores = cores or os.cpu_count() or 1
+    n = len(tk)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        def one_step(step):
+            jobs = []
+            for w in range(cores):
+                a = ((step * cores + w) * chunk) % (n - chunk)
+                jobs.append((tk[a:a + chunk].copy(), rho[a:a + chunk].copy(), np.ascontiguousarray(y[:, a:a + chunk]),
+                             ISOR))
+            t0 = time.perf_counter()
+            out = pool.map(_ref_worker, jobs)
+            return sum(o[0] for o in out), time.perf_counter() - t0, [o[2] for o in out]
+        pool.map(_ref_worker, [(tk[:64].copy(), rho[:64].copy(), np.ascontiguousarray(y[:, :64]), 1)] * cores)
+        for w in range(warmup):
+            one_step(w)
+        cells, secs, passes = 0, 0.0, []
+        for s in range(steps):
+            c, t, p = one_step(warmup + s)
+            cells += c
+            secs += t
+            passes += p
+    return cells, secs, passes, chunk, cores
+
+
+# ---------------------------------------------------------------- surrogate
+def train_surrogate(ntrain, steps, chunk=1 << 20, seed0=100):
+    """Training set of exact FP64 omega on states of the C3/C4 distribution (seeds seed0..), then Adam."""
+    import torch
+    from unicorn_b200 import unichem
+    from unicorn_b200.fields import batch_cells, nondimensional
+    from unicorn_b200.surrogate import Surrogate, raw_features
+    chunk = min(ntrain, chunk)
+    t0 = time.perf_counter()
+    s = Surrogate(capacity=ntrain, seed=1)
+    u = unichem.UniChem(chunk)
+    hull_lo, hull_hi, norm = None, None, None
+    for c in range(ntrain // chunk):
+        f = batch_cells(chunk, seed=seed0 + c)
+        tk, rho = nondimensional(f, u.scales, u.wm)
+        pref = u.scales["PBACK"] * u.scales["PSTR"]
+        u.upload(tk, rho, f.y)
+        u.set_pressure(f.p / u.scales["PSTR"])
+        feats = raw_features(f.T, f.p / pref, f.y)
+        if norm is None:
+            sub = np.arange(0, chunk, max(1, chunk // 65536))
+            q = u.omega().qdsp
+            norm = Surrogate.norm_from_sample(feats[:, sub], q[:, sub])
+            s.set_norm(**norm)
+        lo, hi = feats.min(axis=1), feats.max(axis=1)
+        hull_lo = lo if hull_lo is None else np.minimum(hull_lo, lo)
+        hull_hi = hi if hull_hi is None else np.maximum(hull_hi, hi)
+        s.add_data(u)
+    u.close()
+    norm.update(hull_lo=hull_lo, hull_hi=hull_hi)
+    s.set_norm(**norm)
+    t_data = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = s.train(steps=steps, batch=8192, lr=1e-3, seed=3)
+    t_train = time.perf_counter() - t0
+    info = {"train_states": ntrain, "train_steps": steps, "batch": 8192, "lr": 1e-3, "train_s": round(t_train, 2),
+            "data_s": round(t_data, 2), "train_samples_per_s": round(steps * 8192 / t_train, 1),
+            "loss_first": float(loss[:10].mean()), "loss_last": float(loss[-50:].mean())}
+    return s, info
+
+
+# ---------------------------------------------------------------- our arm
+def run_c2(args, dev, pk):
+    """The FP64 sweep of the 601x301 heptane jet field, each step from the seeded state."""
+    import torch
+    from unicorn_b200 import unichem
+    from unicorn_b200.fields import jet_field, nondimensional
+    f = jet_field(NZ, NR, fuel=FUEL, t_peak=TPEAK, seed=0)
+    u = unichem.UniChem(f.n, device=dev)
+    tk, rho = nondimensional(f, u.scales, u.wm)
+    st = DeviceState(u, tk, rho, f.y, dev)
+    ext = torch.cuda.ExternalStream(unichem_view(u)["stream"], device=dev)
+    ms, passes, kt = time_sweeps(u, st, ext, unichem.FP64, args.steps, args.warmup)
+    u.close()
+    return {"workload": "601x301 heptane jet field (fuel=11, T_peak 2300 K, seed 0), FP64 sweep from the seeded state",
+            "cells": f.n, "value": round(f.n * args.steps / (ms / 1e3), 1), "ms_per_step": round(ms / args.steps, 3),
+            "update_passes_per_step": passes,
+            "kernel_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in kt.items() if v[1]}}
+
+
+def run_forms(args, u, st, ext, f, tk, rho, fp64_sweep_ms, dev, pk):
+    """FP64 against the mixed form and the surrogate with per-cell fallback on the same field:
+    sweep and omega+property throughput and the error of each against FP64."""
+    from unicorn_b200 import unichem
+    n = f.n
+    res = {}
+    # mixed sweep
+    ms_mx, passes_mx, kt_mx = time_sweeps(u, st, ext, unichem.MIXED, args.steps, args.warmup)
+    fp64_tiles = u.stat("mixed_fp64_tiles") / u.stat("tiles")
+    # omega and properties of the seeded state, FP64 and mixed (outputs compared on the host)
+    out, evals = {}, {}
+    for name, prec in (("fp64", unichem.FP64), ("mixed", unichem.MIXED)):
+        st.restore()
+        evals[name] = time_calls(lambda prec=prec: u.chem_props(prec), ext, args.steps, args.warmup)
+        st.restore()
+        u.chem_props(prec)
+        d = {k: np.empty((52, n)) if k in ("qdsp", "vdf") else np.empty(n) for k in ("qdsp", "vmu", "vtc", "vdf", "cp", "h")}
+        u.download_outputs(d)
+        out[name] = d
+    ex, mx = out["fp64"], out["mixed"]
+    r_mx = omega_rel_error(mx["qdsp"], ex["qdsp"], f.y)
+    prop_err = {k: float((np.abs(mx[k] - ex[k]) / np.abs(ex[k])).max()) for k in ("vmu", "vtc", "vdf", "cp")}
+    big = np.abs(ex["h"]) > 1e-3 * np.abs(ex["h"]).max()
+    prop_err["h"] = float((np.abs(mx["h"] - ex["h"])[big] / np.abs(ex["h"][big])).max())
+    res["fp64"] = {"sweep_cell_updates_per_s": round(n * args.steps / (fp64_sweep_ms / 1e3), 1),
+                   "omega_props_ms": round(evals["fp64"], 3),
+                   "omega_props_cell_updates_per_s": round(n / (evals["fp64"] / 1e3), 1)}
+    res["mixed"] = {"sweep_cell_updates_per_s": round(n * args.steps / (ms_mx / 1e3), 1),
+                    "sweep_speedup_vs_fp64": round(fp64_sweep_ms / ms_mx, 3),
+                    "update_passes_per_step": passes_mx, "fp64_fallback_tiles": round(fp64_tiles, 4),
+                    "omega_props_ms": round(evals["mixed"], 3),
+                    "omega_props_cell_updates_per_s": round(n / (evals["mixed"] / 1e3), 1),
+                    "omega_props_speedup_vs_fp64": round(evals["fp64"] / evals["mixed"], 3),
+                    "omega_err_vs_fp64": err_summary(r_mx), "props_max_rel_err_vs_fp64": prop_err,
+                    "kernel_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in kt_mx.items() if v[1]}}
+    # surrogate with per-cell fallback
+    if args.no_mlp:
+        return res
+    try:
+        s, info = train_surrogate(args.train_states, args.train_steps)
+        u.set_pressure(f.p / u.scales["PSTR"])
+        ml = {"training": info}
+        for tol in MLP_TOLS + (float("inf"),):
+            def ev(tol=tol):
+                u.props(download=False)
+                u.cp_h(download=False)
+                s.omega(u, tol=tol, stats=False)
+            st.restore()
+            ms = time_calls(ev, ext, args.steps, args.warmup)
+            st.restore()
+            u.props(download=False)
+            stt = s.omega(u, tol=tol)
+            q = {"qdsp": np.empty((52, n))}
+            u.download_outputs(q)
+            r = omega_rel_error(q["qdsp"], ex["qdsp"], f.y)
+            key = "network_alone" if tol == float("inf") else f"tol={tol:g}"
+            ml[key] = {"omega_props_ms": round(ms, 3), "omega_props_cell_updates_per_s": round(n / (ms / 1e3), 1),
+                       "omega_props_speedup_vs_fp64": round(evals["fp64"] / ms, 3), "fallback": stt,
+                       "omega_err_vs_fp64": err_summary(r)}
+        s.close()
+        res["mlp_fallback"] = ml
+    except Exception as e:          # the headline stands; the failure is reported in the line
+        res["mlp_fallback"] = {"error": f"{type(e).__name__}: {e}"}
+    return res
+
+
+def main_ours(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from unicorn_b200 import unichem
+    from unicorn_b200.fields import nondimensional
+    pk = peaks()
+    f = head_field(args.cells or HEAD_CELLS, seed=HEAD_SEED + rank)
+    n = f.n
+    u = unichem.UniChem(n, device=dev)
+    tk, rho = nondimensional(f, u.scales, u.wm)
+    st = DeviceState(u, tk, rho, f.y, dev)
+    ext = torch.cuda.ExternalStream(unichem_view(u)["stream"], device=dev)
+    # ---------------- device-resident FP64 sweeps (the headline)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = ClockSampler(dev)
+    ms, passes, kt = time_sweeps(u, st, ext, unichem.FP64, args.steps, args.warmup, clocks=clk)
+    ms = max_over_ranks(ms, world)
+    # ---------------- end to end through the C ABI (pinned host buffers in and out)
+    pin = lambda *s: torch.empty(s, dtype=torch.float64, pin_memory=True).numpy()
+    h_tk, h_rho, h_y = pin(n), pin(n), pin(52, n)
+    h_tk[:], h_rho[:], h_y[:] = tk, rho, f.y
+    outs = dict(qdsp=pin(52, n), qdot=pin(n), domega_dy=pin(52, n), vmu=pin(n), vtc=pin(n), vdf=pin(52, n),
+                cp=pin(n), h=pin(n))
+    h_yout = pin(52, n)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    t0 = time.perf_counter()
+    e2e_passes = []
+    for _ in range(args.steps):
+        u.upload(h_tk, h_rho, h_y)
+        e2e_passes.append(u.sweep(DT, precision=unichem.FP64, isor=ISOR, relx=RELX, tol=TOL))
+        u.download_outputs(outs)
+        u.lib.uc_download_fields(u._h, None, None, unichem._p(h_yout), None, None)
+    u.sync()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    passes_run = float(np.mean([min(p, ISOR) for p in passes]))
+    line = None
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(world * n * args.steps / (ms / 1e3), 1), "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded heptane-generator field; the reference ships no benchmark data)",
+                "config": head_config(n, world, {"update_passes_per_step": passes, "e2e_update_passes": e2e_passes}),
+                "e2e": {"value": round(world * n * args.steps / e2e_s, 1), "unit": UNIT,
+                        "h2d_bytes_per_step": (2 + 52) * 8 * n, "d2h_bytes_per_step": (52 * 4 + 5) * 8 * n},
+                "gpu_launches": world * sum(c for _, c in kt.values()), "clocks": clk.summary(),
+                "roofline": roofline(kt, n, passes_run, pk),
+                "kernel_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in kt.items() if v[1]}}
+    # ---------------- the three forms and the C2 field (rank 0 of a one-GPU run)
+    if rank == 0 and world == 1:
+        if not args.no_forms:
+            line["forms"] = run_forms(args, u, st, ext, f, tk, rho, ms, dev, pk)
+        u.close()
+        if not args.no_c2:
+            line["c2"] = run_c2(args, dev, pk)
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_port(tk, rho, f.y)
+        print(json.dumps(line), flush=True)
+    else:
+        u.close()
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- reference arm
 def main_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -314,42 +530,23 @@ def main_reference(args):
                           "is not built: run python -c 'import __graft_entry__ as g; g.build()' where the reference "
                           "checkout exists"}))
         return
-    import multiprocessing as mp
-    from unicorn_b200.fields import jet_field, nondimensional
+    from unicorn_b200.fields import nondimensional
     r0 = R.RefUnicorn()
-    f = jet_field(NZ, NR, fuel=FUEL, t_peak=TPEAK, seed=0)
+    f = head_field(args.cells or HEAD_CELLS)
     tk, rho = nondimensional(f, r0.scales, r0.wm)
-    chunk = r0.chunk
-    cores = os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
-        def one_step(step):
-            jobs = []
-            for w in range(cores):
-                a = ((step * cores + w) * chunk) % (f.n - chunk)
-                jobs.append((tk[a:a + chunk].copy(), rho[a:a + chunk].copy(),
-                             np.ascontiguousarray(f.y[:, a:a + chunk]), ISOR))
-            t0 = time.perf_counter()
-            out = pool.map(_ref_worker, jobs)
-            return sum(o[0] for o in out), time.perf_counter() - t0, [o[2] for o in out]
-        for w in range(args.warmup):
-            one_step(w)
-        cells, secs, passes = 0, 0.0, []
-        for s in range(args.steps):
-            c, t, p = one_step(args.warmup + s)
-            cells += c
-            secs += t
-            passes += p
+    cells, secs, passes, chunk, cores = reference_steps(tk, rho, f.y, args.steps, args.warmup)
     v = cells / secs
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(secs / args.steps * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded C2 generator)",
-        "config": workload_config(1, {"update_passes_per_chunk": passes[:8]}),
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded heptane-generator field)",
+        "config": head_config(f.n, 1, {"update_passes_per_chunk": passes}),
         "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"{cores} chunks of {chunk} cells of the C2 field per step, one process per core, "
-                                   "each running the reference's PROPS/CKRATES/SOLVESP/SOLVEH-rate code "
-                                   "(translated from its Fortran, gcc -O2)"},
+                         "per_core": round(v / cores, 1),
+                         "sample": f"{cores} chunks of {chunk} cells of the field per step, one process per core, "
+                                   "each running the reference's property block, TCP, CKRATES, SOLVEH rates and "
+                                   "SOLVESP (translated from its Fortran, gcc -O2)"},
         "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
 
 
@@ -458,41 +655,10 @@ def main_c4(args):
     import torch
     from unicorn_b200 import unichem
     from unicorn_b200.fields import batch_cells, nondimensional
-    from unicorn_b200.surrogate import Surrogate, raw_features
-    ntrain = args.cells * 4 if args.cells else C4_TRAIN
+    ntrain = args.cells * 4 if args.cells else args.train_states
     nfield = args.cells or C4_FIELD
-    chunk = min(ntrain, 1 << 20)
     steps = args.train_steps
-    # ---- training set: exact FP64 omega of C3-distribution states, in chunks
-    t0 = time.perf_counter()
-    s = Surrogate(capacity=ntrain, seed=1)
-    u = unichem.UniChem(chunk)
-    hull_lo, hull_hi, norm = None, None, None
-    for c in range(ntrain // chunk):
-        f = batch_cells(chunk, seed=100 + c)
-        tk, rho = nondimensional(f, u.scales, u.wm)
-        pref = u.scales["PBACK"] * u.scales["PSTR"]
-        u.upload(tk, rho, f.y)
-        u.set_pressure(f.p / u.scales["PSTR"])
-        feats = raw_features(f.T, f.p / pref, f.y)
-        if norm is None:
-            sub = np.arange(0, chunk, max(1, chunk // 65536))
-            q = u.omega().qdsp
-            norm = Surrogate.norm_from_sample(feats[:, sub], q[:, sub])
-            s.set_norm(**norm)
-        lo, hi = feats.min(axis=1), feats.max(axis=1)
-        hull_lo = lo if hull_lo is None else np.minimum(hull_lo, lo)
-        hull_hi = hi if hull_hi is None else np.maximum(hull_hi, hi)
-        s.add_data(u)
-    u.close()
-    norm.update(hull_lo=hull_lo, hull_hi=hull_hi)
-    s.set_norm(**norm)
-    t_data = time.perf_counter() - t0
-    # ---- training (device time of the whole run, graph per step)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    loss = s.train(steps=steps, batch=8192, lr=1e-3, seed=3)
-    t_train = time.perf_counter() - t0
+    s, tinfo = train_surrogate(ntrain, steps)
     # ---- inference on a fresh field: exact FP64 omega vs surrogate + fallback
     f = batch_cells(nfield, seed=7)
     u = unichem.UniChem(nfield)
@@ -515,46 +681,40 @@ def main_c4(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps, r
 
+    pk = peaks()
     ms_exact, _ = timed(lambda: u.omega(download=False), args.steps)
     u.download_outputs(out)
     exact = out["qdsp"].copy()
     res = {}
     with ClockSampler(0) as clk:
-        for tol in (1e-3, 1e-1, 1e300, float("inf")):
+        for tol in MLP_TOLS + (float("inf"),):
             ms, _ = timed(lambda: s.omega(u, tol=tol, stats=False), args.steps)
-            st = s.omega(u, tol=tol)
+            stt = s.omega(u, tol=tol)
             u.download_outputs(out)
-            q = out["qdsp"]
-            wmax = np.abs(exact).max(axis=0)
-            r = np.abs(q - exact) / np.maximum(np.abs(exact), 1e-6 * wmax + 1e-300)
-            r[f.y <= 1e-8] = 0.0
-            err = r.max(axis=0)
-            res["tol=%g" % tol] = {"ms": round(ms, 3), "cell_updates_per_s": round(nfield / (ms / 1e3), 1),
-                                  "speedup_vs_fp64": round(ms_exact / ms, 3), "tiles_exact": round(st["tiles_exact"], 4),
-                                  "cells_outside_hull": round(st["cells_outside_hull"], 5),
-                                  "median_sampled_residual": st["median_residual"],
-                                  "err_vs_fp64_p50": float(np.median(err)), "err_vs_fp64_p99": float(np.quantile(err, 0.99)),
-                                  "frac_cells_err_le_1e-3": round(float((err <= 1e-3).mean()), 4)}
+            r = omega_rel_error(out["qdsp"], exact, f.y)
+            key = "network_alone" if tol == float("inf") else f"tol={tol:g}"
+            res[key] = {"ms": round(ms, 3), "cell_updates_per_s": round(nfield / (ms / 1e3), 1),
+                        "speedup_vs_fp64": round(ms_exact / ms, 3), "fallback": stt,
+                        "omega_err_vs_fp64": err_summary(r)}
     u.close()
     s.close()
-    pure = res["tol=inf"]          # the network alone: features, 5 tensor-core layers, decode
+    pure = res["network_alone"]          # features, 5 tensor-core layers, decode
     tflops = MLP_FLOP_PER_CELL * nfield / (pure["ms"] / 1e3) / 1e12
-    line = {"metric": "omega cell-updates/s: learned surrogate + per-tile FP64 fallback at the stated error",
+    line = {"metric": "omega cell-updates/s: learned surrogate + per-cell FP64 fallback at the stated error",
             "value": res["tol=0.001"]["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": res["tol=0.001"]["ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16 network / f64 fallback", "data": "synthetic (seeded C3/C4 generators)",
-            "config": {"workload": f"C4: network 54-256x4-52 GELU, Adam lr 1e-3 batch 8192, {steps} steps on {ntrain} "
+            "config": {"workload": f"C4: network 54-256x4-52 GELU, Adam batch 8192, {steps} steps on {ntrain} "
                                    f"exact-FP64 states of the C3 distribution; inference on a fresh {nfield}-cell field "
-                                   "with fallback per 32-cell tile (training hull, one sampled residual per tile)",
+                                   "with per-cell fallback to the exact FP64 kernel",
                        "fp64_omega_ms": round(ms_exact, 3),
                        "fp64_omega_cell_updates_per_s": round(nfield / (ms_exact / 1e3), 1),
-                       "by_tolerance": res, "train_s": round(t_train, 2), "data_s": round(t_data, 2),
-                       "train_samples_per_s": round(steps * 8192 / t_train, 1),
-                       "loss_first": float(loss[:10].mean()), "loss_last": float(loss[-50:].mean())},
+                       "by_tolerance": res, "training": tinfo},
             "e2e": None, "gpu_launches": None, "clocks": clk.summary(),
-            "roofline": {"kernel": "surrogate forward (features, 5 tensor-core layers, decode; tol=inf)", "bound": "tensor",
-                         "achieved": round(tflops, 2), "peak": 1693.5, "peak_source": "measured (bf16 burst)",
-                         "unit": "TFLOP/s", "frac": round(tflops / 1693.5, 4), "traffic": None,
+            "roofline": {"kernel": "surrogate forward (features, 5 tensor-core layers, decode; network alone)",
+                         "bound": "tensor", "achieved": round(tflops, 2), "peak": pk["bf16_tflops"],
+                         "peak_source": pk["source"] + ", bf16 burst", "unit": "TFLOP/s",
+                         "frac": round(tflops / pk["bf16_tflops"], 4), "traffic": None,
                          "flops_rule": f"{MLP_FLOP_PER_CELL} flop per cell (padded 64-256x4-64 layers) / forward time"}}
     print(json.dumps(line), flush=True)
 
@@ -781,14 +941,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cells", type=int, default=0, help="use only the first N cells (profiling runs)")
     ap.add_argument("--isor", type=int, default=ISOR, help="update passes cap (profiling runs)")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "c5-live"],
-                    help="c2: the species sweep of the 601x301 heptane field (headline); c3: batched stiff "
-                         "integration; c4: learned surrogate with fallback; c5: in-loop sweeps; c5-live: in-loop "
-                         "sweeps with live transport faces and the enthalpy equation")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="c3, c5-live: precision")
+    ap.add_argument("--workload", default="head", choices=["head", "c3", "c4", "c5", "c5-live"],
+                    help="head: the species sweep of the 1M-cell heptane field with the FP64 / mixed / surrogate "
+                         "comparison and the 601x301 field (headline); c3: batched stiff integration; c4: learned "
+                         "surrogate with fallback; c5: in-loop sweeps; c5-live: in-loop sweeps with live transport "
+                         "faces and the enthalpy equation")
     ap.add_argument("--sweeps", type=int, default=1000, help="c5: sweeps")
     ap.add_argument("--presweeps", type=int, default=200, help="c5-live: species-only sweeps before the live ones")
-    ap.add_argument("--train-steps", type=int, default=2000, help="c4: Adam steps")
+    ap.add_argument("--train-steps", type=int, default=TRAIN_STEPS, help="surrogate: Adam steps")
+    ap.add_argument("--train-states", type=int, default=TRAIN_STATES, help="surrogate: training states")
+    ap.add_argument("--no-forms", action="store_true", help="head: skip the mixed / surrogate comparison")
+    ap.add_argument("--no-mlp", action="store_true", help="head: skip the surrogate")
+    ap.add_argument("--no-c2", action="store_true", help="head: skip the 601x301 field")
     args = ap.parse_args()
     if args.workload == "c3":
         main_c3(args)

@@ -77,6 +77,16 @@ int uc_get_scales(const uc_ctx *ctx, uc_scales *sc, double *wm, double *hfo);
 int uc_upload_fields(uc_ctx *ctx, const double *tk, const double *rho, const double *fsp,
                      const double *stmf, const double *stnd);
 
+/* The same from arrays already in device memory (a host whose fields live on
+ * the GPU: CUDA Fortran / OpenACC device arrays): tk, rho [ld], fsp [52][ld],
+ * stmf, stnd [ld] or NULL, with row stride ld >= n elements. Asynchronous on
+ * the context's stream (uc_device_view_get().stream): writes to the source
+ * arrays made on other streams must be complete or ordered before the call,
+ * and the sources must not change until the copies have run (uc_sync).
+ * Replaces: the same COMMON state as uc_upload_fields. */
+int uc_upload_fields_device(uc_ctx *ctx, const double *tk, const double *rho, const double *fsp,
+                            const double *stmf, const double *stnd, int ld);
+
 /* Copy the device-resident state back (any pointer may be NULL). */
 int uc_download_fields(uc_ctx *ctx, double *tk, double *rho, double *fsp, double *stmf,
                        double *stnd);
@@ -130,6 +140,14 @@ int uc_temperature_from_h(uc_ctx *ctx, const double *ht);
  * preceded by the property block of main:821-1006. */
 int uc_sweep(uc_ctx *ctx, int precision, double dt, int isor, double relx, double tol, double spnorm,
              const double *face_sum, const double *face_nbr, int *passes);
+
+/* The chemistry and properties of the device-resident state without the
+ * update: the Y clip with transport properties, cp and h, then omega and
+ * d(omega)/dY (the first three steps of uc_sweep, in its order; no RC plane is
+ * kept). Asynchronous; read the outputs with uc_download_outputs.
+ * Replaces: the property block of main:821-1006, the TCP loop of
+ * spgsolv.f:102-173 and the rate part of SOLVEH (solveh.f:116-1145). */
+int uc_chem_props(uc_ctx *ctx, int precision);
 
 /* ---------------------------------------------------------------------------
  * The species equations' face coefficients on the device.

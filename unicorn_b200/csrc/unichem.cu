@@ -580,6 +580,42 @@ extern "C" int uc_upload_fields(uc_ctx *ctx, const double *tk, const double *rho
     return UC_OK;
 }
 
+// rows of a device array with row stride ld (elements) into a context array [rows][npad]
+static int copy_rows_device(uc_ctx *ctx, double *dst, const double *src, int rows, int ld)
+{
+    if (src) {
+        CK(cudaMemcpy2DAsync(dst, (size_t)ctx->npad * sizeof(double), src, (size_t)ld * sizeof(double),
+                             (size_t)ctx->n * sizeof(double), rows, cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+        CK(cudaMemsetAsync(dst, 0, (size_t)rows * ctx->npad * sizeof(double), ctx->stream));
+    }
+    if (ctx->npad > ctx->n) {
+        pad_rows_kernel<<<64, 256, 0, ctx->stream>>>(dst, rows, ctx->n, ctx->npad);
+        CK(cudaGetLastError());
+    }
+    return UC_OK;
+}
+
+extern "C" int uc_upload_fields_device(uc_ctx *ctx, const double *tk, const double *rho, const double *fsp,
+                                       const double *stmf, const double *stnd, int ld)
+{
+    if (!ctx || !tk || !rho || !fsp)
+        return set_err(ctx, UC_E_ARG, "uc_upload_fields_device: tk, rho and fsp are required");
+    if (ld < ctx->n) return set_err(ctx, UC_E_ARG, "uc_upload_fields_device: row stride %d below n = %d", ld, ctx->n);
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(copy_rows_device(ctx, ctx->tk, tk, 1, ld));
+    RET_IF(copy_rows_device(ctx, ctx->rho, rho, 1, ld));
+    RET_IF(copy_rows_device(ctx, ctx->y, fsp, LSP, ld));
+    RET_IF(copy_rows_device(ctx, ctx->soot, stmf, 1, ld));
+    RET_IF(copy_rows_device(ctx, ctx->soot + ctx->npad, stnd, 1, ld));
+    CK(cudaMemcpyAsync(ctx->y0, ctx->y, (size_t)LSP * ctx->npad * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->soot0, ctx->soot, 2 * (size_t)ctx->npad * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    ctx->have_fields = true;
+    ctx->have_rc = false;
+    ctx->rc_start = false;
+    return UC_OK;
+}
+
 extern "C" int uc_download_fields(uc_ctx *ctx, double *tk, double *rho, double *fsp, double *stmf, double *stnd)
 {
     if (!ctx) return UC_E_ARG;
@@ -773,6 +809,17 @@ static int cp_h_impl(uc_ctx *ctx, int precision, double *cp, double *h)
 extern "C" int uc_cp_h(uc_ctx *ctx, double *cp, double *h)
 {
     return cp_h_impl(ctx, UC_FP64, cp, h);
+}
+
+extern "C" int uc_chem_props(uc_ctx *ctx, int precision)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "uc_chem_props before uc_upload_fields");
+    if (precision != UC_FP64 && precision != UC_MIXED) return set_err(ctx, UC_E_ARG, "unknown precision %d", precision);
+    RET_IF(props_impl(ctx, precision, nullptr, nullptr, nullptr));
+    RET_IF(cp_h_impl(ctx, precision, nullptr, nullptr));
+    CK(cudaSetDevice(ctx->device));
+    return launch_chem(ctx, precision, false, true);
 }
 
 extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, double tol, double spnorm,

@@ -90,6 +90,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.uc_get_scales.argtypes = [vp, ctypes.POINTER(Scales), P, P]
     lib.uc_upload_fields.argtypes = [vp, P, P, P, P, P]
     lib.uc_download_fields.argtypes = [vp, P, P, P, P, P]
+    lib.uc_upload_fields_device.argtypes = [vp, vp, vp, vp, vp, vp, ctypes.c_int]
     lib.uc_rates.argtypes = [vp, ctypes.c_int, P]
     lib.uc_omega.argtypes = [vp, ctypes.c_int, P, P, P]
     lib.uc_props.argtypes = [vp, P, P, P]
@@ -100,6 +101,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.uc_sweep.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                              ctypes.c_double, P, P, ctypes.POINTER(ctypes.c_int)]
     lib.uc_download_outputs.argtypes = [vp, P, P, P, P, P, P, P, P]
+    lib.uc_chem_props.argtypes = [vp, ctypes.c_int]
     lib.uc_profile.argtypes = [vp, ctypes.c_int]
     lib.uc_profile_read.argtypes = [vp, P, ctypes.POINTER(ctypes.c_int)]
     lib.uc_stat.argtypes = [vp, ctypes.c_char_p, P]
@@ -202,6 +204,11 @@ class UniChem:
         stmf, stnd = _in(stmf, (n,)), _in(stnd, (n,))
         self._ck(self.lib.uc_upload_fields(self._h, _p(tk), _p(rho), _p(y), _p(stmf), _p(stnd)))
 
+    def upload_device(self, tk, rho, y, stmf=None, stnd=None, ld=None):
+        """State from device memory: integer device addresses (e.g. torch's data_ptr()) of
+        tk, rho [ld], y [52][ld], stmf, stnd [ld] (or None); asynchronous on the context's stream."""
+        self._ck(self.lib.uc_upload_fields_device(self._h, tk, rho, y, stmf, stnd, int(ld if ld is not None else self.n)))
+
     def download(self):
         n = self.n
         tk, rho, y, s1, s2 = np.empty(n), np.empty(n), np.empty((LSP, n)), np.empty(n), np.empty(n)
@@ -268,6 +275,10 @@ class UniChem:
         self._ck(self.lib.uc_sweep(self._h, precision, dt, int(isor), relx, tol, spnorm, _p(fs), _p(fn),
                                    ctypes.byref(passes)))
         return passes.value
+
+    def chem_props(self, precision: int = FP64):
+        """Y clip + transport, cp/h, omega and d(omega)/dY of the device state (no update); asynchronous."""
+        self._ck(self.lib.uc_chem_props(self._h, precision))
 
     def download_outputs(self, out: dict | None = None) -> dict:
         """Copy omega, d(omega)/dY, QDOT, transport, cp and h of the last sweep to host arrays."""
