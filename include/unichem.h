@@ -133,9 +133,10 @@ int uc_temperature_from_h(uc_ctx *ctx, const double *ht);
  * and h, rate coefficients with omega and d(omega)/dY at the start-of-step
  * state (CKRATES + SOLVEH rates), then the point-implicit update (SOLVESP)
  * with the arguments of uc_species_update. Outputs stay on the device
- * (uc_device_view_get / the download calls). With UC_MIXED the property
- * polynomials, square roots and sums also run in FP32 (the state's clip and
- * closure, Kc and the update stay FP64).
+ * (uc_device_view_get / the download calls). With UC_MIXED the per-pair
+ * terms of the transport sums (square roots, divisions, products) also run in
+ * FP32; the polynomials in T, the sums over species, cp and h, the state's
+ * clip and closure, Kc and the update stay FP64.
  * Replaces: CALL SPGSOLV's chemistry part (src/lib/spgsolv.f:102-176,1291-1298)
  * preceded by the property block of main:821-1006. */
 int uc_sweep(uc_ctx *ctx, int precision, double dt, int isor, double relx, double tol, double spnorm,

@@ -1,18 +1,25 @@
-"""Mixed-precision form (UC_MIXED) against the FP64 oracle.
+"""Mixed-precision form (UC_MIXED) against the FP64 oracle, at the stated accuracy.
 
-The stated accuracy of the mixed form: omega_k within 1e-3 relative on
-species above 1e-8 mass fraction. Where omega_k is a near-cancelling net of
-large gross rates, FP32 rate terms cannot meet a relative bound on the net,
-so the bound used is |d omega| <= 1e-3 * max(|omega|, 1e-4 * gross) -- the
-reported statistics give the plain relative figure as well.
+Stated accuracy of the mixed form: omega_k within 1e-3 relative on every
+(cell, species) with Y_k > 1e-8, where the only floor is the stated
+near-zero net: |omega_k| below 1e-6 of the cell's largest |omega_j| is
+measured against that 1e-6 max|omega_j|; the transport properties, cp and h
+within 1e-6 relative on every cell.
 """
 import numpy as np
 import pytest
 
-from test_gpu_parity import gross
-from unicorn_b200.fields import jet_field, nondimensional
+from unicorn_b200.fields import batch_cells, jet_field, nondimensional
 
 pytestmark = pytest.mark.gpu
+
+
+def omega_bound_ok(q, exact, y, tol=1e-3):
+    """|q - exact| <= tol * max(|exact|, 1e-6 max_j |exact_j|) on species above 1e-8; (ok mask, rel)."""
+    wmax = np.abs(exact).max(axis=0, keepdims=True)
+    rel = np.abs(q - exact) / np.maximum(np.abs(exact), 1e-6 * wmax + 1e-300)
+    mask = y > 1e-8
+    return rel[mask], mask
 
 
 @pytest.fixture(scope="module")
@@ -29,25 +36,47 @@ def test_mixed_omega_error(oracle, c2_slice):
     with unichem.UniChem(len(tk)) as u:
         u.upload(tk, rho, y)
         om = u.omega(precision=unichem.MIXED)
+        fp64_tiles = u.stat("mixed_fp64_tiles") / u.stat("tiles")
         rc32 = u.ckrates(precision=unichem.MIXED, return_rc=True)
     assert np.isfinite(om.qdsp).all() and np.isfinite(om.domega_dy).all() and np.isfinite(rc32).all()
     q, qd, h, d = oracle.omega(tk, rho, y)
-    g = gross(oracle, tk, rho, y)
-    mask = y > 1e-8
-    err = np.abs(om.qdsp - q)
-    rel = err / np.maximum(np.abs(q), 1e-300)
-    frac_rel = np.mean(rel[mask] <= 1e-3)
-    bound = 1e-3 * np.maximum(np.abs(q), 1e-4 * g)
-    print(f"\nmixed omega: {mask.sum()} (cell,species) pairs with Y>1e-8; "
-          f"{100 * frac_rel:.3f}% within 1e-3 relative; median rel {np.median(rel[mask]):.2e}; "
-          f"max err/gross {np.max(err[mask] / np.maximum(g[mask], 1e-300)):.2e}")
-    assert np.all(err[mask] <= bound[mask])
-    assert frac_rel > 0.99
+    rel, mask = omega_bound_ok(om.qdsp, q, y)
+    print(f"\nmixed omega on the C2 slice: {mask.sum()} (cell, species) pairs with Y>1e-8; max rel {rel.max():.2e}, "
+          f"median {np.median(rel):.2e}; tiles recomputed in FP64 {100 * fp64_tiles:.1f}%")
+    assert rel.max() <= 1e-3
     # diagonal linearisation: all-positive sums
     assert np.allclose(om.domega_dy, d, rtol=1e-4, atol=0)
     rc64, _ = oracle.rates(tk, rho, y)
     big = np.abs(rc64) > 1e-30
     assert np.allclose(rc32[big], rc64[big], rtol=1e-5, atol=0)
+
+
+def test_mixed_omega_and_properties_on_the_1m_field():
+    """The mixed form against the FP64 form (itself pinned to the oracle at 1e-11) on every 4th cell of
+    the 1M-cell heptane benchmark field: omega and every property at the stated bounds."""
+    from unicorn_b200 import unichem
+    f = batch_cells(1 << 20, seed=7)
+    sel = np.arange(0, f.n, 4)
+    out = {}
+    with unichem.UniChem(len(sel)) as u:
+        tk, rho = nondimensional(f, u.scales, u.wm)
+        tk, rho, y = tk[sel].copy(), rho[sel].copy(), np.ascontiguousarray(f.y[:, sel])
+        for prec in (unichem.FP64, unichem.MIXED):
+            u.upload(tk, rho, y)
+            u.chem_props(prec)
+            d = {k: np.empty((52, len(sel))) if k in ("qdsp", "vdf") else np.empty(len(sel))
+                 for k in ("qdsp", "vmu", "vtc", "vdf", "cp", "h")}
+            u.download_outputs(d)
+            out[prec] = d
+        fp64_tiles = u.stat("mixed_fp64_tiles") / u.stat("tiles")
+    ex, mx = out[unichem.FP64], out[unichem.MIXED]
+    rel, mask = omega_bound_ok(mx["qdsp"], ex["qdsp"], y)
+    print(f"\n1M field (every 4th cell): omega max rel {rel.max():.2e}; tiles recomputed in FP64 {100 * fp64_tiles:.1f}%")
+    assert rel.max() <= 1e-3
+    for k in ("vmu", "vtc", "vdf", "cp", "h"):
+        r = np.abs(mx[k] - ex[k]) / np.abs(ex[k])
+        print(f"  {k}: max rel {r.max():.2e}")
+        assert r.max() <= 1e-6, (k, r.max())
 
 
 def test_mixed_sweep_vs_fp64_sweep(oracle, c2_slice):
@@ -70,16 +99,10 @@ def test_mixed_sweep_vs_fp64_sweep(oracle, c2_slice):
 
 
 def test_mixed_properties_vs_oracle(oracle, c2_slice):
-    """Mixed-form properties (FP32 polynomials, square roots and sums) against the FP64 oracle.
-
-    mu, lambda, D_k and cp are sums of positive terms. The median relative
-    error is at most 1e-6 (the stated property accuracy); the largest is
-    bounded by 1e-5 for mu, lambda and cp (FP32 rounding of the polynomials in
-    T up to T^5 and of the sums over the sub-mixture) and by 3e-5 for D_k,
-    whose collision integral is a quartic in T* = T/eps_ij with
-    alternating-sign coefficients (main:944-952), evaluated in FP32. The
-    mixture enthalpy h = sum Y_k h_k is a signed sum (formation enthalpies),
-    so it is compared against the scale sum |Y_k h_k|."""
+    """Mixed-form properties (FP32 per-pair terms of the transport sums; polynomials, sums, cp and h in
+    FP64) against the FP64 oracle: every cell within 1e-6 relative. The mixture enthalpy h = sum Y_k h_k
+    is a signed sum (formation enthalpies); it is compared against |h| where |h| is above 1e-3 of the
+    field's largest, and against the scale sum |Y_k h_k| everywhere."""
     from unicorn_b200 import unichem
     tk, rho, y = c2_slice
     with unichem.UniChem(len(tk)) as u:
@@ -94,12 +117,11 @@ def test_mixed_properties_vs_oracle(oracle, c2_slice):
     for name, a, b in (("mu", out["vmu"], mu), ("lambda", out["vtc"], lam), ("D_k", out["vdf"], dk), ("cp", out["cp"], cp)):
         rel = np.abs(a - b) / np.abs(b)
         stats[name] = (np.median(rel), rel.max())
+    big = np.abs(hm) > 1e-3 * np.abs(hm).max()
+    rel_h = np.abs(out["h"] - hm)[big] / np.abs(hm[big])
+    stats["h"] = (np.median(rel_h), rel_h.max())
     print("\nmixed properties (median, max rel): " + ", ".join(f"{k} {v[0]:.1e}/{v[1]:.1e}" for k, v in stats.items()))
     for name, (med, mx) in stats.items():
-        assert med <= 1e-6, (name, med)
-        assert mx <= (3e-5 if name == "D_k" else 1e-5), (name, mx)
+        assert mx <= 1e-6, (name, mx)
     hscale = (np.abs(yc * hk)).sum(0)
-    rel_h = np.abs(out["h"] - hm) / hscale
-    stats["h"] = (np.median(rel_h), rel_h.max())
-    print(f"mixed h (median, max rel to sum |Y_k h_k|): {stats['h'][0]:.1e}/{stats['h'][1]:.1e}")
-    assert rel_h.max() <= 1e-5
+    assert (np.abs(out["h"] - hm) / hscale).max() <= 1e-6

@@ -47,8 +47,22 @@ struct ChemMArgs {
 enum { SM_TKD = 0, SM_LNT, SM_INVT, SM_LNRHO, SM_LNRUT, SM_RHO, SM_LNDMOLEA, SM_TB0, SM_STMF = SM_TB0 + 11,
        SM_STND, SM_N };
 
-constexpr size_t CHEMM_SMEM = PAIRTABM_BYTES + sizeof(float) * (size_t)(LRX * TILE + LSP * TILE) +
+constexpr size_t CHEMM_SMEM = PAIRTABM_BYTES + sizeof(float) * (size_t)(LRX * TILE + 3 * LSP * TILE) +
                               sizeof(double) * (size_t)(2 * LSP * TILE + SM_N * TILE) + 64;
+
+// Error control of the FP32 species sums. Every term of a net rate carries at
+// most UC_MIXED_TERM_ERR relative error (a few FP32 roundings of the rate
+// coefficient, the fall-off factor and the Y products), so the net of species k
+// is off by at most UC_MIXED_TERM_ERR * gross_k. A tile in which that bound
+// exceeds UC_MIXED_OMEGA_TOL * max(|omega_k|, 1e-6 * max_j |omega_j|) for a
+// species above 1e-8 mass fraction is recomputed in FP64, as are tiles with a
+// rate beyond the FP32 range.
+#ifndef UC_MIXED_TERM_ERR
+#define UC_MIXED_TERM_ERR 2.0e-6
+#endif
+#ifndef UC_MIXED_OMEGA_TOL
+#define UC_MIXED_OMEGA_TOL 1.0e-3
+#endif
 
 // e^x for a double argument: n = round(x/ln2) and the remainder in FP64,
 // the exponential of the remainder in FP32, scaled by 2^n.
@@ -75,7 +89,9 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_mixed_kernel(const ChemM
     PairTabM *sTab = reinterpret_cast<PairTabM *>(smem);
     float *sRC = reinterpret_cast<float *>(smem + PAIRTABM_BYTES);   // [544][32]
     float *sYf = sRC + LRX * TILE;                                   // [52][32]
-    double *sY = reinterpret_cast<double *>(sYf + LSP * TILE);       // [52][32]
+    float *sNet = sYf + LSP * TILE;                                  // [52][32] |W_k net_k|
+    float *sGross = sNet + LSP * TILE;                               // [52][32] W_k sum |terms|
+    double *sY = reinterpret_cast<double *>(sGross + LSP * TILE);    // [52][32]
     double *sG = sY + LSP * TILE;                                    // [52][32] Gibbs exponents, then HRR terms
     double *sC = sG + LSP * TILE;                                    // [SM_N][32]
     uint64_t *bar = reinterpret_cast<uint64_t *>(sC + SM_N * TILE);
@@ -248,7 +264,7 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_mixed_kernel(const ChemM
             const int ns = P.nspec_of_warp[warp];
             for (int s = 0; s < ns; ++s) {
                 const int k = P.spec_of_warp[warp][s];
-                float sum = 0.0f, cmp = 0.0f;
+                float sum = 0.0f, cmp = 0.0f, gross = 0.0f;
                 const int len = P.prd_len[k], off = P.prd_off[k];
                 for (int t = 0; t < len; ++t) {
                     const unsigned code = P.prd_term[off + t];
@@ -258,9 +274,12 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_mixed_kernel(const ChemM
                     for (int q = 0; q < P.ra_len[r]; ++q) v *= sYf[P.ra_sp[r * 3 + q] * TILE + lane];
                     if (code & 0x4000) v *= (float)P.prd_coef[off + t];
                     neumaier_add(sum, cmp, (code & 0x8000) ? -v : v);
+                    gross += fabsf(v);
                 }
                 const float net = sum + cmp;                      // sum over the PRD list of species k
                 const float wnet = (float)P.WM[k] * net;
+                sNet[k * TILE + lane] = fabsf(wnet);
+                sGross[k * TILE + lane] = (float)P.WM[k] * gross;
                 if (a.qdsp) a.qdsp[(size_t)k * a.npad + cell] = -(double)(RCONVf * wnet);
                 const double *pa = P.poly + k * 14 + ip;
                 const float HS = ((float)pa[0] * TKD + (float)pa[1] * TKD2 * 0.5f + (float)pa[2] * TKD3 * (1.0f / 3.0f) +
@@ -292,6 +311,20 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_mixed_kernel(const ChemM
             for (int k = 0; k < LSP; ++k) neumaier_add(s, c, (float)sG[k * TILE + lane]);
             a.qdot[cell] = -(double)((s + c) * RCONVf);
         }
+        if (warp == 1) {
+            // error bound of the FP32 nets against the stated accuracy (see UC_MIXED_TERM_ERR)
+            float wmax = 0.0f;
+            for (int k = 0; k < LSP; ++k) wmax = fmaxf(wmax, sNet[k * TILE + lane]);
+            bool bad = false;
+            for (int k = 0; k < LSP; ++k) {
+                const float ref = fmaxf(sNet[k * TILE + lane], 1.0e-6f * wmax);
+                if (sY[k * TILE + lane] > 1.0e-8 &&
+                    (double)UC_MIXED_TERM_ERR * sGross[k * TILE + lane] > (double)UC_MIXED_OMEGA_TOL * ref)
+                    bad = true;
+            }
+            if (__any_sync(0xffffffffu, bad) && lane == 0) s_flag = 1;
+        }
+        __syncthreads();
         if (tid == 0) {
             a.tile_flag[tile] = s_flag;
             s_flag = 0;                 // read again only after the next tile's first barrier

@@ -145,6 +145,128 @@ __global__ void __launch_bounds__(128) props_kernel(const PropArgs a)
     }
 }
 
+// The collision integral CI11 of the pair (i, j) in Horner form with the
+// argument t = T / ETLJ1 from the reciprocal table: FP64, no division
+// (the quartic in T* has alternating-sign coefficients and cancels).
+__device__ __forceinline__ double ci11_horner(const DevParams &P, int ij, double TKD1)
+{
+    const double t = TKD1 * P.RETLJ1[ij];
+    const double *c = P.ci11 + ci_range(t) * 5;
+    return fma(fma(fma(fma(c[4], t, c[3]), t, c[2]), t, c[1]), t, c[0]);
+}
+
+// The mixed form of src/unicornd-mild-sd-5.f:821-1006: the per-pair work of
+// the Wilke sums and of the binary diffusion sums (square roots, divisions,
+// the products of each term) runs in FP32; what cancels or accumulates stays
+// FP64 -- the polynomials in T (cp/R of the Eucken factor, the Omega(2,2) fit
+// to T^5, the CI11 quartic, all in Horner form), the sums over species, the
+// mole numbers and TMOLE - X_i, and the per-species values ATC, AMU. Every
+// pair term then carries a few FP32 roundings and nothing adds them up, so
+// mu, lambda and D_k stay within a few 1e-7 of the FP64 form.
+__global__ void __launch_bounds__(128) props_mixed_kernel(const PropArgs a)
+{
+    const DevParams &P = *a.P;
+    const size_t np = a.npad;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < (size_t)a.n; c += (size_t)gridDim.x * blockDim.x) {
+        double TMASS = 0.0;
+        for (int k = 0; k < LSP - 1; ++k) {
+            double yk = a.y[k * np + c];
+            if (yk < 0.0) { yk = 0.0; a.y[k * np + c] = 0.0; }
+            TMASS = TMASS + yk;
+        }
+        a.y[(LSP - 1) * np + c] = 1.0 - TMASS;
+        int8_t sub[LSP];
+        double X[LSP];
+        int IA = 0;
+        double TMASSD = 0.0, TMOLE = 0.0;
+        for (int k = 0; k < LSP - 1; ++k) {
+            const double yk = a.y[k * np + c];
+            if (yk < 1.0e-03) continue;
+            sub[IA] = (int8_t)k;
+            TMASSD = TMASSD + yk;
+            X[IA] = yk / P.WM[k];
+            TMOLE = TMOLE + X[IA];
+            ++IA;
+        }
+        int LSPT = IA + 1;
+        if (LSPT >= LSP) LSPT = LSP;
+        sub[LSPT - 1] = LSP - 1;
+        X[LSPT - 1] = (1.0 - TMASSD) / P.WM[LSP - 1];
+        TMOLE = TMOLE + X[LSPT - 1];
+        const double tk = a.tk[c];
+        const double TKRT = sqrt(tk);
+        const double TKD1 = tk * P.TSTR;
+        const int IPL1 = TKD1 >= UC_TPOL1 ? 7 : 0, IPL2 = TKD1 >= UC_TPOL1 ? 6 : 0;
+        const float TKBP = (float)(tk * TKRT / P.PBACK);
+        double ATC[LSP], AMU[LSP];
+        float ATCf[LSP], AMUf[LSP], Xf[LSP];
+        for (int i = 0; i < LSPT; ++i) {
+            const int k = sub[i];
+            const double *p = P.poly + k * 14 + IPL1;
+            const double *q = P.om22 + k * 12 + IPL2;
+            const double cpr = fma(fma(fma(fma(p[4], TKD1, p[3]), TKD1, p[2]), TKD1, p[1]), TKD1, p[0]);
+            const double EUKEN = (double)0.115f + (double)0.354f * cpr;
+            const double om = fma(fma(fma(fma(fma(q[5], TKD1, q[4]), TKD1, q[3]), TKD1, q[2]), TKD1, q[1]), TKD1, q[0]);
+            const double SIOME = P.cdia[k] * P.cdia[k] * om;
+            ATC[i] = P.CONVRC * EUKEN * TKRT / P.WMIK[k * LSP + k] / SIOME;
+            AMU[i] = P.CONVRM * TKRT * P.WMIK[k * LSP + k] / SIOME;
+            ATCf[i] = (float)ATC[i];
+            AMUf[i] = (float)AMU[i];
+            Xf[i] = (float)X[i];
+        }
+        double VTC = 0.0, VMU = 0.0;
+        double VDFQ[LSP];
+        for (int i = 0; i < LSPT; ++i) {
+            const int k = sub[i];
+            double PHIK = 0.0, PHDIK = 0.0, EFDIK = 0.0;
+            for (int j = 0; j < LSPT; ++j) {
+                if (j == i) continue;
+                const int kb = sub[j];
+                const int ij = k * LSP + kb;
+                const float w = (float)P.WMIK[ij], dw = (float)P.DWMIK[ij];
+                const float t1 = 1.0f + sqrtf(ATCf[i] / ATCf[j]) * w;
+                const float t2 = 1.0f + sqrtf(AMUf[i] / AMUf[j]) * w;
+                PHIK += (double)(Xf[j] * (t1 * t1) / dw);
+                PHDIK += (double)(Xf[j] * (t2 * t2) / dw);
+                const float CI = (float)ci11_horner(P, i < j ? k * LSP + kb : kb * LSP + k, TKD1);
+                EFDIK += (double)(Xf[j] * CI / ((float)P.WMCD[ij] * TKBP));
+            }
+            VTC = VTC + ATC[i] * X[i] / (X[i] + (double)1.065f * PHIK);
+            VMU = VMU + AMU[i] * X[i] / (X[i] + PHDIK);
+            const double AA = TMOLE - X[i];
+            if (AA <= 1.0e-10) {
+                double d = 0.0;
+                if (i != LSPT - 1) {
+                    const int kl = sub[LSPT - 1];
+                    d = P.WMCD[k * LSP + kl] * (double)TKBP / ci11_horner(P, k * LSP + kl, TKD1);
+                }
+                VDFQ[i] = P.CONVRD * d;
+            } else {
+                VDFQ[i] = P.CONVRD * AA / EFDIK;
+            }
+        }
+        a.vtc[c] = VTC;
+        a.vmu[c] = VMU;
+        int pos = 0;
+        for (int k = 0; k < LSP; ++k) {
+            double v;
+            if (k < LSP - 1 && pos < LSPT - 1 && sub[pos] == k) {
+                v = VDFQ[pos];
+                ++pos;
+            } else {
+                double EFD = 0.0;
+                for (int b = 0; b < LSPT; ++b) {
+                    const int nb = sub[b];
+                    const float CI = (float)ci11_horner(P, k * LSP + nb, TKD1);
+                    EFD += (double)(Xf[b] * CI / ((float)P.WMCD[k * LSP + nb] * TKBP));
+                }
+                v = P.CONVRD * TMOLE / EFD;
+            }
+            a.vdf[k * np + c] = v;
+        }
+    }
+}
+
 // Mixture cp (spgsolv.f:102-173) and h = sum_k Y_k h_k (h_k: solveh.f:39-57).
 struct CpHArgs {
     const DevParams *P;

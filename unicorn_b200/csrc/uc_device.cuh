@@ -52,6 +52,7 @@ struct DevParams {
     double ci11[20];
     double WMIK[LSP * LSP], DWMIK[LSP * LSP], WMCD[LSP * LSP];
     double ETLJ1[LSP * LSP], ETLJ2[LSP * LSP], ETLJ3[LSP * LSP], ETLJ4[LSP * LSP];
+    double RETLJ1[LSP * LSP];             // 1 / ETLJ1 (the mixed form's collision-integral argument)
     // third-body groups 1..10 (TBODY + sum sign*coef*Y/W)
     int16_t tb_off[11], tb_len[11];
     int8_t tb_sp[64], tb_sign[64], tb_hascoef[64];

@@ -229,6 +229,7 @@ static void build_params(const uc_inputs &in, DevParams &P, std::vector<PairTab>
             P.ETLJ2[ij] = P.ETLJ1[ij] * P.ETLJ1[ij];
             P.ETLJ3[ij] = P.ETLJ2[ij] * P.ETLJ1[ij];
             P.ETLJ4[ij] = P.ETLJ3[ij] * P.ETLJ1[ij];
+            P.RETLJ1[ij] = 1.0 / P.ETLJ1[ij];
         }
     for (int g = 0; g < 11; ++g) { P.tb_off[g] = uc_tb_off[g]; P.tb_len[g] = uc_tb_len[g]; }
     const int ntb = (int)(sizeof(uc_tb_sp) / sizeof(uc_tb_sp[0]));
@@ -762,7 +763,7 @@ static int props_impl(uc_ctx *ctx, int precision, double *vmu, double *vtc, doub
     int slot;
     prof_begin(ctx, UC_K_PROPS, slot);
     if (precision == UC_MIXED)
-        props_kernel<float><<<grid, 128, 0, ctx->stream>>>(a);
+        props_mixed_kernel<<<grid, 128, 0, ctx->stream>>>(a);
     else
         props_kernel<double><<<grid, 128, 0, ctx->stream>>>(a);
     prof_end(ctx, slot);
@@ -792,10 +793,10 @@ static int cp_h_impl(uc_ctx *ctx, int precision, double *cp, double *h)
     const int grid = std::min((ctx->n + 255) / 256, ctx->nsm * 8);
     int slot;
     prof_begin(ctx, UC_K_CPH, slot);
-    if (precision == UC_MIXED)
-        cp_h_kernel<float><<<grid, 256, 0, ctx->stream>>>(a);
-    else
-        cp_h_kernel<double><<<grid, 256, 0, ctx->stream>>>(a);
+    // cp and h stay FP64 in the mixed form too: the kernel is bound by reading the 52 Y rows, and h is
+    // a signed sum (formation enthalpies) that FP32 cannot hold to 1e-6 of itself
+    (void)precision;
+    cp_h_kernel<double><<<grid, 256, 0, ctx->stream>>>(a);
     prof_end(ctx, slot);
     CK(cudaGetLastError());
     if (cp || h) {
