@@ -1,9 +1,12 @@
-"""The two FP64 species-update kernels against each other and the oracle: the
-default one with Y in place (update_kernel<double, 14, true>, 14 warps per SM)
-and the two-Y-set one (8 warps per SM, UNICHEM_UPDATE=twoset at uc_init).
+"""The FP64 species-update kernels against each other and the oracle: the
+default tile-resident one (update_tr_kernel: RC blocks on chip across a chunk
+of passes), the per-pass one with Y in place (UNICHEM_UPDATE=inplace,
+update_kernel<double, 14, true>) and the per-pass two-Y-set one
+(UNICHEM_UPDATE=twoset, 8 warps per SM), selected at uc_init.
 Same pass counts, Y within 1e-9 of the oracle (the tolerance of the FP64
 update tests), on the C1 field, a many-tile batch that runs several rounds per
-warp, and frozen transport terms."""
+warp, frozen transport terms, and stopping passes inside and at the end of a
+chunk of the tile-resident kernel."""
 import numpy as np
 import pytest
 
@@ -11,7 +14,8 @@ from test_gpu_parity import assert_rel, c1  # noqa: F401  (c1: the 101x61 CH4 fi
 from unicorn_b200.fields import batch_cells, nondimensional
 
 pytestmark = pytest.mark.gpu
-KINDS = ["inplace", "twoset"]
+KINDS = ["resident", "inplace", "twoset"]
+KIND_ID = {"resident": 0, "inplace": 1, "twoset": 2}
 
 
 @pytest.fixture(scope="module")
@@ -23,10 +27,12 @@ def cuda():
     return unichem
 
 
-def run_update(cuda, monkeypatch, kind, tk, rho, y, **kw):
+def run_update(cuda, monkeypatch, kind, tk, rho, y, chunk=None, **kw):
     monkeypatch.setenv("UNICHEM_UPDATE", kind)
+    if chunk is not None:
+        monkeypatch.setenv("UNICHEM_TR_CHUNK", str(chunk))
     with cuda.UniChem(len(tk)) as u:
-        assert u.stat("update_ip_warps") == (0.0 if kind == "twoset" else 14.0)
+        assert u.stat("update_kind") == KIND_ID[kind]
         u.upload(tk, rho, y)
         u.ckrates()
         passes = u.solvesp(1e-3, **kw)
@@ -52,8 +58,24 @@ def test_inplace_many_rounds_matches_twoset(cuda, oracle, monkeypatch):
     tk, rho = nondimensional(f, oracle.scales, oracle.wm)
     pa, ya, _ = run_update(cuda, monkeypatch, "twoset", tk, rho, f.y, isor=100, relx=0.99, tol=1e-8)
     pb, yb, _ = run_update(cuda, monkeypatch, "inplace", tk, rho, f.y, isor=100, relx=0.99, tol=1e-8)
-    assert pa == pb and pa > 3
+    pc, yc, _ = run_update(cuda, monkeypatch, "resident", tk, rho, f.y, isor=100, relx=0.99, tol=1e-8)
+    assert pa == pb == pc and pa > 3
     assert_rel(yb, ya, 1e-9, 1e-18, "Y in place vs two Y sets")
+    assert_rel(yc, ya, 1e-9, 1e-18, "Y tile-resident vs two Y sets")
+
+
+@pytest.mark.parametrize("chunk", [1, 3, 8, 16])
+def test_resident_chunks_stop_where_the_per_pass_kernel_stops(cuda, oracle, monkeypatch, chunk):
+    """The converging pass falls inside a chunk, at its end or in a later chunk depending on the
+    chunk length; pass count and Y equal those of the per-pass kernel (and, on a C1 slice, the oracle's)."""
+    f = batch_cells(8192, seed=6)
+    tk, rho = nondimensional(f, oracle.scales, oracle.wm)
+    pa, ya, sa = run_update(cuda, monkeypatch, "inplace", tk, rho, f.y, isor=100, relx=0.99, tol=1e-8)
+    pc, yc, sc = run_update(cuda, monkeypatch, "resident", tk, rho, f.y, chunk=chunk, isor=100, relx=0.99, tol=1e-8)
+    assert 3 < pa <= 100 and pc == pa
+    print(f"\nchunk {chunk}: {pc} passes; Y values differing from the per-pass kernel: {(yc != ya).sum()}")
+    assert_rel(yc, ya, 1e-12, 1e-30, "Y tile-resident vs in place")      # the same arithmetic in the same order
+    assert_rel(sc, sa, 1e-12, 1e-30, "soot tile-resident vs in place")
 
 
 @pytest.mark.parametrize("kind", KINDS)

@@ -67,3 +67,20 @@ def test_inplace_program_equals_two_set_program(oracle, harness, isor):
     p2 = harness.harness_update_ip(*args(y2))
     assert p1 == p2 and np.array_equal(y1, y2)
     assert np.abs(y1 - y).max() > 1e-8            # the update moved Y
+
+
+@pytest.mark.parametrize("isor", [1, 3])
+def test_tile_resident_program_equals_two_set_program(oracle, harness, isor):
+    """The tile-resident form (RC rows split between shared and tensor memory, tensor-memory
+    operands loaded into two register banks segment by segment) gives bit for bit what the
+    two-array form gives."""
+    tk, rho, y = random_state(oracle, 300, 23)
+    rc, sour = oracle.rates(tk, rho, y)
+    sour[:] = 0.0
+    P = lambda a: np.ascontiguousarray(a).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    args = lambda yy: (len(tk), P(rho), P(y), P(yy), P(rc), P(sour), P(oracle.wm), ctypes.c_double(1e-3), isor,
+                       ctypes.c_double(0.99), ctypes.c_double(1e-8), ctypes.c_double(len(tk) * 51.0))
+    y1, y2 = np.ascontiguousarray(y.copy()), np.ascontiguousarray(y.copy())
+    p1 = harness.harness_update(*args(y1))
+    p2 = harness.harness_update_tr(*args(y2))
+    assert p1 == p2 and np.array_equal(y1, y2)

@@ -73,3 +73,38 @@ extern "C" int harness_update_ip(int n, const double *rho_a, const double *y0_a,
     }
     return pass;
 }
+
+// The tile-resident form (UC_UPDATE_PROGRAM_TR): the in-place program with its
+// RC operands split between "shared-memory rows" and "tensor-memory rows"
+// loaded into two register banks segment by segment; here both stores are
+// host arrays holding the cell's RC values in the program's row order.
+#include "../unicorn_b200/csrc/generated/update_program_tr.cuh"
+extern "C" int harness_update_tr(int n, const double *rho_a, const double *y0_a, double *y_a,
+                                 const double *rc_a, const double *sour_a, const double *wm,
+                                 double dt, int isor, double relx, double tol, double spnorm)
+{
+    const double sor1 = relx, sor2 = 1.0 - relx;
+    double y[LSP], y0[LSP], sour[6], ysh[UC_IP_NSHADOW], srows[UC_TR_NS], trows[UC_TR_NT], bank[2][UC_TR_SEG];
+    int pass;
+    for (pass = 1; pass <= isor; ++pass) {
+        double rsd = 0.0;
+        for (int c = 0; c < n; ++c) {
+            for (int k = 0; k < LSP; ++k) { y[k] = y_a[k * n + c]; y0[k] = y0_a[k * n + c]; }
+            for (int m = 0; m < 6; ++m) sour[m] = sour_a[m * n + c];
+            for (int i = 0; i < UC_TR_NS; ++i) srows[i] = rc_a[uc_tr_srow[i] * n + c];
+            for (int i = 0; i < UC_TR_NT; ++i) trows[i] = rc_a[uc_tr_trow[i] * n + c];
+            const double rho = rho_a[c];
+#undef YOS
+#define YOS(m) ysh[m]
+#define RCS(i) srows[i]
+#define TM_LD(b, q, col) bank[b][q] = trows[(col) / 2]
+#define TM_WAIT(b) do { } while (0)
+#define RCT(b, q) bank[b][q]
+            UC_TR_SHADOW_SAVE();
+            UC_UPDATE_PROGRAM_TR();
+            for (int k = 0; k < LSP - 1; ++k) y_a[k * n + c] = y[k];
+        }
+        if (rsd / spnorm <= tol) break;
+    }
+    return pass;
+}

@@ -38,7 +38,8 @@ def sources() -> list[Path]:
 
 def regenerate():
     from unicorn_b200.mech import codegen
-    gen = [CSRC / "generated" / "mech_tables.h", CSRC / "generated" / "update_program.cuh"]
+    gen = [CSRC / "generated" / "mech_tables.h", CSRC / "generated" / "update_program.cuh",
+           CSRC / "generated" / "update_program_tr.cuh"]
     src = [codegen.MECH, Path(codegen.__file__)]
     if any(not g.exists() for g in gen) or max(s.stat().st_mtime for s in src) > min(g.stat().st_mtime for g in gen):
         codegen.main()

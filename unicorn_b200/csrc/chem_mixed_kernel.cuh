@@ -37,6 +37,7 @@ struct ChemMArgs {
     const PairTabM *tab;
     const double *tk, *rho, *y, *stmf, *stnd;
     float *rc32;                 // [544][npad] or null
+    double *rc64;                // [544][npad] or null: the same values stored as doubles
     int *tile_flag;              // [ntile]: 1 if a rate of the tile leaves the FP32 range
     double *sour;                // [6][npad] or null
     double *qdsp, *qdot, *dwdy;  // outputs (any may be null)
@@ -257,6 +258,8 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_mixed_kernel(const ChemM
         // ---------------- phase 3: RC out (FP32), species sums
         if (a.rc32)
             for (int r = warp; r < LRX; r += CHEM_WARPS) a.rc32[(size_t)r * a.npad + cell] = sRC[r * TILE + lane];
+        if (a.rc64)
+            for (int r = warp; r < LRX; r += CHEM_WARPS) a.rc64[(size_t)r * a.npad + cell] = (double)sRC[r * TILE + lane];
         {
             const float TKD = (float)sC[SM_TKD * TILE + lane];
             const float TKD2 = TKD * TKD, TKD3 = TKD * TKD2, TKD4 = TKD * TKD3, TKD5 = TKD * TKD4;

@@ -14,6 +14,7 @@
 #include "chem_mixed_kernel.cuh"
 #include "props_kernel.cuh"
 #include "update_kernel.cuh"
+#include "update_tr_kernel.cuh"
 #include "integrate_kernel.cuh"
 #include "faces_kernel.cuh"
 #include "fdetail_kernel.cuh"
@@ -64,6 +65,10 @@ struct uc_ctx {
     bool have_fields = false, have_rc = false;
     int upd_grid = 0;
     int upd_ip = 0, ip_grid = 0;       // FP64 update with Y in place: warps per CTA (0: two Y sets, 8 warps)
+    int upd_kind = 0;                  // 0: tile-resident (default), 1: Y in place per pass, 2: two Y sets per pass
+    int tr_chunk = 8;                  // tile-resident update: passes per chunk
+    double *tr_snap = nullptr, *tr_partial = nullptr;
+    size_t tr_snap_cap = 0;
     // species-equation faces assembled on the device (grid, flow, coefficients)
     int lj = 0, li = 0, isym = 0;
     double sigsp = 0.0;
@@ -339,7 +344,7 @@ static void free_ctx(uc_ctx *c)
     if (!c) return;
     double **bufs[] = {&c->tk, &c->rho, &c->y, &c->y0, &c->soot, &c->soot0, &c->rc, &c->sour, &c->qdsp,
                        &c->qdot, &c->dwdy, &c->vmu, &c->vtc, &c->vdf, &c->cp, &c->h, &c->face_sum,
-                       &c->face_nbr, &c->ht, &c->partial};
+                       &c->face_nbr, &c->ht, &c->partial, &c->tr_snap, &c->tr_partial};
     for (auto b : bufs)
         if (*b) { cudaFree(*b); *b = nullptr; }
     if (c->dP) cudaFree(c->dP);
@@ -524,8 +529,21 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
         if (per_sm < 1) per_sm = 1;
         ctx->upd_grid = std::min(per_sm * ctx->nsm, std::max(1, (ctx->ntile + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32)));
         if ((rc = dalloc(ctx, &ctx->partial, 2 * (size_t)per_sm * ctx->nsm))) break;
-        ctx->upd_ip = UPD_IP_WARPS;        // UNICHEM_UPDATE=twoset selects the two-Y-set kernel instead
-        if (const char *k = getenv("UNICHEM_UPDATE")) if (!strcmp(k, "twoset")) ctx->upd_ip = 0;
+        // the update kernel: the tile-resident form unless UNICHEM_UPDATE names a per-pass one
+        ctx->upd_ip = UPD_IP_WARPS;
+        ctx->upd_kind = 0;
+        if (const char *k = getenv("UNICHEM_UPDATE")) {
+            if (!strcmp(k, "twoset")) { ctx->upd_ip = 0; ctx->upd_kind = 2; }
+            else if (!strcmp(k, "inplace")) ctx->upd_kind = 1;
+        }
+        if (const char *k = getenv("UNICHEM_TR_CHUNK")) ctx->tr_chunk = std::max(1, std::min(TR_CHUNK_MAX, atoi(k)));
+        if (ctx->upd_kind == 0) {
+            e = cudaFuncSetAttribute(update_tr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM);
+            if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "smem attribute: %s", cudaGetErrorString(e)); break; }
+            int tr_per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tr_per_sm, update_tr_kernel, TR_WARPS * 32, TR_SMEM);
+            if (tr_per_sm < 1) { rc = set_err(ctx, UC_E_CUDA, "the tile-resident update does not fit an SM"); break; }
+        }
         if (ctx->upd_ip) {
             const void *fn, *fnm; size_t sm;
             ip_kernel(true, &fnm, &sm);
@@ -634,7 +652,7 @@ extern "C" int uc_download_fields(uc_ctx *ctx, double *tk, double *rho, double *
 static int launch_chem(uc_ctx *ctx, int precision, bool want_rc, bool want_omega)
 {
     if (precision != UC_FP64 && precision != UC_MIXED) return set_err(ctx, UC_E_ARG, "unknown precision %d", precision);
-    if (precision == UC_MIXED && want_rc && !ctx->rc32) {
+    if (precision == UC_MIXED && want_rc && ctx->upd_kind != 0 && !ctx->rc32) {
         cudaError_t e = cudaMalloc((void **)&ctx->rc32, (size_t)LRX * ctx->npad * sizeof(float));
         if (e != cudaSuccess) { ctx->rc32 = nullptr; return set_err(ctx, UC_E_NOMEM, "FP32 RC plane: %s", cudaGetErrorString(e)); }
     }
@@ -654,7 +672,9 @@ static int launch_chem(uc_ctx *ctx, int precision, bool want_rc, bool want_omega
         ChemMArgs m{};
         m.P = ctx->dP; m.tab = ctx->dTabM;
         m.tk = ctx->tk; m.rho = ctx->rho; m.y = ctx->y; m.stmf = ctx->soot; m.stnd = ctx->soot + ctx->npad;
-        m.rc32 = want_rc ? ctx->rc32 : nullptr;
+        // the tile-resident update reads an FP64 plane: the FP32 rates are stored as doubles
+        m.rc32 = want_rc && ctx->upd_kind != 0 ? ctx->rc32 : nullptr;
+        m.rc64 = want_rc && ctx->upd_kind == 0 ? ctx->rc : nullptr;
         m.sour = ctx->sour;
         m.qdsp = want_omega ? ctx->qdsp : nullptr;
         m.qdot = want_omega ? ctx->qdot : nullptr;
@@ -682,7 +702,7 @@ static int launch_chem(uc_ctx *ctx, int precision, bool want_rc, bool want_omega
         chem_fp64_kernel<<<std::min(ctx->ntile, ctx->nsm), CHEM_THREADS, CHEM_SMEM, ctx->stream>>>(f);
         prof_end(ctx, slot);
         CK(cudaGetLastError());
-        if (want_rc) ctx->rc_prec = UC_MIXED;
+        if (want_rc) ctx->rc_prec = ctx->upd_kind == 0 ? UC_FP64 : UC_MIXED;   // the type of the plane
         return UC_OK;
     }
     ChemArgs a{};
@@ -714,7 +734,7 @@ extern "C" int uc_rates(uc_ctx *ctx, int precision, double *rc)
     RET_IF(launch_chem(ctx, precision, true, false));
     ctx->have_rc = true;
     ctx->rc_start = false;
-    if (rc && precision == UC_FP64) {
+    if (rc && ctx->rc_prec == UC_FP64) {
         RET_IF(download_rows(ctx, rc, ctx->rc, LRX));
         CK(cudaStreamSynchronize(ctx->stream));
         RET_IF(check_status(ctx));
@@ -868,6 +888,32 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
     a.isor = isor; a.n = ctx->n; a.npad = ctx->npad; a.ntile = ctx->ntile;
     void *args[] = {&a};
     int slot;
+    if (ctx->upd_kind == 0 && ctx->rc_prec == UC_FP64) {
+        const int C = std::min(ctx->tr_chunk, isor);
+        const size_t need = (size_t)std::max(1, C - 1) * TR_SNAP_ROWS * ctx->npad;
+        if (ctx->tr_snap_cap < need) {
+            if (ctx->tr_snap) cudaFree(ctx->tr_snap);
+            ctx->tr_snap = nullptr;
+            ctx->tr_snap_cap = 0;
+            RET_IF(dalloc(ctx, &ctx->tr_snap, need));
+            ctx->tr_snap_cap = need;
+        }
+        RET_IF(dalloc(ctx, &ctx->tr_partial, 2 * (size_t)TR_CHUNK_MAX * ctx->nsm));
+        TrArgs t{ctx->tr_snap, ctx->tr_partial, C, ctx->status};
+        void *targs[] = {&a, &t};
+        prof_begin(ctx, UC_K_UPDATE, slot);
+        CK(cudaLaunchCooperativeKernel((const void *)update_tr_kernel, dim3(ctx->nsm), dim3(TR_WARPS * 32), targs,
+                                       TR_SMEM, ctx->stream));
+        prof_end(ctx, slot);
+        if (passes) {
+            CK(cudaMemcpyAsync(passes, ctx->passes, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            RET_IF(check_status(ctx));
+        }
+        ctx->have_rc = false;
+        ctx->rc_start = true;
+        return UC_OK;
+    }
     prof_begin(ctx, UC_K_UPDATE, slot);
     if (ctx->upd_ip) {
         const void *fn; size_t sm;
@@ -969,6 +1015,8 @@ extern "C" int uc_stat(uc_ctx *ctx, const char *name, double *value)
     if (!strcmp(name, "tiles")) { *value = ctx->ntile; return UC_OK; }
     if (!strcmp(name, "int_warps")) { *value = ctx->int_warps; return UC_OK; }
     if (!strcmp(name, "update_ip_warps")) { *value = ctx->upd_ip; return UC_OK; }
+    if (!strcmp(name, "update_kind")) { *value = ctx->upd_kind; return UC_OK; }
+    if (!strcmp(name, "update_chunk")) { *value = ctx->tr_chunk; return UC_OK; }
     if (!strcmp(name, "int_sorted")) { *value = ctx->int_sorted; return UC_OK; }
     if (!strcmp(name, "int_tune_best_ms")) { *value = ctx->tune_best; return UC_OK; }
     if (!strcmp(name, "int_tune_worst_ms")) { *value = ctx->tune_worst; return UC_OK; }

@@ -266,6 +266,117 @@ def gen_inplace_program(blocks, uses: dict) -> str:
     L.append("#ifdef __CUDACC__")
     L.append(f"static __constant__ int8_t uc_ip_shadow[{max(1, len(ctx.shadow))}] = UC_IP_SHADOW_LIST;")
     L.append("#endif")
+    gen_inplace_program.shadow = list(ctx.shadow)
+    return "\n".join(L) + "\n"
+
+
+# ------------------------------------------------------------------ tile-resident form
+
+TR_NTMEM, TR_SEG = 256, 12
+
+
+class _TRCtx(_InPlaceCtx):
+    """Emission context of the tile-resident program: RC(r) becomes a token
+    that is later bound to a shared-memory row or a tensor-memory register."""
+
+    def rc(self, r0: int) -> str:
+        return f"@{r0}@"
+
+
+def gen_tr_program(blocks, uses: dict, shadow: list[int]) -> str:
+    """The in-place program for a tile whose RC block lives on chip: the RC rows
+    used least often (TR_NTMEM of them) in tensor memory, two 32-bit columns
+    each, the others in shared memory. Tensor-memory operands are loaded into
+    registers ahead of use in segments of at most TR_SEG values, alternating
+    between two register banks: the loads of segment s+1 are issued before the
+    statements of segment s run and waited for after them, so their latency is
+    hidden behind segment s. The arithmetic, its operands and their order are
+    those of the in-place program."""
+    import re
+    ctx = _TRCtx(uses)
+    body = []
+    for b in blocks:
+        k = b["species"]
+        if b["prod"] is not None:
+            body += emit_sum(b["prod"], ctx, "prod")
+        body += emit_sum(b["extra"], ctx, "extra")
+        body.append(f"rhs1 = rho * Y0({k}) + dt * WM({k}) * (prod + extra);")
+        if b["loss"] is None:
+            body.append("rhs2 = 0.0;")
+        else:
+            body += emit_sum(b["loss"], ctx, "loss")
+            body.append(f"rhs2 = -(dt * WM({k}) * loss);")
+        body.append(f"ppp = rho - FACE_SUM({k});")
+        body.append(f"fnew = sor2 * YO({k}) + (rhs1 - FACE_NBR({k})) * sor1 / (ppp - rhs2);")
+        body.append(f"rsd += fabs(YO({k}) - fnew);")
+        body.append(f"UC_UPDATE_TAIL({k});")
+        ctx.updated.add(k)
+    assert ctx.shadow == shadow, "the tile-resident and in-place programs must shadow the same species"
+    tok = re.compile(r"@(\d+)@")
+    rows = sorted(uses, key=lambda r: (uses[r], r))
+    trow = sorted(rows[:TR_NTMEM])
+    srow = sorted(rows[TR_NTMEM:])
+    tcol = {r: i for i, r in enumerate(trow)}
+    scol = {r: i for i, r in enumerate(srow)}
+    # segments: runs of statements with at most TR_SEG distinct tensor-memory rows
+    segs = []          # (statements, tensor-memory rows in first-use order)
+    cur, cur_rows = [], []
+    for st in body:
+        need = [int(x) for x in tok.findall(st) if int(x) in tcol]
+        new = [r for r in dict.fromkeys(need) if r not in cur_rows]
+        if cur and len(cur_rows) + len(new) > TR_SEG:
+            segs.append((cur, cur_rows))
+            cur, cur_rows = [], []
+            new = list(dict.fromkeys(need))
+        cur.append(st)
+        cur_rows += new
+    segs.append((cur, cur_rows))
+    out = []
+
+    def loads(si):
+        bank = si % 2
+        return [f"TM_LD({bank}, {q}, {2 * tcol[r]});" for q, r in enumerate(segs[si][1])]
+
+    out += loads(0)
+    out.append("TM_WAIT(0);")
+    for si, (stmts, trs) in enumerate(segs):
+        bank = si % 2
+        slot = {r: q for q, r in enumerate(trs)}
+        if si + 1 < len(segs):
+            out += loads(si + 1)
+
+        def bind(m, slot=slot, bank=bank):
+            r = int(m.group(1))
+            return f"RCT({bank}, {slot[r]})" if r in tcol else f"RCS({scol[r]})"
+        out += [tok.sub(bind, st) for st in stmts]
+        if si + 1 < len(segs):
+            out.append(f"TM_WAIT({(si + 1) % 2});")
+    nld = sum(len(t) for _, t in segs)
+    L = ["// Generated by unicorn_b200/mech/codegen.py: the in-place species-update program",
+         "// (src/lib/solvesp.f:85-2806) for a tile whose RC block is held on chip.",
+         f"// RC rows: {len(trow)} in tensor memory (row i in columns 2i, 2i+1: low and high",
+         f"// word), {len(srow)} in shared memory. Requires RCS(i) (shared-memory row i of the",
+         "// cell), TM_LD(bank, q, col) (load the double at column col into slot q of a",
+         "// register bank), TM_WAIT(bank) (wait for the loads of that bank), RCT(bank, q),",
+         "// and the accessors of the in-place program (YO, YN, YOS, Y0, SOUR, WM, FACE_SUM,",
+         "// FACE_NBR, UC_UPDATE_TAIL; scalars rho, dt, sor1, sor2, rsd).",
+         f"// {len(segs)} segments and {nld} tensor-memory loads per cell and pass.",
+         "#pragma once",
+         f"#define UC_TR_NT {len(trow)}",
+         f"#define UC_TR_NS {len(srow)}",
+         f"#define UC_TR_SEG {TR_SEG}",
+         "#define UC_TR_SHADOW_SAVE() do { " + " ".join(f"YOS({m}) = YO({k});" for m, k in enumerate(shadow)) + " } while (0)",
+         "#define UC_UPDATE_PROGRAM_TR() do { \\",
+         "    double prod = 0.0, extra, loss, rhs1, rhs2, ppp, fnew; \\"]
+    L.extend("    " + x + " \\" for x in out)
+    L.append("} while (0)")
+    L.append("#ifdef __CUDACC__")
+    L.append(f"static __constant__ int16_t uc_tr_trow[{len(trow)}] = {{{', '.join(map(str, trow))}}};")
+    L.append(f"static __constant__ int16_t uc_tr_srow[{len(srow)}] = {{{', '.join(map(str, srow))}}};")
+    L.append("#else")
+    L.append(f"static const short uc_tr_trow[{len(trow)}] = {{{', '.join(map(str, trow))}}};")
+    L.append(f"static const short uc_tr_srow[{len(srow)}] = {{{', '.join(map(str, srow))}}};")
+    L.append("#endif")
     return "\n".join(L) + "\n"
 
 
@@ -415,7 +526,16 @@ def main():
     GEN.mkdir(parents=True, exist_ok=True)
     (GEN / "mech_tables.h").write_text(gen_tables(mech))
     (GEN / "update_program.cuh").write_text(gen_update_program(mech))
-    print(f"wrote {GEN / 'mech_tables.h'} and {GEN / 'update_program.cuh'}")
+    blocks = resolve_update(mech)
+    uses: dict[int, int] = {}
+    for b in blocks:
+        for key in ("prod", "extra", "loss"):
+            for _, t in (b[key] or []):
+                for leaf in leaves(t, []):
+                    if leaf.kind == "RC":
+                        uses[leaf.idx] = uses.get(leaf.idx, 0) + 1
+    (GEN / "update_program_tr.cuh").write_text(gen_tr_program(blocks, uses, gen_inplace_program.shadow))
+    print(f"wrote {GEN / 'mech_tables.h'}, {GEN / 'update_program.cuh'} and {GEN / 'update_program_tr.cuh'}")
 
 
 if __name__ == "__main__":
