@@ -87,6 +87,20 @@ int uc_upload_fields(uc_ctx *ctx, const double *tk, const double *rho, const dou
 int uc_upload_fields_device(uc_ctx *ctx, const double *tk, const double *rho, const double *fsp,
                             const double *stmf, const double *stnd, int ld);
 
+/* The reference's skip flags ISKIP(LJ,LI) [n] (src/lib/skipdf.f: 3 marks
+ * injection cells, 10 and above body cells); NULL clears them. As the
+ * reference does, cells with ISKIP >= 3 keep their RC and SOUR in the rate
+ * calls (ckrates.f:94), keep Y and stay out of the residual and the N2
+ * closure in the species update (solvesp.f:89,2842), and keep T in
+ * uc_temperature_from_h (solveh.f:1173); cells with ISKIP >= 10 also keep
+ * omega, QDOT and d(omega)/dY (solveh.f:119), while those below 10 take them
+ * from the RC they kept. Planes never computed start at zero, like the
+ * reference's COMMON blocks. The transport properties are computed for every
+ * cell (the property block has no skip test); the batched integration, the
+ * face assembly and the enthalpy equation do not read ISKIP.
+ * Replaces: ISKIP of COMMON /CB01/ as CKRATES, SOLVESP and SOLVEH read it. */
+int uc_set_iskip(uc_ctx *ctx, const int *iskip);
+
 /* Copy the device-resident state back (any pointer may be NULL). */
 int uc_download_fields(uc_ctx *ctx, double *tk, double *rho, double *fsp, double *stmf,
                        double *stnd);

@@ -328,6 +328,54 @@ class Oracle:
         del keep
         return y, s, passes
 
+    # ---------------------------------------------------------------- ISKIP
+    # The reference skips cells with ISKIP >= 3 in CKRATES (ckrates.f:94), SOLVESP (solvesp.f:89,2842)
+    # and the T Newton (solveh.f:1173), and cells with ISKIP >= 10 in SOLVEH's rates (solveh.f:119).
+    # A skipped cell keeps what its arrays hold; in a fresh run that is zero (the COMMON blocks), and
+    # a cell with 3 <= ISKIP < 10 gets its omega from that zero RC, i.e. zero. The per-cell routines
+    # above are unchanged; these wrappers apply the skips around them.
+    @staticmethod
+    def _skipped(iskip, level):
+        return np.asarray(iskip) >= level
+
+    def rates_iskip(self, tk, rho, y, iskip, stmf=None, stnd=None):
+        rc, sour = self.rates(tk, rho, y, stmf, stnd)
+        s = self._skipped(iskip, 3)
+        rc[:, s] = 0.0
+        sour[:, s] = 0.0
+        return rc, sour
+
+    def omega_iskip(self, tk, rho, y, iskip, stmf=None, stnd=None):
+        q, qd, h, d = self.omega(tk, rho, y, stmf, stnd)
+        s = self._skipped(iskip, 3)
+        q[:, s] = 0.0
+        qd[s] = 0.0
+        d[:, s] = 0.0
+        return q, qd, h, d
+
+    def species_update_iskip(self, rho, y0, rc, sour, dt, iskip, **kw):
+        """The update of the cells with ISKIP < 3 (in their order, the residual over them only, the
+        spnorm of the whole field); skipped cells keep Y and soot."""
+        n = y0.shape[1]
+        act = ~self._skipped(iskip, 3)
+        kw.setdefault("spnorm", float(n * (LSP - 1)))
+        sub = lambda a: None if a is None else np.ascontiguousarray(a[..., act])
+        y_start = kw.pop("y_start", None)
+        soot0 = kw.pop("soot0", None)
+        ya, sa, passes = self.species_update(rho[act], sub(y0), sub(rc), sub(sour), dt, y_start=sub(y_start),
+                                             soot0=sub(soot0), **kw)
+        y = np.array(y0 if y_start is None else y_start, dtype=np.float64, copy=True)
+        soot = np.zeros((2, n)) if soot0 is None else np.array(soot0, dtype=np.float64, copy=True)
+        y[:, act] = ya
+        soot[:, act] = sa
+        return y, soot, passes
+
+    def temperature_iskip(self, tk_guess, y, ht, iskip):
+        t = self.temperature(tk_guess, y, ht)
+        s = self._skipped(iskip, 3)
+        t[s] = np.asarray(tk_guess)[s]
+        return t
+
     def nsub(self, rho, y, qdsp, dt, c_tau=1.0, y_tau=1e-3, nsub_max=200):
         """Per-cell sub-step counts of the batched integration and the ratio x they come from."""
         n = len(rho)

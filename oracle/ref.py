@@ -132,7 +132,7 @@ class RefUnicorn:
         i = 1 + c // self.nj
         return j, i
 
-    def _load(self, tk, rho, y, stmf, stnd):
+    def _load(self, tk, rho, y, stmf, stnd, iskip=None):
         n = len(tk)
         M = "UNICORN"
         TK = self.var(M, "TK").reshape(self.LJ, self.LI, order="F")
@@ -154,6 +154,12 @@ class RefUnicorn:
         FSP[j, i, :] = y.T
         STMF[j, i] = stmf
         STND[j, i] = stnd
+        if iskip is not None:
+            # ISKIP of /CB01/ (lib/skipdf.f); the arrays a skipped cell keeps start at zero, as the
+            # COMMON blocks do in a fresh run
+            ISKIP.reshape(self.LJ, self.LI, order="F")[j, i] = iskip
+            for unit, nm in (("SOLVESP", "RC"), ("CKRATES", "SOUR"), ("SOLVEH", "QDSP"), ("SOLVEH", "QDOT")):
+                self.var(unit, nm)[:] = 0.0
         return j, i
 
     def _chunks(self, n):
@@ -165,14 +171,16 @@ class RefUnicorn:
         return (np.zeros(n) if stmf is None else np.asarray(stmf, float),
                 np.zeros(n) if stnd is None else np.asarray(stnd, float))
 
-    def ckrates(self, tk, rho, y, stmf=None, stnd=None):
-        """CKRATES (lib/ckrates.f:1-1363): returns RC[544,n] and SOUR[6,n]."""
+    def ckrates(self, tk, rho, y, stmf=None, stnd=None, iskip=None):
+        """CKRATES (lib/ckrates.f:1-1363): returns RC[544,n] and SOUR[6,n]. With iskip, cells
+        with ISKIP >= 3 keep the zero RC and SOUR of a fresh run (ckrates.f:94)."""
         n = len(tk)
         stmf, stnd = self._soot(n, stmf, stnd)
         rc = np.empty((LRX, n))
         sour = np.empty((6, n))
         for a, b in self._chunks(n):
-            j, i = self._load(tk[a:b], rho[a:b], y[:, a:b], stmf[a:b], stnd[a:b])
+            j, i = self._load(tk[a:b], rho[a:b], y[:, a:b], stmf[a:b], stnd[a:b],
+                              None if iskip is None else iskip[a:b])
             self.lib.f77_ckrates()
             RC = self.var("SOLVESP", "RC")
             SOUR = self.var("CKRATES", "SOUR")
@@ -180,7 +188,7 @@ class RefUnicorn:
             sour[:, a:b] = SOUR[j, i, :].T
         return rc, sour
 
-    def omega(self, tk, rho, y, stmf=None, stnd=None):
+    def omega(self, tk, rho, y, stmf=None, stnd=None, iskip=None):
         """CKRATES then SOLVEH's rate part (lib/solveh.f:34-57,116-1145).
 
         Returns QDSP[52,n] (the reference's per-species rate, = -omega),
@@ -191,7 +199,8 @@ class RefUnicorn:
         qdot = np.empty(n)
         henth = np.empty((LSP, n))
         for a, b in self._chunks(n):
-            j, i = self._load(tk[a:b], rho[a:b], y[:, a:b], stmf[a:b], stnd[a:b])
+            j, i = self._load(tk[a:b], rho[a:b], y[:, a:b], stmf[a:b], stnd[a:b],
+                              None if iskip is None else iskip[a:b])
             self.lib.f77_ckrates()
             SSP = self.var("SOLVEH", "SSP").reshape(self.LJ, self.LI, LSP, order="F")
             FSP = self.var("UNICORN", "FSP").reshape(self.LJ, self.LI, LSP, order="F")
@@ -240,7 +249,7 @@ class RefUnicorn:
         return yc, vmu, vtc, vdf
 
     def species_update(self, tk, rho, y0, dt, isor=100, relx=0.99, tol=1e-8, y_start=None,
-                       stmf=None, stnd=None, spnorm=None):
+                       stmf=None, stnd=None, spnorm=None, iskip=None):
         """CKRATES then SOLVESP (lib/solvesp.f) with zero face coefficients.
 
         One chunk only (the pass count is a property of the whole field).
@@ -250,7 +259,7 @@ class RefUnicorn:
             raise ValueError(f"species_update handles at most {self.chunk} cells per call")
         stmf, stnd = self._soot(n, stmf, stnd)
         self.set_dt(dt)
-        j, i = self._load(tk, rho, y0, stmf, stnd)
+        j, i = self._load(tk, rho, y0, stmf, stnd, iskip)
         self.lib.f77_ckrates()
         for blk in ("DUMMY", "DUM0", "DUMX"):
             self._block(blk)[:] = 0

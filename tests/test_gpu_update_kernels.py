@@ -67,12 +67,17 @@ def test_inplace_many_rounds_matches_twoset(cuda, oracle, monkeypatch):
 @pytest.mark.parametrize("chunk", [1, 3, 8, 16])
 def test_resident_chunks_stop_where_the_per_pass_kernel_stops(cuda, oracle, monkeypatch, chunk):
     """The converging pass falls inside a chunk, at its end or in a later chunk depending on the
-    chunk length; pass count and Y equal those of the per-pass kernel (and, on a C1 slice, the oracle's)."""
-    f = batch_cells(8192, seed=6)
+    chunk length; pass count and Y equal those of the per-pass kernel."""
+    f = batch_cells(65536, seed=5)
     tk, rho = nondimensional(f, oracle.scales, oracle.wm)
-    pa, ya, sa = run_update(cuda, monkeypatch, "inplace", tk, rho, f.y, isor=100, relx=0.99, tol=1e-8)
-    pc, yc, sc = run_update(cuda, monkeypatch, "resident", tk, rho, f.y, chunk=chunk, isor=100, relx=0.99, tol=1e-8)
-    assert 3 < pa <= 100 and pc == pa
+    # the loosest tolerance of a decade ladder at which the per-pass kernel stops after a few passes
+    for tol in (1e-2, 1e-3, 1e-4, 1e-5, 1e-6, 1e-7):
+        pa, ya, sa = run_update(cuda, monkeypatch, "inplace", tk, rho, f.y, isor=100, relx=0.99, tol=tol)
+        if 5 <= pa <= 60:
+            break
+    pc, yc, sc = run_update(cuda, monkeypatch, "resident", tk, rho, f.y, chunk=chunk, isor=100, relx=0.99, tol=tol)
+    assert 5 <= pa <= 60, pa
+    assert pc == pa
     print(f"\nchunk {chunk}: {pc} passes; Y values differing from the per-pass kernel: {(yc != ya).sum()}")
     assert_rel(yc, ya, 1e-12, 1e-30, "Y tile-resident vs in place")      # the same arithmetic in the same order
     assert_rel(sc, sa, 1e-12, 1e-30, "soot tile-resident vs in place")

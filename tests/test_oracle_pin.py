@@ -69,3 +69,35 @@ def test_temperature_bitwise(oracle, ref):
     t_o = oracle.temperature(guess, y, ht)
     assert np.array_equal(t_r, t_o)
     assert np.abs(t_o * oracle.scales["TSTR"] - T).max() < 2e-3
+
+
+@pytest.mark.parametrize("isor,tol", [(3, 0.0), (100, 1e-8)])
+def test_iskip_bitwise(oracle, ref, isor, tol):
+    """ISKIP (lib/skipdf.f: 3 injection cells, 10 and 11 body cells; 1 and 2 skip nothing here) in
+    CKRATES (ckrates.f:94), SOLVEH's rates (solveh.f:119) and SOLVESP (solvesp.f:89,2842), starting
+    from the zero arrays of a fresh run: the oracle's wrappers give the translated reference's
+    results bit for bit, and skipped cells keep their state."""
+    f = jet_field(40, 50, fuel=11, t_peak=2300.0, seed=3)      # 2000 cells: one reference chunk
+    tk, rho = nondimensional(f, oracle.scales, oracle.wm)
+    y = f.y
+    iskip = np.zeros(f.n, dtype=np.int32)
+    iskip[100:180] = 3
+    iskip[500:520] = 10
+    iskip[900:905] = 11
+    iskip[1200:1210] = 1
+    iskip[1300:1310] = 2
+    rc_r, s_r = ref.ckrates(tk, rho, y, iskip=iskip)
+    rc_o, s_o = oracle.rates_iskip(tk, rho, y, iskip)
+    assert np.array_equal(rc_r, rc_o) and np.array_equal(s_r, s_o)
+    assert not rc_o[:, 100:180].any() and rc_o[:, 1200:1210].any()
+    q_r, qd_r, _ = ref.omega(tk, rho, y, iskip=iskip)
+    q_o, qd_o, _, _ = oracle.omega_iskip(tk, rho, y, iskip)
+    assert np.array_equal(q_r, q_o) and np.array_equal(qd_r, qd_o)
+    yr, s1, s2, pr = ref.species_update(tk, rho, y, 1e-3, isor=isor, relx=0.99, tol=tol, iskip=iskip)
+    yo, so, po = oracle.species_update_iskip(rho, y, rc_o, s_o, 1e-3, iskip, isor=isor, tol=tol,
+                                             spnorm=float(ref.LE * 51))
+    assert pr == po
+    assert np.array_equal(yr, yo)
+    assert np.array_equal(s1, so[0]) and np.array_equal(s2, so[1])
+    skipped = iskip >= 3
+    assert np.array_equal(yo[:, skipped], y[:, skipped])

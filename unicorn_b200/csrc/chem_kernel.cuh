@@ -34,6 +34,11 @@ struct ChemArgs {
     int *status;
     const int *tile_list;        // optional: only these tiles ([*tile_count] entries)
     const int *tile_count;
+    // optional ISKIP class per cell (0: computed; 1: 3 <= ISKIP < 10; 2: ISKIP >= 10). Classes 1 and 2
+    // keep their RC and SOUR (ckrates.f:94); class 2 keeps its omega, QDOT and d(omega)/dY too
+    // (solveh.f:119), class 1 takes them from its kept RC (rc_stale, zero when null).
+    const int8_t *skip;
+    const double *rc_stale;
 };
 
 constexpr size_t CHEM_SMEM = PAIRTAB_BYTES + sizeof(double) * (size_t)(LRX * TILE + 2 * LSP * TILE + SC_N * TILE) + 64;
@@ -58,7 +63,8 @@ __device__ __forceinline__ double gibbs_exp(const double *a, double ELOGT, doubl
 template <int NW>
 __device__ __forceinline__ void tile_rates_fp64(const DevParams &P, const PairTab *sTab, double *sRC,
                                                 const double *sY, double *sG, double *sC, double *sour,
-                                                size_t sstride, size_t soff, int lane, int warp)
+                                                size_t sstride, size_t soff, int lane, int warp,
+                                                bool keep_sour = false)
 {
     const double C1ST = P.C1ST, C2ND = P.C2ND, C3RD = P.C3RD;
     // ---------------- phase 1a: Gibbs functions; Y/W rows (scratch in sRC)
@@ -92,8 +98,8 @@ __device__ __forceinline__ void tile_rates_fp64(const DevParams &P, const PairTa
                 acc = P.tb_sign[o + t] > 0 ? acc + term : acc - term;
             }
             sC[(SC_TB0 + g) * TILE + lane] = acc;
-        } else if (sour) {
-            // ckrates.f:1337-1352
+        } else if (sour && !keep_sour) {
+            // ckrates.f:1337-1352 (skipped cells, ISKIP >= 3, keep theirs: ckrates.f:94)
             const double PI = 3.1415927e+00, RSOOT = 1.9000e+03, SIGB = 1.38e-23, AVNO = 6.0232e+23;
             const double CMIN = (double)100.0f, CAGL = (double)9.0f;
             const double TKD = sC[SC_TKD * TILE + lane], rho = sC[SC_RHO * TILE + lane];
@@ -222,6 +228,8 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_fp64_kernel(const ChemAr
         const int tile = a.tile_list ? a.tile_list[w] : w;
         const size_t c0 = (size_t)tile * TILE;
         const size_t cell = c0 + lane;
+        const int cls = a.skip ? a.skip[cell] : 0;
+        const bool tile_skips = a.skip && __syncthreads_or(cls != 0);
         // ---------------- phase 0: load
         for (int k = warp; k < LSP; k += CHEM_WARPS) sY[k * TILE + lane] = a.y[(size_t)k * a.npad + cell];
         if (warp == CHEM_WARPS - 1) {
@@ -238,11 +246,19 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_fp64_kernel(const ChemAr
             sC[SC_STND * TILE + lane] = a.stnd ? a.stnd[cell] : 0.0;
         }
         __syncthreads();
-        tile_rates_fp64<CHEM_WARPS>(P, sTab, sRC, sY, sG, sC, a.sour, a.npad, cell, lane, warp);
+        tile_rates_fp64<CHEM_WARPS>(P, sTab, sRC, sY, sG, sC, a.sour, a.npad, cell, lane, warp, cls != 0);
         __syncthreads();
         // ---------------- phase 3: RC out (optional), species sums
-        if (a.rc)
+        if (a.rc && cls == 0)
             for (int r = warp; r < LRX; r += CHEM_WARPS) a.rc[(size_t)r * a.npad + cell] = sRC[r * TILE + lane];
+        if (tile_skips) {
+            // a skipped cell's omega comes from the RC it kept (solveh.f:116-1145 reads RC as it is)
+            if (cls == 1)
+                for (int r = warp; r < LRX; r += CHEM_WARPS)
+                    sRC[r * TILE + lane] = a.rc_stale ? a.rc_stale[(size_t)r * a.npad + cell] : 0.0;
+            __syncthreads();
+        }
+        const bool put = cls < 2;
         {
             const double TKD = sC[SC_TKD * TILE + lane];
             const double TKD2 = TKD * TKD, TKD3 = TKD * TKD2, TKD4 = TKD * TKD3, TKD5 = TKD * TKD4;
@@ -269,14 +285,14 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_fp64_kernel(const ChemAr
                     }
                     prd = P.WM[k] * P.HFO[k] * acc;
                 }
-                if (a.qdsp) a.qdsp[(size_t)k * a.npad + cell] = -(RCONV * prd / P.HFO[k]);
+                if (a.qdsp && put) a.qdsp[(size_t)k * a.npad + cell] = -(RCONV * prd / P.HFO[k]);
                 // species enthalpy (solveh.f:39-57) for the heat-release sum
                 const double *pa = P.poly + k * 14 + ip;
                 const double HSSP = (pa[0] * TKD + pa[1] * TKD2 / 2.0 + pa[2] * TKD3 / 3.0 + pa[3] * TKD4 / 4.0 +
                                      pa[4] * TKD5 / 5.0) / P.WM[k] * P.HCONVR;
                 const double H = HSSP * P.WMSTR * P.HSTR + pa[5] / P.WM[k] * P.GASC;
                 sG[k * TILE + lane] = prd * H / P.HFO[k];
-                if (a.dwdy) {
+                if (a.dwdy && put) {
                     double L = 0.0;
                     const int lo = P.loss_off[k], ll = P.loss_len[k];
                     for (int t = 0; t < ll; ++t) {
@@ -296,7 +312,7 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_fp64_kernel(const ChemAr
         }
         __syncthreads();
         // ---------------- phase 4: QDOT
-        if (warp == 0 && a.qdot) {
+        if (warp == 0 && a.qdot && put) {
             double hrr = 0.0;
             for (int k = 0; k < LSP; ++k) hrr = hrr + sG[k * TILE + lane];
             a.qdot[cell] = -(hrr * RCONV);

@@ -43,6 +43,7 @@ struct ChemMArgs {
     double *qdsp, *qdot, *dwdy;  // outputs (any may be null)
     int n, npad, ntile;
     int *status;
+    const int8_t *skip;          // optional ISKIP class per cell (see ChemArgs): tiles with one go to FP64
 };
 
 enum { SM_TKD = 0, SM_LNT, SM_INVT, SM_LNRHO, SM_LNRUT, SM_RHO, SM_LNDMOLEA, SM_TB0, SM_STMF = SM_TB0 + 11,
@@ -120,6 +121,7 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_mixed_kernel(const ChemM
 
     for (int tile = blockIdx.x; tile < a.ntile; tile += gridDim.x) {
         const size_t cell = (size_t)tile * TILE + lane;
+        const bool skipped = a.skip && a.skip[cell] != 0;   // the FP64 kernel redoes this tile
         // ---------------- phase 0: load
         for (int k = warp; k < LSP; k += CHEM_WARPS) {
             const double yk = a.y[(size_t)k * a.npad + cell];
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_mixed_kernel(const ChemM
                 acc = P.tb_sign[o + t] > 0 ? acc + term : acc - term;
             }
             sC[(SM_TB0 + g) * TILE + lane] = acc;
-        } else if (warp == 11 && a.sour) {
+        } else if (warp == 11 && a.sour && !skipped) {
             // soot sources (ckrates.f:1337-1352); FP64, a handful of terms per cell
             const double PI = 3.1415927e+00, RSOOT = 1.9000e+03, SIGB = 1.38e-23, AVNO = 6.0232e+23;
             const double TKD = sC[SM_TKD * TILE + lane], rho = sC[SM_RHO * TILE + lane];
@@ -256,9 +258,10 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_mixed_kernel(const ChemM
         }
         __syncthreads();
         // ---------------- phase 3: RC out (FP32), species sums
-        if (a.rc32)
+        if (skipped) s_flag = 1;
+        if (a.rc32 && !skipped)
             for (int r = warp; r < LRX; r += CHEM_WARPS) a.rc32[(size_t)r * a.npad + cell] = sRC[r * TILE + lane];
-        if (a.rc64)
+        if (a.rc64 && !skipped)
             for (int r = warp; r < LRX; r += CHEM_WARPS) a.rc64[(size_t)r * a.npad + cell] = (double)sRC[r * TILE + lane];
         {
             const float TKD = (float)sC[SM_TKD * TILE + lane];
@@ -283,13 +286,13 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_mixed_kernel(const ChemM
                 const float wnet = (float)P.WM[k] * net;
                 sNet[k * TILE + lane] = fabsf(wnet);
                 sGross[k * TILE + lane] = (float)P.WM[k] * gross;
-                if (a.qdsp) a.qdsp[(size_t)k * a.npad + cell] = -(double)(RCONVf * wnet);
+                if (a.qdsp && !skipped) a.qdsp[(size_t)k * a.npad + cell] = -(double)(RCONVf * wnet);
                 const double *pa = P.poly + k * 14 + ip;
                 const float HS = ((float)pa[0] * TKD + (float)pa[1] * TKD2 * 0.5f + (float)pa[2] * TKD3 * (1.0f / 3.0f) +
                                   (float)pa[3] * TKD4 * 0.25f + (float)pa[4] * TKD5 * 0.2f + (float)pa[5]) *
                                  (float)(P.GASC / P.WM[k]);
                 sG[k * TILE + lane] = (double)(wnet * HS);         // PRD*HENTH/HFO
-                if (a.dwdy) {
+                if (a.dwdy && !skipped) {
                     float L = 0.0f;
                     const int lo = P.loss_off[k], ll = P.loss_len[k];
                     for (int t = 0; t < ll; ++t) {
@@ -309,7 +312,7 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_mixed_kernel(const ChemM
         }
         __syncthreads();
         // ---------------- phase 4: QDOT (compensated); tile flag
-        if (warp == 0 && a.qdot) {
+        if (warp == 0 && a.qdot && !skipped) {
             float s = 0.0f, c = 0.0f;
             for (int k = 0; k < LSP; ++k) neumaier_add(s, c, (float)sG[k * TILE + lane]);
             a.qdot[cell] = -(double)((s + c) * RCONVf);

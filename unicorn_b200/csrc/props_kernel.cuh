@@ -309,6 +309,7 @@ struct TempArgs {
     double *tk;
     int *status;
     int n, npad;
+    const int8_t *skip;              // optional ISKIP class: skipped cells keep T (solveh.f:1173)
 };
 
 __global__ void __launch_bounds__(128) temperature_fp64_kernel(const TempArgs a)
@@ -316,6 +317,7 @@ __global__ void __launch_bounds__(128) temperature_fp64_kernel(const TempArgs a)
     const DevParams &P = *a.P;
     const size_t np = a.npad;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < (size_t)a.n; c += (size_t)gridDim.x * blockDim.x) {
+        if (a.skip && a.skip[c]) continue;
         double ENTH = (a.ht[c] - (double)0.5f * 0.0) * P.HSTR;
         for (int k = 0; k < LSP; ++k) ENTH = ENTH + a.y[k * np + c] * P.HFO[k] * P.HSTR;
         int IPL = 0;

@@ -76,6 +76,11 @@ struct uc_ctx {
     double *f_u = nullptr, *f_v = nullptr, *f_tmu = nullptr;
     double *fe = nullptr, *fw = nullptr, *fn = nullptr, *fs = nullptr;
     uint8_t *hold = nullptr;
+    // ISKIP of the reference (src/lib/skipdf.f): class per cell 0 (computed), 1 (3 <= ISKIP < 10),
+    // 2 (ISKIP >= 10); skip_hold = class >= 1; hold_comb = that or the grid boundary
+    int8_t *skip = nullptr;
+    uint8_t *skip_hold = nullptr, *hold_comb = nullptr;
+    bool have_skip = false;
     bool have_grid = false, have_flow = false, faces_ready = false;
     double *fd_x = nullptr, *fd_y = nullptr, *fd_u = nullptr, *fd_v = nullptr, *fd_out = nullptr;
     // enthalpy equation (SOLVEH)
@@ -363,7 +368,7 @@ static void free_ctx(uc_ctx *c)
         if (c->pnd) cudaFree(c->pnd);
         if (c->enth) cudaFree(c->enth);
         void *fb[] = {c->g_xxs, c->g_xxc, c->g_yys, c->g_yyc, c->g_yr, c->f_u, c->f_v, c->f_tmu,
-                      c->fe, c->fw, c->fn, c->fs, c->hold, c->fd_x, c->fd_y, c->fd_u, c->fd_v, c->fd_out,
+                      c->fe, c->fw, c->fn, c->fs, c->hold, c->skip, c->skip_hold, c->hold_comb, c->fd_x, c->fd_y, c->fd_u, c->fd_v, c->fd_out,
                       c->e_w, c->e_ekt, c->e_rdhsp, c->e_prod, c->e_fpz, c->e_ze, c->e_zw, c->e_zn, c->e_zs,
                       c->e_rhsz, c->e_cf, c->e_f0s, c->e_part};
         for (void *b : fb)
@@ -515,6 +520,7 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
             (rc = dalloc(ctx, &ctx->soot, 2 * np)) || (rc = dalloc(ctx, &ctx->soot0, 2 * np)) ||
             (rc = dalloc(ctx, &ctx->sour, 6 * np)))
             break;
+        cudaMemset(ctx->sour, 0, 6 * np * sizeof(double));
         e = cudaFuncSetAttribute(chem_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CHEM_SMEM);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(chem_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CHEMM_SMEM);
@@ -599,6 +605,61 @@ extern "C" int uc_upload_fields(uc_ctx *ctx, const double *tk, const double *rho
     return UC_OK;
 }
 
+static int ensure_u8(uc_ctx *ctx, uint8_t **p, size_t count)
+{
+    if (*p) return UC_OK;
+    if (cudaMalloc((void **)p, count) != cudaSuccess) {
+        *p = nullptr;
+        return set_err(ctx, UC_E_NOMEM, "device allocation of a %zu-byte mask failed", count);
+    }
+    return UC_OK;
+}
+
+// ISKIP (int per cell) -> class 0 (computed), 1 (3 <= ISKIP < 10), 2 (ISKIP >= 10) and the mask of
+// cells that keep their state in the update; padding cells are class 0
+__global__ void skip_class_kernel(const int *iskip, int n, int npad, int8_t *cls, uint8_t *keep)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < npad; c += gridDim.x * blockDim.x) {
+        const int v = c < n ? iskip[c] : 0;
+        const int8_t k = v >= 10 ? 2 : (v >= 3 ? 1 : 0);
+        cls[c] = k;
+        keep[c] = k != 0;
+    }
+}
+
+__global__ void or_mask_kernel(const uint8_t *a, const uint8_t *b, int npad, uint8_t *out)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < npad; c += gridDim.x * blockDim.x)
+        out[c] = (uint8_t)(a[c] | b[c]);
+}
+
+extern "C" int uc_set_iskip(uc_ctx *ctx, const int *iskip)
+{
+    if (!ctx) return UC_E_ARG;
+    CK(cudaSetDevice(ctx->device));
+    if (!iskip) {
+        ctx->have_skip = false;
+        return UC_OK;
+    }
+    if (!ctx->skip && cudaMalloc((void **)&ctx->skip, ctx->npad) != cudaSuccess) {
+        ctx->skip = nullptr;
+        return set_err(ctx, UC_E_NOMEM, "ISKIP class array");
+    }
+    RET_IF(ensure_u8(ctx, &ctx->skip_hold, ctx->npad));
+    int *tmp = nullptr;
+    CK(cudaMalloc((void **)&tmp, (size_t)ctx->n * sizeof(int)));
+    cudaError_t e = cudaMemcpyAsync(tmp, iskip, (size_t)ctx->n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        skip_class_kernel<<<ctx->nsm * 4, 256, 0, ctx->stream>>>(tmp, ctx->n, ctx->npad, ctx->skip, ctx->skip_hold);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return set_err(ctx, UC_E_CUDA, "uc_set_iskip: %s", cudaGetErrorString(e));
+    ctx->have_skip = true;
+    return UC_OK;
+}
+
 // rows of a device array with row stride ld (elements) into a context array [rows][npad]
 static int copy_rows_device(uc_ctx *ctx, double *dst, const double *src, int rows, int ld)
 {
@@ -656,18 +717,30 @@ static int launch_chem(uc_ctx *ctx, int precision, bool want_rc, bool want_omega
         cudaError_t e = cudaMalloc((void **)&ctx->rc32, (size_t)LRX * ctx->npad * sizeof(float));
         if (e != cudaSuccess) { ctx->rc32 = nullptr; return set_err(ctx, UC_E_NOMEM, "FP32 RC plane: %s", cudaGetErrorString(e)); }
     }
-    if (want_rc) RET_IF(dalloc(ctx, &ctx->rc, (size_t)LRX * ctx->npad));   // mixed: FP64 plane of fallback tiles
+    if (want_rc && !ctx->rc) {         // mixed: FP64 plane of fallback tiles
+        RET_IF(dalloc(ctx, &ctx->rc, (size_t)LRX * ctx->npad));
+        // zero like the reference's COMMON: cells skipped by ISKIP keep what the plane holds
+        CK(cudaMemsetAsync(ctx->rc, 0, (size_t)LRX * ctx->npad * sizeof(double), ctx->stream));
+    }
     if (precision == UC_MIXED && !ctx->tile_flag) {
         if (cudaMalloc((void **)&ctx->tile_flag, ctx->ntile * sizeof(int)) != cudaSuccess ||
             cudaMalloc((void **)&ctx->tile_list, ctx->ntile * sizeof(int)) != cudaSuccess ||
             cudaMalloc((void **)&ctx->tile_count, sizeof(int)) != cudaSuccess)
             return set_err(ctx, UC_E_NOMEM, "tile flag buffers");
     }
-    if (want_omega) {
+    if (want_omega && !ctx->qdsp) {
         RET_IF(dalloc(ctx, &ctx->qdsp, (size_t)LSP * ctx->npad));
-        RET_IF(dalloc(ctx, &ctx->qdot, ctx->npad));
-        RET_IF(dalloc(ctx, &ctx->dwdy, (size_t)LSP * ctx->npad));
+        CK(cudaMemsetAsync(ctx->qdsp, 0, (size_t)LSP * ctx->npad * sizeof(double), ctx->stream));
     }
+    if (want_omega && !ctx->qdot) {
+        RET_IF(dalloc(ctx, &ctx->qdot, ctx->npad));
+        CK(cudaMemsetAsync(ctx->qdot, 0, (size_t)ctx->npad * sizeof(double), ctx->stream));
+    }
+    if (want_omega && !ctx->dwdy) {
+        RET_IF(dalloc(ctx, &ctx->dwdy, (size_t)LSP * ctx->npad));
+        CK(cudaMemsetAsync(ctx->dwdy, 0, (size_t)LSP * ctx->npad * sizeof(double), ctx->stream));
+    }
+    const int8_t *skip = ctx->have_skip ? ctx->skip : nullptr;
     if (precision == UC_MIXED) {
         ChemMArgs m{};
         m.P = ctx->dP; m.tab = ctx->dTabM;
@@ -681,6 +754,7 @@ static int launch_chem(uc_ctx *ctx, int precision, bool want_rc, bool want_omega
         m.dwdy = want_omega ? ctx->dwdy : nullptr;
         m.n = ctx->n; m.npad = ctx->npad; m.ntile = ctx->ntile; m.status = ctx->status;
         m.tile_flag = ctx->tile_flag;
+        m.skip = skip;
         const int grid = std::min(ctx->ntile, ctx->nsm);
         int slot;
         prof_begin(ctx, UC_K_CHEM, slot);
@@ -698,6 +772,7 @@ static int launch_chem(uc_ctx *ctx, int precision, bool want_rc, bool want_omega
         f.qdsp = m.qdsp; f.qdot = m.qdot; f.dwdy = m.dwdy;
         f.n = ctx->n; f.npad = ctx->npad; f.ntile = ctx->ntile; f.status = ctx->status;
         f.tile_list = ctx->tile_list; f.tile_count = ctx->tile_count;
+        f.skip = skip; f.rc_stale = ctx->rc;
         prof_begin(ctx, UC_K_CHEM, slot);
         chem_fp64_kernel<<<std::min(ctx->ntile, ctx->nsm), CHEM_THREADS, CHEM_SMEM, ctx->stream>>>(f);
         prof_end(ctx, slot);
@@ -716,6 +791,7 @@ static int launch_chem(uc_ctx *ctx, int precision, bool want_rc, bool want_omega
     a.dwdy = want_omega ? ctx->dwdy : nullptr;
     a.n = ctx->n; a.npad = ctx->npad; a.ntile = ctx->ntile;
     a.status = ctx->status;
+    a.skip = skip; a.rc_stale = ctx->rc;
     const int grid = std::min(ctx->ntile, ctx->nsm);
     int slot;
     prof_begin(ctx, UC_K_CHEM, slot);
@@ -878,6 +954,17 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
         RET_IF(upload_rows(ctx, ctx->face_nbr, face_nbr, LSP - 1));
         fn = ctx->face_nbr;
     }
+    if (ctx->have_skip) {
+        // cells skipped by ISKIP keep their state and leave the residual (solvesp.f:89,2842)
+        if (hold) {
+            RET_IF(ensure_u8(ctx, &ctx->hold_comb, ctx->npad));
+            or_mask_kernel<<<ctx->nsm * 4, 256, 0, ctx->stream>>>(hold, ctx->skip_hold, ctx->npad, ctx->hold_comb);
+            CK(cudaGetLastError());
+            hold = ctx->hold_comb;
+        } else {
+            hold = ctx->skip_hold;
+        }
+    }
     UpdArgs a{};
     a.P = ctx->dP; a.rc = ctx->rc; a.rc32 = ctx->rc32; a.sour = ctx->sour;
     a.tile_flag = ctx->rc_prec == UC_MIXED ? ctx->tile_flag : nullptr; a.rho = ctx->rho; a.y0 = ctx->y0; a.soot0 = ctx->soot0;
@@ -940,7 +1027,7 @@ extern "C" int uc_temperature_from_h(uc_ctx *ctx, const double *ht)
     CK(cudaSetDevice(ctx->device));
     RET_IF(dalloc(ctx, &ctx->ht, ctx->npad));
     RET_IF(upload_rows(ctx, ctx->ht, ht, 1));
-    TempArgs a{ctx->dP, ctx->y, ctx->ht, ctx->tk, ctx->status, ctx->n, ctx->npad};
+    TempArgs a{ctx->dP, ctx->y, ctx->ht, ctx->tk, ctx->status, ctx->n, ctx->npad, ctx->have_skip ? ctx->skip : nullptr};
     const int grid = std::min((ctx->n + 127) / 128, ctx->nsm * 16);
     int slot;
     prof_begin(ctx, UC_K_TEMP, slot);

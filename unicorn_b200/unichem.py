@@ -102,6 +102,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
                              ctypes.c_double, P, P, ctypes.POINTER(ctypes.c_int)]
     lib.uc_download_outputs.argtypes = [vp, P, P, P, P, P, P, P, P]
     lib.uc_chem_props.argtypes = [vp, ctypes.c_int]
+    lib.uc_set_iskip.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     lib.uc_profile.argtypes = [vp, ctypes.c_int]
     lib.uc_profile_read.argtypes = [vp, P, ctypes.POINTER(ctypes.c_int)]
     lib.uc_stat.argtypes = [vp, ctypes.c_char_p, P]
@@ -208,6 +209,16 @@ class UniChem:
         """State from device memory: integer device addresses (e.g. torch's data_ptr()) of
         tk, rho [ld], y [52][ld], stmf, stnd [ld] (or None); asynchronous on the context's stream."""
         self._ck(self.lib.uc_upload_fields_device(self._h, tk, rho, y, stmf, stnd, int(ld if ld is not None else self.n)))
+
+    def set_iskip(self, iskip=None):
+        """The reference's ISKIP per cell (int [n]); None clears it."""
+        if iskip is None:
+            self._ck(self.lib.uc_set_iskip(self._h, None))
+            return
+        a = np.ascontiguousarray(iskip, dtype=np.int32)
+        if a.shape != (self.n,):
+            raise ValueError(f"expected shape ({self.n},), got {a.shape}")
+        self._ck(self.lib.uc_set_iskip(self._h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
 
     def download(self):
         n = self.n
