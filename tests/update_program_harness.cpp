@@ -85,6 +85,7 @@ extern "C" int harness_update_tr(int n, const double *rho_a, const double *y0_a,
 {
     const double sor1 = relx, sor2 = 1.0 - relx;
     double y[LSP], y0[LSP], sour[6], ysh[UC_IP_NSHADOW], srows[UC_TR_NS], trows[UC_TR_NT], bank[2][UC_TR_SEG];
+    double y0s[2], fss[2], fns[2];
     int pass;
     for (pass = 1; pass <= isor; ++pass) {
         double rsd = 0.0;
@@ -100,6 +101,11 @@ extern "C" int harness_update_tr(int n, const double *rho_a, const double *y0_a,
 #define TM_LD(b, q, col) bank[b][q] = trows[(col) / 2]
 #define TM_WAIT(b) do { } while (0)
 #define RCT(b, q) bank[b][q]
+#define UC_TR_PF(s, k) do { y0s[s] = y0[k]; fss[s] = 0.0; fns[s] = 0.0; } while (0)
+#define Y0S(s) y0s[s]
+#define FSS(s) fss[s]
+#define FNS(s) fns[s]
+#define UC_TR_SYNC() do { } while (0)
             UC_TR_SHADOW_SAVE();
             UC_UPDATE_PROGRAM_TR();
             for (int k = 0; k < LSP - 1; ++k) y_a[k * n + c] = y[k];

@@ -67,6 +67,7 @@ struct uc_ctx {
     int upd_ip = 0, ip_grid = 0;       // FP64 update with Y in place: warps per CTA (0: two Y sets, 8 warps)
     int upd_kind = 0;                  // 0: tile-resident (default), 1: Y in place per pass, 2: two Y sets per pass
     int tr_chunk = 8;                  // tile-resident update: passes per chunk
+    bool tr_lock = true;               // ... with the warps of a block in step species by species
     double *tr_snap = nullptr, *tr_partial = nullptr;
     size_t tr_snap_cap = 0;
     // species-equation faces assembled on the device (grid, flow, coefficients)
@@ -465,6 +466,13 @@ static void ip_kernel(bool mixed, const void **fn, size_t *sm)
     *sm = upd_smem<UPD_IP_WARPS, true>();
 }
 
+// the tile-resident update kernel for the face terms given or not, warps in step or not
+static const void *tr_kernel(bool faces, bool lock)
+{
+    if (faces) return lock ? (const void *)update_tr_kernel<true, true> : (const void *)update_tr_kernel<true, false>;
+    return lock ? (const void *)update_tr_kernel<false, true> : (const void *)update_tr_kernel<false, false>;
+}
+
 #define RET_IF(x)                 \
     do {                          \
         int r_ = (x);             \
@@ -544,11 +552,15 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
         }
         if (const char *k = getenv("UNICHEM_TR_CHUNK")) ctx->tr_chunk = std::max(1, std::min(TR_CHUNK_MAX, atoi(k)));
         if (ctx->upd_kind == 0) {
-            e = cudaFuncSetAttribute(update_tr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM);
-            if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "smem attribute: %s", cudaGetErrorString(e)); break; }
-            int tr_per_sm = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tr_per_sm, update_tr_kernel, TR_WARPS * 32, TR_SMEM);
-            if (tr_per_sm < 1) { rc = set_err(ctx, UC_E_CUDA, "the tile-resident update does not fit an SM"); break; }
+            if (const char *k = getenv("UNICHEM_TR_LOCKSTEP")) ctx->tr_lock = atoi(k) != 0;
+            for (int f = 0; f < 2 && e == cudaSuccess; ++f) {
+                const void *fn = tr_kernel(f != 0, ctx->tr_lock);
+                e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM);
+                int tr_per_sm = 0;
+                if (e == cudaSuccess) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tr_per_sm, fn, TR_WARPS * 32, TR_SMEM);
+                if (e == cudaSuccess && tr_per_sm < 1) e = cudaErrorInvalidConfiguration;
+            }
+            if (e != cudaSuccess) { rc = set_err(ctx, UC_E_CUDA, "tile-resident update set-up: %s", cudaGetErrorString(e)); break; }
         }
         if (ctx->upd_ip) {
             const void *fn, *fnm; size_t sm;
@@ -989,8 +1001,8 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
         TrArgs t{ctx->tr_snap, ctx->tr_partial, C, ctx->status};
         void *targs[] = {&a, &t};
         prof_begin(ctx, UC_K_UPDATE, slot);
-        CK(cudaLaunchCooperativeKernel((const void *)update_tr_kernel, dim3(ctx->nsm), dim3(TR_WARPS * 32), targs,
-                                       TR_SMEM, ctx->stream));
+        CK(cudaLaunchCooperativeKernel(tr_kernel(fs != nullptr || fn != nullptr, ctx->tr_lock), dim3(ctx->nsm),
+                                       dim3(TR_WARPS * 32), targs, TR_SMEM, ctx->stream));
         prof_end(ctx, slot);
         if (passes) {
             CK(cudaMemcpyAsync(passes, ctx->passes, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1104,6 +1116,7 @@ extern "C" int uc_stat(uc_ctx *ctx, const char *name, double *value)
     if (!strcmp(name, "update_ip_warps")) { *value = ctx->upd_ip; return UC_OK; }
     if (!strcmp(name, "update_kind")) { *value = ctx->upd_kind; return UC_OK; }
     if (!strcmp(name, "update_chunk")) { *value = ctx->tr_chunk; return UC_OK; }
+    if (!strcmp(name, "update_lockstep")) { *value = ctx->tr_lock; return UC_OK; }
     if (!strcmp(name, "int_sorted")) { *value = ctx->int_sorted; return UC_OK; }
     if (!strcmp(name, "int_tune_best_ms")) { *value = ctx->tune_best; return UC_OK; }
     if (!strcmp(name, "int_tune_worst_ms")) { *value = ctx->tune_worst; return UC_OK; }

@@ -81,6 +81,10 @@ __device__ __forceinline__ void tr_tmem_st16(uint32_t taddr, const uint32_t (&v)
                  : "memory")
 static_assert(UC_TR_SEG == 12, "UC_TR_WAIT_BANK names 2 x 12 registers");
 
+// FACES: the frozen transport terms are given (else they are zero, as in SOLVESP without faces);
+// LOCK: the warps of a block run each species of the program together (a barrier after each), so
+// that they fetch the program's instructions once instead of three times.
+template <bool FACES, bool LOCK>
 __global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdArgs a, const TrArgs t)
 {
     namespace cg = cooperative_groups;
@@ -88,6 +92,7 @@ __global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdAr
     extern __shared__ __align__(128) double s_rc[];          // [TR_WARPS][UC_TR_NS][32]
     __shared__ double s_wm[LSP];
     __shared__ double s_part[TR_WARPS][TR_CHUNK_MAX];
+    __shared__ double s_cell[TR_WARPS][8][TILE];            // SOUR 1..6 and the two soot values of the old level
     __shared__ __align__(8) uint64_t s_bar[TR_WARPS];
     __shared__ uint32_t s_tmem;
     __shared__ int s_stop;
@@ -121,10 +126,11 @@ __global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdAr
         if (lane < TR_CHUNK_MAX) s_part[w][lane] = 0.0;
         __syncwarp();
         for (int round = 0; round < rounds; ++round) {
-            const int tile = gwarp + round * nwarp;
-            if (tile >= a.ntile) break;
+            int tile = gwarp + round * nwarp;
+            const bool own = tile < a.ntile;          // without a tile of its own a warp repeats the last
+            if (!own) tile = a.ntile - 1;             // one (nothing stored) to keep the barriers matched
             const size_t cell = (size_t)tile * TILE + lane;
-            const bool live = cell < (size_t)a.n && !(a.hold && a.hold[cell]);
+            const bool live = own && cell < (size_t)a.n && !(a.hold && a.hold[cell]);
             // ---- stage the tile's RC block: shared-memory rows by bulk copies, tensor-memory rows via registers
             __syncwarp();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -150,11 +156,13 @@ __global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdAr
 #pragma unroll
             for (int k = 0; k < LSP; ++k) yv[k] = a.y[k * np + cell];
             const double rho = a.rho[cell];
-            double so[6];
+            double *sc = &s_cell[w][0][lane];        // sc[m * TILE]: SOUR(m), m < 6; old soot at 6, 7
 #pragma unroll
-            for (int m = 0; m < 6; ++m) so[m] = a.sour[m * np + cell];
+            for (int m = 0; m < 6; ++m) sc[m * TILE] = a.sour[m * np + cell];
+            sc[6 * TILE] = a.soot0[cell];
+            sc[7 * TILE] = a.soot0[np + cell];
             double st1 = a.soot[cell], st2 = a.soot[np + cell];
-            const double st01 = a.soot0[cell], st02 = a.soot0[np + cell];
+            double y0s0, y0s1, fss0 = 0.0, fss1 = 0.0, fns0 = 0.0, fns1 = 0.0;
             if (!mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES)) {
                 if (lane == 0) atomicExch(t.status, ST_TMA_TIMEOUT);
                 mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES);   // let copies in flight land
@@ -167,11 +175,20 @@ __global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdAr
 #define YO(k) yv[k]
 #define YN(k) yv[k]
 #define YOS(m) ysh[m]
-#define Y0(k) __ldg(a.y0 + (size_t)(k) * np + cell)
-#define SOUR(m) so[m]
+#define SOUR(m) sc[(m) * TILE]
 #define WM(k) s_wm[k]
-#define FACE_SUM(k) (a.face_sum ? __ldg(a.face_sum + (size_t)(k) * np + cell) : 0.0)
-#define FACE_NBR(k) (a.face_nbr ? __ldg(a.face_nbr + (size_t)(k) * np + cell) : 0.0)
+#define UC_TR_PF(s, k)                                                                  \
+    do {                                                                                \
+        y0s##s = __ldg(a.y0 + (size_t)(k) * np + cell);                                \
+        if (FACES) {                                                                    \
+            fss##s = a.face_sum ? __ldg(a.face_sum + (size_t)(k) * np + cell) : 0.0;   \
+            fns##s = a.face_nbr ? __ldg(a.face_nbr + (size_t)(k) * np + cell) : 0.0;   \
+        }                                                                               \
+    } while (0)
+#define Y0S(s) y0s##s
+#define FSS(s) fss##s
+#define FNS(s) fns##s
+#define UC_TR_SYNC() do { if (LOCK) __syncthreads(); } while (0)
 #define UC_UPDATE_TAIL(k) do { if (fnew < 0.0) fnew = 0.0; yv[k] = fnew; } while (0)
 #define RCS(i) slot[(i) * TILE + lane]
 #define TM_LD(b, q, col)                                                                              \
@@ -185,11 +202,13 @@ __global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdAr
 #undef YO
 #undef YN
 #undef YOS
-#undef Y0
 #undef SOUR
 #undef WM
-#undef FACE_SUM
-#undef FACE_NBR
+#undef UC_TR_PF
+#undef Y0S
+#undef FSS
+#undef FNS
+#undef UC_TR_SYNC
 #undef UC_UPDATE_TAIL
 #undef RCS
 #undef TM_LD
@@ -199,14 +218,16 @@ __global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdAr
                 // soot mass fraction and number density (solvesp.f:2807-2832)
                 {
                     const double y2 = yv[1], y4 = yv[3], y5 = yv[4], y22 = yv[21];
-                    double rhs1 = rho * st01 + dt * ((double)0.012011f / P.WMSTR) *
-                                                   (2.0 * so[0] * y22 - so[2] * y2 - so[3] * y5 - so[4] * y4);
+                    const double so0 = sc[0], so1 = sc[TILE], so2 = sc[2 * TILE], so3 = sc[3 * TILE],
+                                 so4 = sc[4 * TILE], so5 = sc[5 * TILE];
+                    double rhs1 = rho * sc[6 * TILE] + dt * ((double)0.012011f / P.WMSTR) *
+                                                       (2.0 * so0 * y22 - so2 * y2 - so3 * y5 - so4 * y4);
                     double fnew = sor2 * st1 + rhs1 * sor1 / ((rho - 0.0) - 0.0);
                     crsd += fabs(st1 - fnew);
                     if (fnew < 0.0) fnew = 0.0;
                     const double n1 = fnew;
-                    rhs1 = rho * st02 + dt * so[1] * y22;
-                    const double rhs2 = -(dt * so[5]);
+                    rhs1 = rho * sc[7 * TILE] + dt * so1 * y22;
+                    const double rhs2 = -(dt * so5);
                     fnew = sor2 * st2 + rhs1 * sor1 / ((rho - 0.0) - rhs2);
                     if (fnew < 0.0) fnew = 0.0;
                     st1 = n1;

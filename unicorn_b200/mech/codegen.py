@@ -294,22 +294,27 @@ def gen_tr_program(blocks, uses: dict, shadow: list[int]) -> str:
     those of the in-place program."""
     import re
     ctx = _TRCtx(uses)
-    body = []
-    for b in blocks:
+    body = [f"UC_TR_PF(0, {blocks[0]['species']});"]
+    for bi, b in enumerate(blocks):
         k = b["species"]
-        if b["prod"] is not None:
-            body += emit_sum(b["prod"], ctx, "prod")
-        body += emit_sum(b["extra"], ctx, "extra")
-        body.append(f"rhs1 = rho * Y0({k}) + dt * WM({k}) * (prod + extra);")
-        if b["loss"] is None:
-            body.append("rhs2 = 0.0;")
-        else:
-            body += emit_sum(b["loss"], ctx, "loss")
-            body.append(f"rhs2 = -(dt * WM({k}) * loss);")
-        body.append(f"ppp = rho - FACE_SUM({k});")
-        body.append(f"fnew = sor2 * YO({k}) + (rhs1 - FACE_NBR({k})) * sor1 / (ppp - rhs2);")
+        slot = bi % 2
+        if bi + 1 < len(blocks):
+            # old time level and face terms of the next species, one block ahead of their use
+            body.append(f"UC_TR_PF({(bi + 1) % 2}, {blocks[bi + 1]['species']});")
+        # the production, extra and loss sums are independent of each other: their statements are
+        # interleaved (each sum keeps its own order) so that two or three chains are in flight
+        sums = [emit_sum(b["prod"], ctx, "prod") if b["prod"] is not None else [],
+                emit_sum(b["extra"], ctx, "extra"),
+                emit_sum(b["loss"], ctx, "loss") if b["loss"] is not None else []]
+        for i in range(max(len(x) for x in sums)):
+            body += [x[i] for x in sums if i < len(x)]
+        body.append(f"rhs1 = rho * Y0S({slot}) + dt * WM({k}) * (prod + extra);")
+        body.append("rhs2 = 0.0;" if b["loss"] is None else f"rhs2 = -(dt * WM({k}) * loss);")
+        body.append(f"ppp = rho - FSS({slot});")
+        body.append(f"fnew = sor2 * YO({k}) + (rhs1 - FNS({slot})) * sor1 / (ppp - rhs2);")
         body.append(f"rsd += fabs(YO({k}) - fnew);")
         body.append(f"UC_UPDATE_TAIL({k});")
+        body.append("UC_TR_SYNC();")
         ctx.updated.add(k)
     assert ctx.shadow == shadow, "the tile-resident and in-place programs must shadow the same species"
     tok = re.compile(r"@(\d+)@")
@@ -358,8 +363,11 @@ def gen_tr_program(blocks, uses: dict, shadow: list[int]) -> str:
          f"// word), {len(srow)} in shared memory. Requires RCS(i) (shared-memory row i of the",
          "// cell), TM_LD(bank, q, col) (load the double at column col into slot q of a",
          "// register bank), TM_WAIT(bank) (wait for the loads of that bank), RCT(bank, q),",
-         "// and the accessors of the in-place program (YO, YN, YOS, Y0, SOUR, WM, FACE_SUM,",
-         "// FACE_NBR, UC_UPDATE_TAIL; scalars rho, dt, sor1, sor2, rsd).",
+         "// UC_TR_PF(slot, k) (fetch Y0, FACE_SUM and FACE_NBR of species k into register slot 0",
+         "// or 1; read as Y0S, FSS, FNS), UC_TR_SYNC() (after every species: a barrier or nothing)",
+         "// and the accessors of the in-place program (YO, YN, YOS, SOUR, WM, UC_UPDATE_TAIL;",
+         "// scalars rho, dt, sor1, sor2, rsd). The production, extra and loss statements of a",
+         "// species are interleaved; each sum keeps the reference's order.",
          f"// {len(segs)} segments and {nld} tensor-memory loads per cell and pass.",
          "#pragma once",
          f"#define UC_TR_NT {len(trow)}",
