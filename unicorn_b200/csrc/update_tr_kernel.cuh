@@ -21,9 +21,11 @@
 // the cell lives in registers (lane = cell). The generated program
 // (generated/update_program_tr.cuh) loads tensor-memory operands into two
 // register banks ahead of use; shared-memory rows are read where used.
-// Shared-memory rows are staged by bulk copies (cp.async.bulk, 256 B per row,
-// completion on the warp's mbarrier with a bounded wait), tensor-memory rows
-// by loads into registers and tcgen05.st.
+// A tile is staged by bulk copies (cp.async.bulk, 256 B per row, completion
+// on the warp's mbarrier with a bounded wait): first its tensor-memory rows
+// into the warp's shared-memory slot, from where tcgen05.st moves them on,
+// then its shared-memory rows (register loads from HBM instead were bound by
+// load latency: 4-5 ms per chunk on 1M cells).
 //
 // Every cell goes through the same operations in the same order as in the
 // in-place kernel, so Y is bit for bit that kernel's; the residual is summed
@@ -131,7 +133,33 @@ __global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdAr
             if (!own) tile = a.ntile - 1;             // one (nothing stored) to keep the barriers matched
             const size_t cell = (size_t)tile * TILE + lane;
             const bool live = own && cell < (size_t)a.n && !(a.hold && a.hold[cell]);
-            // ---- stage the tile's RC block: shared-memory rows by bulk copies, tensor-memory rows via registers
+            // ---- stage the tile's RC block, all rows by bulk copies (bandwidth-bound, not latency-bound):
+            // first the tensor-memory rows into the shared-memory slot, moved on by tcgen05.st, then
+            // the shared-memory rows into the slot
+            __syncwarp();
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_expect_tx(&s_bar[w], (uint32_t)(UC_TR_NT * TILE * sizeof(double)));
+            __syncwarp();
+            for (int i = lane; i < UC_TR_NT; i += 32)
+                bulk_g2s(slot + (size_t)i * TILE, a.rc + (size_t)uc_tr_trow[i] * np + (size_t)tile * TILE,
+                         (uint32_t)(TILE * sizeof(double)), &s_bar[w]);
+            if (!mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES)) {
+                if (lane == 0) atomicExch(t.status, ST_TMA_TIMEOUT);
+                mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES);   // let copies in flight land
+            }
+            phase ^= 1u;
+            for (int i0 = 0; i0 < UC_TR_NT; i0 += 16) {
+                uint32_t v[32];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const double d = slot[(size_t)(i0 + q) * TILE + lane];
+                    v[2 * q] = (uint32_t)__double2loint(d);
+                    v[2 * q + 1] = (uint32_t)__double2hiint(d);
+                }
+                tr_tmem_st16(tbase + (uint32_t)(2 * i0), v);
+            }
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             __syncwarp();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
@@ -140,17 +168,6 @@ __global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdAr
             for (int i = lane; i < UC_TR_NS; i += 32)
                 bulk_g2s(slot + (size_t)i * TILE, a.rc + (size_t)uc_tr_srow[i] * np + (size_t)tile * TILE,
                          (uint32_t)(TILE * sizeof(double)), &s_bar[w]);
-            for (int i0 = 0; i0 < UC_TR_NT; i0 += 16) {
-                uint32_t v[32];
-#pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const double d = __ldcg(a.rc + (size_t)uc_tr_trow[i0 + q] * np + cell);
-                    v[2 * q] = (uint32_t)__double2loint(d);
-                    v[2 * q + 1] = (uint32_t)__double2hiint(d);
-                }
-                tr_tmem_st16(tbase + (uint32_t)(2 * i0), v);
-            }
-            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             // ---- the cell's state (Y in registers)
             double yv[LSP], ysh[UC_IP_NSHADOW];
 #pragma unroll
