@@ -70,6 +70,8 @@ struct uc_ctx {
     bool tr_lock = false;              // ... with the warps of a block in step species by species
                                        // (measured on 1M cells, 100 passes: 227 ms in step, 221 ms free)
     double *tr_snap = nullptr, *tr_partial = nullptr;
+    CUtensorMap tr_map[2];             // the RC plane as a 2-D tensor [544][npad], boxes of 256 and 144 rows
+    const double *tr_map_base = nullptr;
     size_t tr_snap_cap = 0;
     // species-equation faces assembled on the device (grid, flow, coefficients)
     int lj = 0, li = 0, isym = 0;
@@ -465,6 +467,39 @@ static void ip_kernel(bool mixed, const void **fn, size_t *sm)
     *fn = mixed ? (const void *)update_kernel<float, UPD_IP_WARPS, true>
                 : (const void *)update_kernel<double, UPD_IP_WARPS, true>;
     *sm = upd_smem<UPD_IP_WARPS, true>();
+}
+
+// The RC plane [544][npad] (FP64) as a tiled tensor map: boxes of 32 cells x `rows` rows, no swizzle,
+// no interleave (a box lands in shared memory as [rows][32], the slot layout). cuTensorMapEncodeTiled
+// is reached through the runtime's driver entry point, so the library links no driver library.
+typedef CUresult (*uc_encode_tiled_fn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                       const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                       CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static int encode_rc_map(uc_ctx *ctx)
+{
+    if (ctx->tr_map_base == ctx->rc) return UC_OK;
+    static uc_encode_tiled_fn encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+            return set_err(ctx, UC_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        encode = (uc_encode_tiled_fn)fn;
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)ctx->npad, (cuuint64_t)LRX};
+    const cuuint64_t strides[1] = {(cuuint64_t)ctx->npad * sizeof(double)};
+    const cuuint32_t estr[2] = {1, 1};
+    const cuuint32_t rows[2] = {TR_BOX_T, TR_BOX_S};      // the tensor-memory box and the shared-memory boxes
+    for (int m = 0; m < 2; ++m) {
+        const cuuint32_t box[2] = {(cuuint32_t)TILE, rows[m]};
+        CUresult r = encode(&ctx->tr_map[m], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)ctx->rc, dims, strides, box,
+                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return set_err(ctx, UC_E_CUDA, "tensor map of the RC plane: error %d", (int)r);
+    }
+    ctx->tr_map_base = ctx->rc;
+    return UC_OK;
 }
 
 // the tile-resident update kernel for the face terms given or not, warps in step or not
@@ -1000,7 +1035,8 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
         }
         RET_IF(dalloc(ctx, &ctx->tr_partial, 2 * (size_t)TR_CHUNK_MAX * ctx->nsm));
         TrArgs t{ctx->tr_snap, ctx->tr_partial, C, ctx->status};
-        void *targs[] = {&a, &t};
+        RET_IF(encode_rc_map(ctx));
+        void *targs[] = {&a, &t, &ctx->tr_map[0], &ctx->tr_map[1]};
         prof_begin(ctx, UC_K_UPDATE, slot);
         CK(cudaLaunchCooperativeKernel(tr_kernel(fs != nullptr || fn != nullptr, ctx->tr_lock), dim3(ctx->nsm),
                                        dim3(TR_WARPS * 32), targs, TR_SMEM, ctx->stream));

@@ -21,11 +21,14 @@
 // the cell lives in registers (lane = cell). The generated program
 // (generated/update_program_tr.cuh) loads tensor-memory operands into two
 // register banks ahead of use; shared-memory rows are read where used.
-// A tile is staged by bulk copies (cp.async.bulk, 256 B per row, completion
-// on the warp's mbarrier with a bounded wait): first its tensor-memory rows
-// into the warp's shared-memory slot, from where tcgen05.st moves them on,
-// then its shared-memory rows (register loads from HBM instead were bound by
-// load latency: 4-5 ms per chunk on 1M cells).
+// Slots 0..255 live in tensor memory and slots 256..543 in shared memory, so
+// each part is one contiguous range of the plane's rows. A tile is staged by
+// three tiled bulk copies through tensor maps of the plane ([32 cells] x [rows]
+// boxes, completion on the warp's mbarrier with a bounded wait): first the
+// tensor-memory rows into the warp's shared-memory slot, from where tcgen05.st
+// moves them on, then the shared-memory rows (loads of the rows into
+// registers, or one 256-byte bulk copy per row, were bound by latency or by
+// the copy count: 4-5 and 3-4 ms per chunk on 1M cells).
 //
 // Every cell goes through the same operations in the same order as in the
 // in-place kernel, so Y is bit for bit that kernel's; the residual is summed
@@ -33,6 +36,7 @@
 // blocks in block order.
 #pragma once
 #include <cooperative_groups.h>
+#include <cuda.h>                       // CUtensorMap (the type only; encoded through the runtime's entry point)
 
 #include "uc_device.cuh"
 #include "update_kernel.cuh"
@@ -45,8 +49,11 @@ constexpr int TR_CHUNK_MAX = 16;
 constexpr int TR_SNAP_ROWS = LSP - 1 + 2;          // Y of species 1..51 and the two soot scalars
 constexpr size_t TR_SLOT_DOUBLES = (size_t)UC_TR_NS * TILE;
 constexpr size_t TR_SMEM = TR_WARPS * TR_SLOT_DOUBLES * sizeof(double);
-static_assert(TR_SMEM + 4096 <= 232448, "shared memory of the tile-resident update");
+static_assert(TR_SMEM + 8192 <= 232448, "shared memory of the tile-resident update");
 static_assert(UC_TR_NT * 2 <= 512 && UC_TR_NT % 16 == 0, "tensor-memory rows of the tile-resident update");
+static_assert(UC_TR_NT <= 256 && UC_TR_NS % 2 == 0 && UC_TR_NS / 2 <= 256 && UC_TR_NT <= UC_TR_NS,
+              "boxes of the tiled bulk copies (at most 256 rows each; the tensor-memory rows pass through the slot)");
+constexpr uint32_t TR_BOX_T = UC_TR_NT, TR_BOX_S = UC_TR_NS / 2;   // rows per box
 
 struct TrArgs {
     double *snap;          // [chunk - 1][TR_SNAP_ROWS][npad]
@@ -86,8 +93,20 @@ static_assert(UC_TR_SEG == 12, "UC_TR_WAIT_BANK names 2 x 12 registers");
 // FACES: the frozen transport terms are given (else they are zero, as in SOLVESP without faces);
 // LOCK: the warps of a block run each species of the program together (a barrier after each), so
 // that they fetch the program's instructions once instead of three times.
+// rows [y, y + box) of the RC plane for the 32 cells from x, into shared memory as [box][32]: one tiled bulk
+// copy through the plane's tensor map (no multicast), completion on the mbarrier
+__device__ __forceinline__ void tr_box_load(double *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
 template <bool FACES, bool LOCK>
-__global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdArgs a, const TrArgs t)
+__global__ void __launch_bounds__(TR_WARPS * 32, 1)
+update_tr_kernel(const UpdArgs a, const TrArgs t, const __grid_constant__ CUtensorMap map_t,
+                 const __grid_constant__ CUtensorMap map_s)
 {
     namespace cg = cooperative_groups;
     cg::grid_group grid = cg::this_grid();
@@ -139,11 +158,11 @@ __global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdAr
             __syncwarp();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_expect_tx(&s_bar[w], (uint32_t)(UC_TR_NT * TILE * sizeof(double)));
+            if (lane == 0) {
+                mbar_expect_tx(&s_bar[w], (uint32_t)(UC_TR_NT * TILE * sizeof(double)));
+                tr_box_load(slot, &map_t, tile * TILE, 0, &s_bar[w]);            // slots 0 .. NT-1
+            }
             __syncwarp();
-            for (int i = lane; i < UC_TR_NT; i += 32)
-                bulk_g2s(slot + (size_t)i * TILE, a.rc + (size_t)uc_tr_trow[i] * np + (size_t)tile * TILE,
-                         (uint32_t)(TILE * sizeof(double)), &s_bar[w]);
             if (!mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES)) {
                 if (lane == 0) atomicExch(t.status, ST_TMA_TIMEOUT);
                 mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES);   // let copies in flight land
@@ -163,11 +182,12 @@ __global__ void __launch_bounds__(TR_WARPS * 32, 1) update_tr_kernel(const UpdAr
             __syncwarp();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_expect_tx(&s_bar[w], (uint32_t)(UC_TR_NS * TILE * sizeof(double)));
+            if (lane == 0) {
+                mbar_expect_tx(&s_bar[w], (uint32_t)(UC_TR_NS * TILE * sizeof(double)));
+                tr_box_load(slot, &map_s, tile * TILE, UC_TR_NT, &s_bar[w]);     // slots NT .. NT+NS/2-1
+                tr_box_load(slot + (size_t)TR_BOX_S * TILE, &map_s, tile * TILE, UC_TR_NT + TR_BOX_S, &s_bar[w]);
+            }
             __syncwarp();
-            for (int i = lane; i < UC_TR_NS; i += 32)
-                bulk_g2s(slot + (size_t)i * TILE, a.rc + (size_t)uc_tr_srow[i] * np + (size_t)tile * TILE,
-                         (uint32_t)(TILE * sizeof(double)), &s_bar[w]);
             // ---- the cell's state (Y in registers)
             double yv[LSP], ysh[UC_IP_NSHADOW];
 #pragma unroll

@@ -318,9 +318,10 @@ def gen_tr_program(blocks, uses: dict, shadow: list[int]) -> str:
         ctx.updated.add(k)
     assert ctx.shadow == shadow, "the tile-resident and in-place programs must shadow the same species"
     tok = re.compile(r"@(\d+)@")
-    rows = sorted(uses, key=lambda r: (uses[r], r))
-    trow = sorted(rows[:TR_NTMEM])
-    srow = sorted(rows[TR_NTMEM:])
+    # by slot number: slots [0, TR_NTMEM) in tensor memory, the rest in shared memory, so that each
+    # part is one contiguous range of the RC plane's rows and is staged by a few tiled bulk copies
+    trow = list(range(TR_NTMEM))
+    srow = list(range(TR_NTMEM, LRX))
     tcol = {r: i for i, r in enumerate(trow)}
     scol = {r: i for i, r in enumerate(srow)}
     # segments: runs of statements with at most TR_SEG distinct tensor-memory rows
@@ -359,8 +360,8 @@ def gen_tr_program(blocks, uses: dict, shadow: list[int]) -> str:
     nld = sum(len(t) for _, t in segs)
     L = ["// Generated by unicorn_b200/mech/codegen.py: the in-place species-update program",
          "// (src/lib/solvesp.f:85-2806) for a tile whose RC block is held on chip.",
-         f"// RC rows: {len(trow)} in tensor memory (row i in columns 2i, 2i+1: low and high",
-         f"// word), {len(srow)} in shared memory. Requires RCS(i) (shared-memory row i of the",
+         f"// RC slots 0..{len(trow) - 1} in tensor memory (slot i in columns 2i, 2i+1: low and high",
+         f"// word), slots {len(trow)}..{LRX - 1} in shared memory. Requires RCS(i) (shared-memory row i of the",
          "// cell), TM_LD(bank, q, col) (load the double at column col into slot q of a",
          "// register bank), TM_WAIT(bank) (wait for the loads of that bank), RCT(bank, q),",
          "// UC_TR_PF(slot, k) (fetch Y0, FACE_SUM and FACE_NBR of species k into register slot 0",
