@@ -163,15 +163,6 @@ update_tr_kernel(const UpdArgs a, const TrArgs t, const __grid_constant__ CUtens
                 tr_box_load(slot, &map_t, tile * TILE, 0, &s_bar[w]);            // slots 0 .. NT-1
             }
             __syncwarp();
-            // the old level (and face) rows the passes read species by species: into L2 now, so that
-            // the first pass of the chunk does not wait on HBM at every species (two 128-byte lines
-            // per row and tile)
-            for (int i = lane; i < 2 * (LSP - 1); i += 32) {
-                const size_t off = (size_t)(i >> 1) * np + (size_t)tile * TILE + (size_t)(i & 1) * 16;
-                asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(a.y0 + off));
-                if (FACES && a.face_sum) asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(a.face_sum + off));
-                if (FACES && a.face_nbr) asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(a.face_nbr + off));
-            }
             if (!mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES)) {
                 if (lane == 0) atomicExch(t.status, ST_TMA_TIMEOUT);
                 mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES);   // let copies in flight land
