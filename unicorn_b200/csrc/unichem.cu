@@ -66,7 +66,8 @@ struct uc_ctx {
     int upd_grid = 0;
     int upd_ip = 0, ip_grid = 0;       // FP64 update with Y in place: warps per CTA (0: two Y sets, 8 warps)
     int upd_kind = 0;                  // 0: tile-resident (default), 1: Y in place per pass, 2: two Y sets per pass
-    int tr_chunk = 8;                  // tile-resident update: passes per chunk
+    int tr_chunk = 16;                 // tile-resident update: passes per chunk (1M cells, 100 passes:
+                                       // chunks of 4, 8, 16 took 234, 202, 182 ms)
     bool tr_lock = false;              // ... with the warps of a block in step species by species
                                        // (measured on 1M cells, 100 passes: 227 ms in step, 221 ms free)
     double *tr_snap = nullptr, *tr_partial = nullptr;
