@@ -801,7 +801,7 @@ def main_c5(args):
                 entry.update({"omega_err_mixed_p50": float(np.median(e_mx)), "omega_err_mixed_p99": float(np.quantile(e_mx, 0.99)),
                               "omega_mixed_frac_le_1e-3": round(float((e_mx <= 1e-3).mean()), 4),
                               "omega_err_mlp_p50": float(np.median(e_ml)), "omega_err_mlp_p99": float(np.quantile(e_ml, 0.99)),
-                              "mlp_tiles_exact_at_1e-3": round(fb["tiles_exact"], 4)})
+                              "mlp_cells_exact_at_1e-3": round(fb["cells_exact"], 4)})
                 rep[f"sweep_{sw}"] = entry
         timing[name] = {"ms_per_sweep": round(ms_total / args.sweeps, 3),
                         "cell_updates_per_s": round(n * args.sweeps / (ms_total / 1e3), 1)}

@@ -367,7 +367,7 @@ int uc_gemm_bf16(int device, int kernel, int M, int N, int K, const uint16_t *a,
  * weights and FP32 accumulation; inputs T, ln p and ln max(Y_k, 1e-12) scaled
  * by uc_mlp_set_norm, outputs asinh(QDSP_k / s_k) scaled likewise. Trained
  * with Adam on states whose targets the exact FP64 kernel computes, run with
- * a per-tile fallback to that kernel (uc_mlp_omega). All matrix products run
+ * a per-cell fallback to that kernel (uc_mlp_omega). All matrix products run
  * on the tensor cores (uc_gemm_bf16's kernel).
  */
 typedef struct uc_mlp uc_mlp;
@@ -382,16 +382,31 @@ int uc_mlp_set_norm(uc_mlp *mlp, const float *feat_mu, const float *feat_sd, con
                     const float *hull_hi, const float *tgt_mu, const float *tgt_sd, const float *tgt_scale);
 /* Append the context's cells (fields and uc_set_pressure pressures) with their exact omega. */
 int uc_mlp_add_data(uc_mlp *mlp, uc_ctx *ctx);
-/* Adam (beta 0.9/0.999, eps 1e-8) over `steps` batches; loss[steps] (may be NULL). batch % 64 == 0. */
+/* Adam (beta 0.9/0.999, eps 1e-8) over `steps` batches, the learning rate decaying from lr to lr/100
+ * along a half cosine over the call; loss[steps] (may be NULL). batch % 64 == 0. */
 int uc_mlp_train(uc_mlp *mlp, int steps, int batch, float lr, unsigned long long seed, float *loss);
 /* One forward+backward pass on given rows (M % 64 == 0): x [M][64] BF16 bits, t [M][64];
  * grad [nparams] and loss receive the mean-squared-error gradient and value. */
 int uc_mlp_grad(uc_mlp *mlp, int M, const uint16_t *x, const float *t, float *grad, float *loss);
 /* Omega of the context's state (its QDSP, as uc_omega leaves it) from the surrogate with
- * per-tile fallback to the exact FP64 kernel; stats[3]: fraction of tiles recomputed,
- * fraction of cells outside the training hull, median sampled residual. tol = +infinity
- * gives the network's output alone (no hull check, no fallback). */
+ * per-cell fallback to the exact FP64 kernel. A cell is recomputed exactly when it lies
+ * outside the training hull, or when the surrogate's omega breaks element conservation
+ * (max over C, H, O of |sum_k a_ek omega_k/W_k| / sum_k |a_ek omega_k/W_k|, which is 1e-16
+ * for the exact omega) by more than tol; every 32nd cell is recomputed as well, as a
+ * sample of the surrogate's true error. The flagged cells are gathered into a compact
+ * field, the exact kernel runs on it and the results go back to their cells. QDOT is
+ * written for the recomputed cells only. stats[3] (may be NULL; giving it synchronises):
+ * fraction of cells recomputed, fraction outside the training hull, median error of the
+ * surrogate on the sampled cells (max over species with Y_k > 1e-8 of the error relative to
+ * max(|omega_k|, 1e-6 max_j |omega_j|)). tol = +infinity gives the network's output alone
+ * (no checks, no fallback). */
 int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats);
+/* Statistics of the last uc_mlp_omega that was given stats: "cells_exact",
+ * "cells_outside_hull", "sample_error_p50", "sample_accepted" (fraction of the sampled
+ * cells the checks accepted), "sample_accepted_within_tol" (of those, the fraction whose
+ * true error is at most tol: the estimate for the accepted cells of the field),
+ * "sample_accepted_error_p50", "sample_accepted_error_p99". UC_E_ARG for another name. */
+int uc_mlp_stat(const uc_mlp *mlp, const char *name, double *value);
 const char *uc_mlp_last_error(const uc_mlp *mlp);
 void uc_mlp_destroy(uc_mlp *mlp);
 

@@ -175,6 +175,8 @@ struct AdamArgs {
     int n;
     float lr, b1, b2, eps;
     const int *step;             // steps done before this one
+    const int *iter;             // steps of this training call done before this one (null: constant lr)
+    int total;                   // steps of this training call: lr decays to lr/100 along a half cosine
     // BF16 copies of the weight matrices: layer l occupies w[woff[l] .. + out*in]
     __nv_bfloat16 *wb, *wbt;     // [out][in] and [in][out] per layer, flat with the same offsets
     int woff[MLP_LAYERS], wout[MLP_LAYERS], win[MLP_LAYERS], bfoff[MLP_LAYERS];
@@ -184,13 +186,18 @@ __global__ void adam_kernel(const AdamArgs a)
 {
     const int t = *a.step + 1;
     const float c1 = 1.0f - powf(a.b1, (float)t), c2 = 1.0f - powf(a.b2, (float)t);
+    float lr = a.lr;
+    if (a.iter && a.total > 1) {
+        const float f = (float)*a.iter / (float)(a.total - 1);
+        lr = 0.01f * a.lr + 0.5f * 0.99f * a.lr * (1.0f + cospif(f));
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         const float g = a.g[i];
         const float m = a.b1 * a.m[i] + (1.0f - a.b1) * g;
         const float v = a.b2 * a.v[i] + (1.0f - a.b2) * g * g;
         a.m[i] = m;
         a.v[i] = v;
-        const float w = a.w[i] - a.lr * (m / c1) / (sqrtf(v / c2) + a.eps);
+        const float w = a.w[i] - lr * (m / c1) / (sqrtf(v / c2) + a.eps);
         a.w[i] = w;
         for (int l = 0; l < MLP_LAYERS; ++l) {
             const int rel = i - a.woff[l];
@@ -209,56 +216,92 @@ __global__ void step_incr_kernel(int *step)
     if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
 }
 
-// Sampled residual check: one cell per 32-cell tile of the field (position
-// tile*32 + (hash(tile) & 31), clamped to n-1) is gathered into a compact
-// field; after the exact omega of the compact field, each tile's flag is set
-// if the surrogate's relative error on that cell exceeds tol over the species
-// with Y_k > 1e-8 (relative to max(|w_k|, 1e-6 max_j |w_j|)), or if any of its
-// cells lies outside the training hull.
-__device__ __forceinline__ int sample_pos(int tile, int n)
+// Per-cell checks of the surrogate's omega. A cell falls back to the exact FP64
+// kernel when it lies outside the training hull, or when the surrogate's omega
+// breaks element conservation by more than the tolerance: every reaction of the
+// mechanism conserves C, H and O, so the exact omega satisfies
+// sum_k a_ek omega_k / W_k = 0 to rounding (1e-16 of sum_k |a_ek omega_k / W_k|),
+// while the network's errors show up in that residual cell by cell. Every 32nd
+// cell (position `off` within each group of 32) is recomputed as well, as a
+// sample of the surrogate's true error: its prediction is kept (pred_s) and
+// whether the checks accepted it (pass_s). Flagged cells are appended to `list`.
+__global__ void mlp_cell_check_kernel(const DevParams *Pp, const double *qdsp, const int *outside, int n, int npad,
+                                      double tol, int off, int *list, int *count, double *pred_s, int *pass_s)
 {
-    unsigned h = (unsigned)tile * 2654435761u;
-    h ^= h >> 15;
-    const int p = tile * 32 + (int)(h & 31u);
-    return p < n ? p : n - 1;
-}
-
-__global__ void sample_gather_kernel(const double *tk, const double *rho, const double *y, const double *soot,
-                                     int npad, int n, int ntile, double *stk, double *srho, double *sy, double *ssoot,
-                                     int snpad)
-{
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < snpad; t += gridDim.x * blockDim.x) {
-        const int p = sample_pos(t < ntile ? t : ntile - 1, n);
-        stk[t] = tk[p];
-        srho[t] = rho[p];
-        for (int k = 0; k < LSP; ++k) sy[(size_t)k * snpad + t] = y[(size_t)k * npad + p];
-        ssoot[t] = soot[p];
-        ssoot[snpad + t] = soot[npad + p];
+    const DevParams &P = *Pp;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        double num[3] = {0.0, 0.0, 0.0}, den[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < LSP; ++k) {
+            const double f = qdsp[(size_t)k * npad + c] / P.WM[k];
+            for (int e = 0; e < 3; ++e) {
+                const double t = (double)P.elem[k * 3 + e] * f;
+                num[e] += t;
+                den[e] += fabs(t);
+            }
+        }
+        double r = 0.0;
+        for (int e = 0; e < 3; ++e)
+            if (den[e] > 0.0) r = fmax(r, fabs(num[e]) / den[e]);
+        const bool ok = !outside[c] && r <= tol;           // NaN fails
+        const bool sample = (c & 31) == off;
+        if (sample) {
+            const int sidx = c >> 5;
+            for (int k = 0; k < LSP; ++k) pred_s[(size_t)sidx * LSP + k] = qdsp[(size_t)k * npad + c];
+            pass_s[sidx] = ok ? 1 : 0;
+        }
+        if (!ok || sample) list[atomicAdd(count, 1)] = c;
     }
 }
 
-__global__ void residual_flag_kernel(const double *qdsp_pred, const double *y, int npad, int n, int ntile,
-                                     const double *sq_exact, int snpad, const int *outside, double tol, int *tile_flag,
-                                     double *tile_resid)
+// The flagged cells as a compact field (cell t of the compact field is list[t]; the padding of the last
+// 32-cell tile repeats the last flagged cell) and the tile list the exact kernel walks.
+__global__ void mlp_gather_cells_kernel(const int *list, const int *count, const double *tk, const double *rho,
+                                        const double *y, const double *soot, int npad, double *stk, double *srho,
+                                        double *sy, double *ssoot, int snpad, int *tlist, int *tcount)
 {
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntile; t += gridDim.x * blockDim.x) {
-        const int p = sample_pos(t, n);
+    const int cnt = *count, m = (cnt + 31) & ~31;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        const int c = list[t < cnt ? t : cnt - 1];
+        stk[t] = tk[c];
+        srho[t] = rho[c];
+        for (int k = 0; k < LSP; ++k) sy[(size_t)k * snpad + t] = y[(size_t)k * npad + c];
+        ssoot[t] = soot[c];
+        ssoot[snpad + t] = soot[npad + c];
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m / 32; i += gridDim.x * blockDim.x) tlist[i] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *tcount = m / 32;
+}
+
+// exact omega of the compact field back to the flagged cells
+__global__ void mlp_scatter_cells_kernel(const int *list, const int *count, const double *sq, const double *sqd,
+                                         int snpad, double *qdsp, double *qdot, int npad)
+{
+    const int cnt = *count;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+        const int c = list[t];
+        for (int k = 0; k < LSP; ++k) qdsp[(size_t)k * npad + c] = sq[(size_t)k * snpad + t];
+        if (qdot) qdot[c] = sqd[t];
+    }
+}
+
+// the surrogate's error on each sampled cell: max over species with Y_k > 1e-8 of
+// |predicted - exact| / max(|exact|, 1e-6 max_j |exact_j|); -1 for positions beyond n
+__global__ void mlp_sample_error_kernel(const double *pred_s, const double *qdsp, const double *y, int n, int npad,
+                                        int off, int ns, double *err_s)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < ns; s += gridDim.x * blockDim.x) {
+        const int c = s * 32 + off;
+        if (c >= n) { err_s[s] = -1.0; continue; }
         double wmax = 0.0;
-        for (int k = 0; k < LSP; ++k) wmax = fmax(wmax, fabs(sq_exact[(size_t)k * snpad + t]));
+        for (int k = 0; k < LSP; ++k) wmax = fmax(wmax, fabs(qdsp[(size_t)k * npad + c]));
         double r = 0.0;
         for (int k = 0; k < LSP; ++k) {
-            if (!(y[(size_t)k * npad + p] > 1e-8)) continue;
-            const double e = sq_exact[(size_t)k * snpad + t];
-            const double d = fabs(qdsp_pred[(size_t)k * npad + p] - e) / fmax(fabs(e), 1e-6 * wmax + 1e-300);
+            if (!(y[(size_t)k * npad + c] > 1e-8)) continue;
+            const double e = qdsp[(size_t)k * npad + c];
+            const double d = fabs(pred_s[(size_t)s * LSP + k] - e) / fmax(fabs(e), 1e-6 * wmax + 1e-300);
             r = fmax(r, d != d ? 1e300 : d);
         }
-        int out = 0;
-        for (int i = 0; i < 32; ++i) {
-            const int c = t * 32 + i;
-            if (c < n) out |= outside[c];
-        }
-        tile_resid[t] = r;
-        tile_flag[t] = (out || !(r <= tol)) ? 1 : 0;
+        err_s[s] = r;
     }
 }
 

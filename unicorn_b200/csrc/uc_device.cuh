@@ -46,6 +46,7 @@ struct DevParams {
     double TSTR, RSTR, WMSTR, ALSTR, VSTR, HSTR, GASC, PBACK, CONVRC, CONVRM, CONVRD;
     double C1ST, C2ND, C3RD, RCONV, HCONVR, TKDMIN, RSTR_WMSTR, BETA1, BETA3, REI;
     double WM[LSP], HFO[LSP];
+    int8_t elem[LSP * 3];                 // atoms of C, H, O per species
     double poly[LSP * 14];
     double om22[LSP * 12];
     double cdia[LSP];

@@ -231,6 +231,7 @@ static void build_params(const uc_inputs &in, DevParams &P, std::vector<PairTab>
         P.cdia[k] = uc_cdia[k];
     }
     memcpy(P.poly, uc_poly, sizeof(P.poly));
+    memcpy(P.elem, uc_elem_cho, sizeof(P.elem));
     memcpy(P.om22, uc_om22, sizeof(P.om22));
     memcpy(P.ci11, uc_ci11, sizeof(P.ci11));
     for (int i = 0; i < LSP; ++i)       // main:471-483
@@ -1995,9 +1996,12 @@ struct uc_mlp {
     long icap = 0;
     __nv_bfloat16 *IX = nullptr, *IH0 = nullptr, *IH1 = nullptr;
     float *IOut = nullptr;
-    int *outside = nullptr, *tflag = nullptr, *tlist = nullptr, *tcount = nullptr;
-    double *tresid = nullptr;
-    uc_ctx *sample = nullptr;      // compact field of the sampled cells
+    int *outside = nullptr, *list = nullptr, *count = nullptr, *tlist = nullptr, *tcount = nullptr, *pass_s = nullptr;
+    double *pred_s = nullptr, *err_s = nullptr;
+    uc_ctx *sample = nullptr;      // compact field of the cells recomputed exactly
+    unsigned ncall = 0;
+    // statistics of the last uc_mlp_omega with statistics (uc_mlp_stat)
+    double st_exact = 0, st_outside = 0, st_sample_med = 0, st_acc = 0, st_acc_ok = 0, st_acc_p50 = 0, st_acc_p99 = 0;
     int *status = nullptr;
     char err[256] = {0};
 };
@@ -2269,11 +2273,12 @@ static int mlp_enqueue_fwd_bwd(uc_mlp *mlp, int B, float *loss_hist)
     return UC_OK;
 }
 
-static int mlp_enqueue_adam(uc_mlp *mlp, float lr)
+static int mlp_enqueue_adam(uc_mlp *mlp, float lr, int total)
 {
     AdamArgs a{};
     a.w = mlp->w; a.g = mlp->g; a.m = mlp->m; a.v = mlp->v; a.n = mlp->np;
     a.lr = lr; a.b1 = 0.9f; a.b2 = 0.999f; a.eps = 1e-8f; a.step = mlp->d_t;
+    a.iter = mlp->d_iter; a.total = total;
     a.wb = mlp->wb; a.wbt = mlp->wbt;
     for (int l = 0; l < MLP_LAYERS; ++l) {
         a.woff[l] = mlp->woff[l]; a.wout[l] = mlp->out[l]; a.win[l] = mlp->in[l]; a.bfoff[l] = mlp->bfoff[l];
@@ -2283,7 +2288,8 @@ static int mlp_enqueue_adam(uc_mlp *mlp, float lr)
     return UC_OK;
 }
 
-// Adam training (lr, beta 0.9/0.999, eps 1e-8) for `steps` batches of `batch`
+// Adam training (beta 0.9/0.999, eps 1e-8; the learning rate starts at lr and
+// decays to lr/100 along a half cosine over the call's steps) for `steps` batches of `batch`
 // rows drawn without replacement from the training set (reshuffled every
 // pass over it, generator seeded by `seed`). The whole step is one CUDA graph.
 // loss (host [steps], may be NULL) receives each batch's mean squared error.
@@ -2329,7 +2335,7 @@ extern "C" int uc_mlp_train(uc_mlp *mlp, int steps, int batch, float lr, unsigne
         mlp_gather_kernel<<<256, 256, 0, mlp->stream>>>(mlp->Xall, mlp->Tall, mlp->idx, mlp->d_iter, batch, mlp->H[0], mlp->T);
         int rc = cudaGetLastError() == cudaSuccess ? UC_OK : mlp_err(mlp, UC_E_CUDA, "gather launch");
         if (rc == UC_OK) rc = mlp_enqueue_fwd_bwd(mlp, batch, mlp->loss_hist);
-        if (rc == UC_OK) rc = mlp_enqueue_adam(mlp, lr);
+        if (rc == UC_OK) rc = mlp_enqueue_adam(mlp, lr, steps);
         if (rc == UC_OK) {
             step_incr_kernel<<<1, 32, 0, mlp->stream>>>(mlp->d_iter);
             step_incr_kernel<<<1, 32, 0, mlp->stream>>>(mlp->d_t);
@@ -2389,19 +2395,21 @@ extern "C" int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats)
     if (!ctx->have_fields || !ctx->pnd) return mlp_err(mlp, UC_E_STATE, "the context needs fields and pressures");
     if (ctx->device != mlp->device) return mlp_err(mlp, UC_E_ARG, "context and surrogate on different devices");
     CK(cudaSetDevice(ctx->device));
-    const int n = ctx->n, np = ctx->npad, nt = ctx->ntile;
+    const int n = ctx->n, np = ctx->npad, nt = ctx->ntile, ns = (n + 31) / 32;
     int rc;
     if (mlp->icap < np) {
         if (mlp->icap) return mlp_err(mlp, UC_E_ARG, "a larger field than the first one used");
         if ((rc = mlp_alloc(mlp, &mlp->IX, (size_t)np * MLP_IN)) || (rc = mlp_alloc(mlp, &mlp->IH0, (size_t)np * MLP_H)) ||
             (rc = mlp_alloc(mlp, &mlp->IH1, (size_t)np * MLP_H)) || (rc = mlp_alloc(mlp, &mlp->IOut, (size_t)np * MLP_OUT)) ||
-            (rc = mlp_alloc(mlp, &mlp->outside, (size_t)np)) || (rc = mlp_alloc(mlp, &mlp->tflag, (size_t)nt)) ||
-            (rc = mlp_alloc(mlp, &mlp->tlist, (size_t)nt)) || (rc = mlp_alloc(mlp, &mlp->tcount, 1)) ||
-            (rc = mlp_alloc(mlp, &mlp->tresid, (size_t)nt)))
+            (rc = mlp_alloc(mlp, &mlp->outside, (size_t)np)) || (rc = mlp_alloc(mlp, &mlp->list, (size_t)np)) ||
+            (rc = mlp_alloc(mlp, &mlp->count, 1)) || (rc = mlp_alloc(mlp, &mlp->tlist, (size_t)nt)) ||
+            (rc = mlp_alloc(mlp, &mlp->tcount, 1)) || (rc = mlp_alloc(mlp, &mlp->pass_s, (size_t)ns)) ||
+            (rc = mlp_alloc(mlp, &mlp->pred_s, (size_t)ns * LSP)) || (rc = mlp_alloc(mlp, &mlp->err_s, (size_t)ns)))
             return rc;
         mlp->icap = np;
-        if ((rc = uc_init(&ctx->inputs, nt, ctx->device, &mlp->sample)) != UC_OK)
-            return mlp_err(mlp, rc, "set-up of the sampled-cell field failed");
+        // the compact field of the cells recomputed exactly: at most every cell of the field
+        if ((rc = uc_init(&ctx->inputs, n, ctx->device, &mlp->sample)) != UC_OK)
+            return mlp_err(mlp, rc, "set-up of the compact field of the recomputed cells failed");
     }
     RET_IF(dalloc(ctx, &ctx->qdsp, (size_t)LSP * np));
     cudaStream_t st = ctx->stream;
@@ -2419,64 +2427,96 @@ extern "C" int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats)
     }
     mlp_decode_kernel<<<grid, 256, 0, st>>>(mlp->dnorm, mlp->IOut, np, ctx->qdsp, np, 0);
     CK(cudaGetLastError());
-    if (std::isinf(tol)) {          // the network alone: no hull check, no fallback
+    if (std::isinf(tol)) {          // the network alone: no checks, no fallback
         if (stats) {
             CK(cudaStreamSynchronize(st));
             stats[0] = stats[1] = stats[2] = 0.0;
         }
         return UC_OK;
     }
-    // exact omega of one sampled cell per tile
+    // per-cell checks; the flagged and the sampled cells recomputed by the exact kernel
+    const int off = (int)((mlp->ncall++ * 7u + 3u) & 31u);
+    CK(cudaMemsetAsync(mlp->count, 0, sizeof(int), st));
+    mlp_cell_check_kernel<<<grid, 256, 0, st>>>(ctx->dP, ctx->qdsp, mlp->outside, n, np, tol, off, mlp->list,
+                                                 mlp->count, mlp->pred_s, mlp->pass_s);
+    CK(cudaGetLastError());
     uc_ctx *S = mlp->sample;
-    sample_gather_kernel<<<(S->npad + 255) / 256, 256, 0, st>>>(ctx->tk, ctx->rho, ctx->y, ctx->soot, np, n, nt, S->tk,
-                                                                 S->rho, S->y, S->soot, S->npad);
+    mlp_gather_cells_kernel<<<grid, 256, 0, st>>>(mlp->list, mlp->count, ctx->tk, ctx->rho, ctx->y, ctx->soot, np,
+                                                   S->tk, S->rho, S->y, S->soot, S->npad, mlp->tlist, mlp->tcount);
     CK(cudaGetLastError());
-    cudaEvent_t ev;
-    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    CK(cudaEventRecord(ev, st));
-    CK(cudaStreamWaitEvent(S->stream, ev, 0));
-    S->have_fields = true;
-    RET_IF(launch_chem(S, UC_FP64, false, true));
-    CK(cudaEventRecord(ev, S->stream));
-    CK(cudaStreamWaitEvent(st, ev, 0));
-    cudaEventDestroy(ev);
-    residual_flag_kernel<<<(nt + 255) / 256, 256, 0, st>>>(ctx->qdsp, ctx->y, np, n, nt, S->qdsp, S->npad, mlp->outside,
-                                                           tol, mlp->tflag, mlp->tresid);
-    CK(cudaGetLastError());
-    // exact FP64 omega for the flagged tiles
-    compact_tiles_kernel<<<1, 1024, 0, st>>>(mlp->tflag, nt, mlp->tlist, mlp->tcount);
-    CK(cudaGetLastError());
+    RET_IF(dalloc(S, &S->qdsp, (size_t)LSP * S->npad));
+    RET_IF(dalloc(S, &S->qdot, S->npad));
     ChemArgs c{};
     c.P = ctx->dP; c.tab = ctx->dTab;
-    c.tk = ctx->tk; c.rho = ctx->rho; c.y = ctx->y; c.stmf = ctx->soot; c.stnd = ctx->soot + np;
-    c.qdsp = ctx->qdsp;
-    c.n = n; c.npad = np; c.ntile = nt; c.status = ctx->status;
+    c.tk = S->tk; c.rho = S->rho; c.y = S->y; c.stmf = S->soot; c.stnd = S->soot + S->npad;
+    c.qdsp = S->qdsp; c.qdot = S->qdot;
+    c.n = S->n; c.npad = S->npad; c.ntile = S->ntile; c.status = ctx->status;
     c.tile_list = mlp->tlist; c.tile_count = mlp->tcount;
     int slot;
     prof_begin(ctx, UC_K_CHEM, slot);
-    chem_fp64_kernel<<<std::min(nt, ctx->nsm), CHEM_THREADS, CHEM_SMEM, st>>>(c);
+    chem_fp64_kernel<<<std::min(S->ntile, ctx->nsm), CHEM_THREADS, CHEM_SMEM, st>>>(c);
     prof_end(ctx, slot);
     CK(cudaGetLastError());
+    mlp_scatter_cells_kernel<<<grid, 256, 0, st>>>(mlp->list, mlp->count, S->qdsp, S->qdot, S->npad, ctx->qdsp,
+                                                    ctx->qdot, np);
+    CK(cudaGetLastError());
     if (stats) {
+        mlp_sample_error_kernel<<<(ns + 255) / 256, 256, 0, st>>>(mlp->pred_s, ctx->qdsp, ctx->y, n, np, off, ns,
+                                                                    mlp->err_s);
+        CK(cudaGetLastError());
         int cnt = 0;
-        std::vector<int> outs(n);
-        std::vector<double> res(nt);
-        CK(cudaMemcpyAsync(&cnt, mlp->tcount, sizeof(int), cudaMemcpyDeviceToHost, st));
+        std::vector<int> outs(n), pass(ns);
+        std::vector<double> err(ns);
+        CK(cudaMemcpyAsync(&cnt, mlp->count, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(outs.data(), mlp->outside, n * sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(res.data(), mlp->tresid, nt * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(pass.data(), mlp->pass_s, ns * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(err.data(), mlp->err_s, ns * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         long no = 0;
         for (int v : outs) no += v;
-        std::nth_element(res.begin(), res.begin() + nt / 2, res.end());
-        stats[0] = (double)cnt / nt;
-        stats[1] = (double)no / n;
-        stats[2] = res[nt / 2];
+        std::vector<double> all, acc;
+        for (int i = 0; i < ns; ++i) {
+            if (err[i] < 0.0) continue;
+            all.push_back(err[i]);
+            if (pass[i]) acc.push_back(err[i]);
+        }
+        auto quant = [](std::vector<double> v, double q) {
+            if (v.empty()) return 0.0;
+            const size_t k = std::min(v.size() - 1, (size_t)(q * (double)(v.size() - 1) + 0.5));
+            std::nth_element(v.begin(), v.begin() + k, v.end());
+            return v[k];
+        };
+        long ok = 0;
+        for (double e : acc) ok += e <= tol;
+        mlp->st_exact = (double)cnt / n;
+        mlp->st_outside = (double)no / n;
+        mlp->st_sample_med = quant(all, 0.5);
+        mlp->st_acc = all.empty() ? 0.0 : (double)acc.size() / all.size();
+        mlp->st_acc_ok = acc.empty() ? 1.0 : (double)ok / acc.size();
+        mlp->st_acc_p50 = quant(acc, 0.5);
+        mlp->st_acc_p99 = quant(acc, 0.99);
+        stats[0] = mlp->st_exact;
+        stats[1] = mlp->st_outside;
+        stats[2] = mlp->st_sample_med;
     }
     int s2 = 0;
     CK(cudaMemcpyAsync(&s2, mlp->status, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (s2 == ST_MMA_TIMEOUT) return set_err(ctx, UC_E_TIMEOUT, "a tensor-core wait timed out");
     return UC_OK;
+}
+
+extern "C" int uc_mlp_stat(const uc_mlp *mlp, const char *name, double *value)
+{
+    if (!mlp || !name || !value) return UC_E_ARG;
+    const struct { const char *k; double v; } t[] = {
+        {"cells_exact", mlp->st_exact}, {"cells_outside_hull", mlp->st_outside},
+        {"sample_error_p50", mlp->st_sample_med}, {"sample_accepted", mlp->st_acc},
+        {"sample_accepted_within_tol", mlp->st_acc_ok}, {"sample_accepted_error_p50", mlp->st_acc_p50},
+        {"sample_accepted_error_p99", mlp->st_acc_p99}};
+    for (auto &e : t)
+        if (!strcmp(name, e.k)) { *value = e.v; return UC_OK; }
+    return UC_E_ARG;
 }
 
 extern "C" const char *uc_mlp_last_error(const uc_mlp *mlp) { return mlp ? mlp->err : "null surrogate"; }
@@ -2490,7 +2530,8 @@ extern "C" void uc_mlp_destroy(uc_mlp *mlp)
     if (mlp->train_graph) cudaGraphDestroy(mlp->train_graph);
     void *bufs[] = {mlp->dnorm, mlp->w, mlp->g, mlp->m, mlp->v, mlp->wb, mlp->wbt, mlp->Xall, mlp->Tall,
                     mlp->d_iter, mlp->d_t, mlp->idx, mlp->loss_hist, mlp->IX, mlp->IH0, mlp->IH1, mlp->IOut,
-                    mlp->outside, mlp->tflag, mlp->tlist, mlp->tcount, mlp->tresid, mlp->status};
+                    mlp->outside, mlp->list, mlp->count, mlp->tlist, mlp->tcount, mlp->pass_s, mlp->pred_s,
+                    mlp->err_s, mlp->status};
     for (void *b : bufs)
         if (b) cudaFree(b);
     mlp_free_batch(mlp);

@@ -403,6 +403,20 @@ def arr(name, ctype, vals, per_line=8) -> str:
     return f"static const {ctype} {name}[{len(vals)}] = {{\n" + ",\n".join(rows) + "\n};\n"
 
 
+def element_counts(names) -> list[list[int]]:
+    import re
+    out = []
+    for nm in names:
+        base = re.sub(r"^[A-Z]-", "", nm)
+        c = {"C": 0, "H": 0, "O": 0}
+        if base not in ("AR", "HE", "N2"):
+            assert re.fullmatch(r"([CHO]\d*)+", base), nm
+            for el, cnt in re.findall(r"([CHO])(\d*)", base):
+                c[el] += int(cnt) if cnt else 1
+        out.append([c["C"], c["H"], c["O"]])
+    return out
+
+
 def gen_tables(mech: dict) -> str:
     R = mech["reactions"]
     out = ["// Generated by unicorn_b200/mech/codegen.py from sandiego52.json (the",
@@ -412,6 +426,9 @@ def gen_tables(mech: dict) -> str:
            f"#define UC_LSP {LSP}", f"#define UC_LRX {LRX}", f"#define UC_NPAIR {LRX // 2}",
            f"#define UC_TPOL1 {fmt(mech['tpol'][0])}", f"#define UC_TPOL2 {fmt(mech['tpol'][1])}"]
     out.append(arr("uc_wsp", "double", map(fmt, mech["wsp"])))
+    # atoms of C, H and O per species, read from the species names (T-, S-, I-, N- are isomer prefixes;
+    # AR, HE and N2 carry none of the three): every reaction conserves them, so the exact omega does
+    out.append(arr("uc_elem_cho", "int8_t", (str(v) for row in element_counts(mech["species"]) for v in row), 3))
     out.append(arr("uc_cdia", "double", map(fmt, mech["cdia"])))
     out.append(arr("uc_tlj", "double", map(fmt, mech["tlj"])))
     out.append(arr("uc_poly", "double", (fmt(v) for row in mech["poly"] for v in row)))

@@ -3,7 +3,7 @@
 A 54 -> 256 x 4 (GELU) -> 52 network: inputs T, ln(p/PREF) and ln max(Y_k,
 1e-12), standardised; outputs asinh(QDSP_k / s_k), standardised (QDSP is the
 reference's -omega). Trained with Adam on states whose omega the exact FP64
-kernel computes; evaluated with a per-tile fallback to that kernel.
+kernel computes; evaluated with a per-cell fallback to that kernel.
 """
 from __future__ import annotations
 
@@ -35,6 +35,7 @@ def _lib():
         L.uc_mlp_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_ulonglong, F]
         L.uc_mlp_grad.argtypes = [vp, ctypes.c_int, U16, F, F, F]
         L.uc_mlp_omega.argtypes = [vp, vp, ctypes.c_double, D]
+        L.uc_mlp_stat.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
         L.uc_mlp_last_error.argtypes = [vp]
         L.uc_mlp_last_error.restype = ctypes.c_char_p
         L.uc_mlp_destroy.argtypes = [vp]
@@ -131,11 +132,17 @@ class Surrogate:
 
     # ------------------------------------------------------------ inference
     def omega(self, u: "unichem.UniChem", tol: float = 1e-3, stats: bool = True):
-        """QDSP of u's state into u's device outputs; returns the fallback statistics
-        (which cost a synchronisation and a copy), or None with stats=False."""
+        """QDSP of u's state into u's device outputs, with per-cell fallback to the exact kernel;
+        returns the fallback statistics (which cost a synchronisation and copies), or None."""
         if not stats:
             self._ck(self.lib.uc_mlp_omega(self._h, u._h, tol, None))
             return None
         st = np.zeros(3)
         self._ck(self.lib.uc_mlp_omega(self._h, u._h, tol, st.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
-        return {"tiles_exact": float(st[0]), "cells_outside_hull": float(st[1]), "median_residual": float(st[2])}
+        out = {}
+        for k in ("cells_exact", "cells_outside_hull", "sample_error_p50", "sample_accepted",
+                  "sample_accepted_within_tol", "sample_accepted_error_p50", "sample_accepted_error_p99"):
+            v = ctypes.c_double(0.0)
+            self._ck(self.lib.uc_mlp_stat(self._h, k.encode(), ctypes.byref(v)))
+            out[k] = v.value
+        return out
