@@ -2398,7 +2398,18 @@ extern "C" int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats)
     const int n = ctx->n, np = ctx->npad, nt = ctx->ntile, ns = (n + 31) / 32;
     int rc;
     if (mlp->icap < np) {
-        if (mlp->icap) return mlp_err(mlp, UC_E_ARG, "a larger field than the first one used");
+        // grown to the largest field seen (the buffers of a smaller one are released first)
+        CK(cudaStreamSynchronize(ctx->stream));
+        void *old[] = {mlp->IX, mlp->IH0, mlp->IH1, mlp->IOut, mlp->outside, mlp->list, mlp->count, mlp->tlist,
+                       mlp->tcount, mlp->pass_s, mlp->pred_s, mlp->err_s};
+        for (void *b : old)
+            if (b) cudaFree(b);
+        mlp->IX = mlp->IH0 = mlp->IH1 = nullptr;
+        mlp->IOut = nullptr;
+        mlp->outside = mlp->list = mlp->count = mlp->tlist = mlp->tcount = mlp->pass_s = nullptr;
+        mlp->pred_s = mlp->err_s = nullptr;
+        if (mlp->sample) { uc_destroy(mlp->sample); mlp->sample = nullptr; }
+        mlp->icap = 0;
         if ((rc = mlp_alloc(mlp, &mlp->IX, (size_t)np * MLP_IN)) || (rc = mlp_alloc(mlp, &mlp->IH0, (size_t)np * MLP_H)) ||
             (rc = mlp_alloc(mlp, &mlp->IH1, (size_t)np * MLP_H)) || (rc = mlp_alloc(mlp, &mlp->IOut, (size_t)np * MLP_OUT)) ||
             (rc = mlp_alloc(mlp, &mlp->outside, (size_t)np)) || (rc = mlp_alloc(mlp, &mlp->list, (size_t)np)) ||
