@@ -216,7 +216,9 @@ int uc_assemble_faces(uc_ctx *ctx, double dt, double *e, double *w, double *n, d
  * passes receives ISOR2 as the reference returns it (the converging pass, or
  * isor + 1); resdh = sum|FPZ - HT| / hnorm. At most 1024 interior rows (lj - 2).
  * Returns UC_E_NOCONV (not fatal) when a cell's Newton did not converge and
- * UC_E_TIMEOUT when a bounded wait between passes gave up. */
+ * UC_E_TIMEOUT when a bounded wait between passes gave up (T and HT are then
+ * left unchanged); the waits give up after the number of nanoseconds in the
+ * environment variable UNICHEM_RELAX_WAIT_NS, read at each call (2 s when unset). */
 typedef struct {
     double dt;      /* DT */
     int isor;       /* ISOR2: passes at most */

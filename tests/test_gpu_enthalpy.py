@@ -275,3 +275,28 @@ def test_relax_full_c2_grid(cuda, oracle):
     nb = ze[c] * F[2:, 1:-1] + zw[c] * F[:-2, 1:-1] + zn[c] * F[1:-1, 2:] + zs[c] * F[1:-1, :-2]
     res = np.abs(ppp * F[c] - (rhsz[c] - nb)) / (np.abs(rhsz[c]) + np.abs(ppp * F[c]) + 1e-300)
     assert np.median(res) < 1e-9 and res.max() < 1e-6, (np.median(res), res.max())
+
+
+def test_relaxation_wait_limit_gives_up_cleanly(cuda, oracle, monkeypatch):
+    """Failure detection without a fault: with the wait limit between relaxation passes set to zero the
+    passes give up at their first wait, the call reports UC_E_TIMEOUT and leaves T and HT as they were;
+    the context stays usable and the next call (default limit) succeeds."""
+    g = enthalpy_case(oracle, LJ, LI, 5)
+    n = LJ * LI
+    ht = consistent_ht(oracle, g)
+    with cuda.UniChem(n) as u:
+        u.upload(g["tk"], g["rho"], g["y"], stmf=g["stmf"])
+        u.set_grid(LJ, LI, g["xxs"], g["xxc"], g["yys"], g["yyc"], g["yr"], isym=1)
+        u.set_flow(g["u"], g["v"], g["tmu"], 0.9)
+        u.set_enthalpy(ht)
+        u.sweep(1e-7, isor=4, tol=0.0)
+        tk0 = u.download()[0]
+        monkeypatch.setenv("UNICHEM_RELAX_WAIT_NS", "0")
+        with pytest.raises(cuda.UniChemError) as ei:
+            u.enthalpy_update(1e-7, isor=50, relx=0.99, tol=-1.0, sigh=0.9)
+        assert ei.value.code == -4
+        assert np.array_equal(u.download()[0], tk0)
+        assert np.array_equal(u.enthalpy_get()[0], ht)
+        monkeypatch.delenv("UNICHEM_RELAX_WAIT_NS")
+        passes, _ = u.enthalpy_update(1e-7, isor=50, relx=0.99, tol=-1.0, sigh=0.9)
+        assert passes == 51

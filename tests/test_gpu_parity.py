@@ -212,3 +212,45 @@ def test_errors_are_reported(cuda):
     with pytest.raises(ValueError):
         u.upload(np.ones(7), np.ones(8), np.ones((52, 8)))
     u.close()
+
+
+def test_soot_sources_and_update_with_soot(cuda, oracle):
+    """Non-zero soot (STMF, STND): the soot source terms of ckrates.f:1337-1352 enter the rate kernel's
+    SOUR and the species update of H2, O2, H, O, OH, CO and C2H2 and the two soot scalars
+    (solvesp.f:415,529,697,851,1005,1343-1344,1969, 2807-2832)."""
+    tk, rho, y = random_state(oracle, 3000, 17, 900, 2600)
+    rng = np.random.default_rng(17)
+    stmf = rng.uniform(0.0, 1e-3, 3000)
+    stnd = 10 ** rng.uniform(-1, 14, 3000)
+    with cuda.UniChem(3000) as u:
+        u.upload(tk, rho, y, stmf, stnd)
+        rc = u.ckrates(return_rc=True)
+        passes = u.solvesp(1e-3, isor=4, relx=0.99, tol=0.0)
+        _, _, yg, s1, s2 = u.download()
+    rc_o, sour_o = oracle.rates(tk, rho, y, stmf, stnd)
+    assert np.abs(sour_o[2:5]).max() > 0                      # the surface-growth and oxidation terms are live
+    assert_rel(rc, rc_o, RTOL, 1e-300, "RC with soot")
+    yo, so, po = oracle.species_update(rho, y, rc_o, sour_o, 1e-3, isor=4, tol=0.0,
+                                       soot0=np.vstack([stmf, stnd]))
+    assert passes == po
+    assert_rel(yg, yo, 1e-9, 1e-18, "Y with soot sources")
+    assert_rel(s1, so[0], 1e-9, 1e-30, "soot mass fraction")
+    assert_rel(s2, so[1], 1e-9, 1e-30, "soot number density")
+
+
+def test_c2_slice_sweep_converged(cuda, oracle):
+    """The FP64 sweep with the reference's card settings (isor 100, relaxation 0.99, tolerance 1e-8) on
+    2,056 cells of the 601x301 heptane field (every 88th): the pass count the reference reports and Y."""
+    f = jet_field(601, 301, fuel=11, t_peak=2300.0, seed=0)
+    sel = np.arange(0, f.n, 88)
+    tk, rho = nondimensional(f, oracle.scales, oracle.wm)
+    tk, rho, y = tk[sel].copy(), rho[sel].copy(), np.ascontiguousarray(f.y[:, sel])
+    with cuda.UniChem(len(sel)) as u:
+        u.upload(tk, rho, y)
+        passes = u.sweep(1e-3, isor=100, relx=0.99, tol=1e-8)
+        _, _, yg, _, _ = u.download()
+    yc = oracle.props(tk, y)[0]
+    rc, sour = oracle.rates(tk, rho, yc)
+    yo, _, po = oracle.species_update(rho, yc, rc, sour, 1e-3, isor=100, relx=0.99, tol=1e-8)
+    assert passes == po
+    assert_rel(yg, yo, 1e-9, 1e-18, "Y after the converged C2 sweep")

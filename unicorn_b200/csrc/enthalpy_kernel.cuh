@@ -312,6 +312,10 @@ __device__ __noinline__ int relax_wait(const int *flag, int need, int p, int *st
             __threadfence();
             return v;
         }
+        if (timeout_ns <= 0) {                  // a limit of zero: no waiting at all
+            atomicCAS(status, ST_OK, ST_RELAX_TIMEOUT);
+            return -1;
+        }
         if ((it & 15) == 15) {
             if (ld_acquire(status) != ST_OK || ld_acquire(stop_at) < p) return -1;
             if (gtimer() - t0 > timeout_ns) {

@@ -1340,7 +1340,9 @@ static int launch_relax(uc_ctx *ctx, cudaStream_t st, int nsm, RelaxBuffers &rb,
     a.progress = progress; a.done = done; a.stop_at = stop; a.status = status;
     a.isor = isor; a.R = R;
     a.sor1 = relx; a.sor2 = (double)1.0f - relx; a.tol = tol; a.hnorm = hnorm;
+    // the bounded waits between passes give up after UNICHEM_RELAX_WAIT_NS nanoseconds of wall clock (2 s)
     a.timeout_ns = 2000000000LL;
+    if (const char *e = getenv("UNICHEM_RELAX_WAIT_NS")) a.timeout_ns = std::max(0LL, atoll(e));
     const int threads = (nj + 31) / 32 * 32;
     const size_t smem = 3 * (size_t)nj * sizeof(double);
     int per_sm = 0;
@@ -2442,6 +2444,8 @@ extern "C" int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats)
         if (stats) {
             CK(cudaStreamSynchronize(st));
             stats[0] = stats[1] = stats[2] = 0.0;
+            mlp->st_exact = mlp->st_outside = mlp->st_sample_med = mlp->st_acc = mlp->st_acc_p50 = mlp->st_acc_p99 = 0.0;
+            mlp->st_acc_ok = 0.0;
         }
         return UC_OK;
     }
