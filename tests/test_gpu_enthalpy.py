@@ -298,5 +298,6 @@ def test_relaxation_wait_limit_gives_up_cleanly(cuda, oracle, monkeypatch):
         assert np.array_equal(u.download()[0], tk0)
         assert np.array_equal(u.enthalpy_get()[0], ht)
         monkeypatch.delenv("UNICHEM_RELAX_WAIT_NS")
+        u.sweep(1e-7, isor=4, tol=0.0)                    # an enthalpy update follows a species sweep
         passes, _ = u.enthalpy_update(1e-7, isor=50, relx=0.99, tol=-1.0, sigh=0.9)
         assert passes == 51
