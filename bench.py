@@ -225,19 +225,58 @@ def time_calls(fn, ext, reps, warmup):
     return e0.elapsed_time(e1) / reps
 
 
-def roofline(kt, n, passes_run, pk):
-    """Dominant kernel of the FP64 sweep and its achieved rate against the measured HBM copy bandwidth."""
+def fp64_fma_peak(dev):
+    """FP64 FMA throughput of this GPU, measured: an elementwise kernel of four independent chains of 256
+    fused multiply-adds per element over 2^26 doubles (torch's jiterator compiles it), best of 5, CUDA
+    events. TFLOP/s, counting an FMA as two operations; None if the kernel cannot be built."""
+    try:
+        import torch
+        code = ("template <typename T> T fma_loop(T x, T a, T b) {"
+                " T y0 = x, y1 = x + T(1), y2 = x + T(2), y3 = x + T(3);"
+                " for (int i = 0; i < 256; ++i) { y0 = y0 * a + b; y1 = y1 * a + b; y2 = y2 * a + b; y3 = y3 * a + b; }"
+                " return y0 + y1 + y2 + y3; }")
+        fn = torch.cuda.jiterator._create_jit_fn(code)
+        x = torch.rand(1 << 26, dtype=torch.float64, device=dev)
+        a = torch.full_like(x, 0.999)
+        b = torch.full_like(x, 1e-3)
+        fn(x, a, b)
+        torch.cuda.synchronize(dev)
+        best = None
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn(x, a, b)
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        return (1 << 26) * 4 * 256 * 2 / (best / 1e3) / 1e12
+    except Exception:
+        return None
+
+
+# DRAM read + write of one launch of the tile-resident update under ncu (65,536 cells of the benchmark
+# field, 16 passes: 367 MB + 412 MB), per cell and pass; scaled to a launch by cells x passes run
+UPDATE_DRAM_PER_CELL_PASS = (367.4e6 + 412.3e6) / (65536 * 16)
+
+
+def roofline(kt, n, passes_run, pk, flops_per_cell_pass, fp64_peak):
+    """Dominant kernel of the FP64 sweep and its achieved rate against its bound: the species update
+    holds each tile's RC block on chip across passes and is bound by the FP64 pipe, the others by HBM."""
     name = max(kt, key=lambda k: kt[k][0])
     ms, cnt = kt[name]
-    traffic = None
     if name == "update":
-        per_cell = passes_run * (544 + 52 + 52 + 6 + 2 + 2) * 8 + (52 + 2) * 8
-        rule = (f"per cell and launch: {passes_run:.1f} passes x (RC 544 + Y 52 in + 52 out + SOUR 6 + soot 4) x 8 B "
-                "+ the closure's 54 x 8 B")
-        # DRAM read + write of one launch of the FP64 update under ncu (65,536 C2 cells, 5 passes:
-        # 3.723 GB + 0.193 GB), per cell and pass, scaled to this launch by cells x passes run
-        traffic = round(11951.0 * n * passes_run)
-    elif name == "chem":
+        flops = flops_per_cell_pass * passes_run * n
+        achieved = flops / (ms / cnt / 1e3) / 1e12
+        peak = fp64_peak if fp64_peak else 37.0
+        return {"kernel": name, "bound": "fp64", "achieved": round(achieved, 3), "peak": round(peak, 2),
+                "peak_source": "measured in this run: FP64 FMA loop (bench.py fp64_fma_peak)" if fp64_peak else
+                "nominal B200 FP64 (the measurement did not run)", "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 4), "traffic": round(UPDATE_DRAM_PER_CELL_PASS * n * passes_run),
+                "flops_per_launch": flops, "avg_launch_ms": round(ms / cnt, 4),
+                "flops_rule": f"{flops_per_cell_pass} operations per cell and pass (each multiplication, addition "
+                              f"and division of the update program one) x {passes_run:.1f} passes x {n} cells"}
+    if name == "chem":
         per_cell = (52 + 4) * 8 + (544 + 52 + 52 + 1 + 6) * 8
         rule = "per cell: read T, rho, soot, Y (56 x 8 B); write RC 544, QDSP 52, dw/dY 52, QDOT, SOUR 6"
     else:
@@ -246,7 +285,7 @@ def roofline(kt, n, passes_run, pk):
     achieved = per_cell * n / (ms / cnt / 1e3) / 1e9
     return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
             "peak_source": pk["source"], "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
-            "traffic": traffic, "bytes_per_launch": per_cell * n, "avg_launch_ms": round(ms / cnt, 4),
+            "traffic": None, "bytes_per_launch": per_cell * n, "avg_launch_ms": round(ms / cnt, 4),
             "bytes_rule": rule}
 
 
@@ -497,7 +536,7 @@ def main_ours(args):
                 "e2e": {"value": round(world * n * args.steps / e2e_s, 1), "unit": UNIT,
                         "h2d_bytes_per_step": (2 + 52) * 8 * n, "d2h_bytes_per_step": (52 * 4 + 5) * 8 * n},
                 "gpu_launches": world * sum(c for _, c in kt.values()), "clocks": clk.summary(),
-                "roofline": roofline(kt, n, passes_run, pk),
+                "roofline": roofline(kt, n, passes_run, pk, u.stat("update_flops_per_cell_pass"), fp64_fma_peak(dev)),
                 "kernel_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in kt.items() if v[1]}}
     # ---------------- the three forms and the C2 field (rank 0 of a one-GPU run)
     if rank == 0 and world == 1:
@@ -616,6 +655,8 @@ def main_c3(args):
     u.sync()
     e2e = time.perf_counter() - t0
     u.close()
+    fp64_m = fp64_fma_peak(0)
+    fp64 = fp64_m or 37.0
     substeps = float(ns.sum())
     per_sub_flop = 9.0e3 + 470 + 2 * 2189 * float(pa.sum()) / substeps
     achieved = per_sub_flop * substeps / (ms / args.steps / 1e3) / 1e12
@@ -636,9 +677,10 @@ def main_c3(args):
                     "d2h_bytes_per_step": (2 + 52) * 8 * n},
             "gpu_launches": kt["integrate"][1] * (6 if tune["int_sorted"] else 3),
             "clocks": clk.summary(),
-            "roofline": {"kernel": "integrate", "bound": "fp64", "achieved": round(achieved, 3), "peak": 37.0,
-                         "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)", "unit": "TFLOP/s",
-                         "frac": round(achieved / 37.0, 4), "traffic": None,
+            "roofline": {"kernel": "integrate", "bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64, 2),
+                         "peak_source": "measured in this run: FP64 FMA loop (bench.py fp64_fma_peak)" if fp64_m else
+                         "nominal B200 FP64 (the measurement did not run)", "unit": "TFLOP/s",
+                         "frac": round(achieved / fp64, 4), "traffic": None,
                          "flops_rule": "per cell and sub-step: 9e3 rate flops + 470 transcendentals (1 op each) + "
                                        "2 flops x 2189 update terms x passes"}}
     if not args.no_cpu_baseline:

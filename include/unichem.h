@@ -282,6 +282,14 @@ int uc_profile_read(uc_ctx *ctx, double *ms, int *launches);
  *   "tiles"               32-cell tiles of the context
  *   "mixed_fp64_tiles"    tiles the last UC_MIXED rate call sent to FP64 because a
  *                         rate left the FP32 range
+ *   "update_kind"         species update kernel: 0 tile-resident (default; RC on chip
+ *                         across chunks of passes), 1 per pass with Y in place
+ *                         (UNICHEM_UPDATE=inplace), 2 per pass with two Y sets
+ *                         (UNICHEM_UPDATE=twoset), chosen at uc_init
+ *   "update_chunk"        passes per chunk of the tile-resident update (UNICHEM_TR_CHUNK, 16)
+ *   "update_lockstep"     1 if its warps run species by species in step (UNICHEM_TR_LOCKSTEP)
+ *   "update_flops_per_cell_pass"  floating-point operations of one cell and pass of the
+ *                         update (each multiplication, addition and division one)
  *   "update_ip_warps"     warps per CTA of the species update with Y in place
  *                         (14); 0 when UNICHEM_UPDATE=twoset was set at uc_init and
  *                         the two-Y-set kernel (8 warps) runs instead

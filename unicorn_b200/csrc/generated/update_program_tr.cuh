@@ -14,6 +14,7 @@
 #define UC_TR_NT 256
 #define UC_TR_NS 288
 #define UC_TR_SEG 12
+#define UC_UPDATE_FLOPS_PER_CELL_PASS 6261
 #define UC_TR_SHADOW_SAVE() do { YOS(0) = YO(2); YOS(1) = YO(4); YOS(2) = YO(6); YOS(3) = YO(13); YOS(4) = YO(16); YOS(5) = YO(14); YOS(6) = YO(8); YOS(7) = YO(22); } while (0)
 #define UC_UPDATE_PROGRAM_TR() do { \
     double prod = 0.0, extra, loss, rhs1, rhs2, ppp, fnew; \

@@ -275,30 +275,33 @@ struct CpHArgs {
     int n, npad;
 };
 
-// R = double: the drop-in form; R = float: polynomials and the species sums in FP32
+// cp and h of each cell from the coefficient tables of DevParams (the polynomials of
+// spgsolv.f:102-173 and solveh.f:39-57 with the divisions by W_k, by the powers' orders and
+// the scale factors folded in at set-up), in Horner form: a few fused multiply-adds per
+// species, so the kernel is bound by reading the 52 Y rows (the table form rounds differently
+// from the reference's expression by a few units in the last place). The sums over species
+// keep the reference's order.
 template <typename R>
 __global__ void __launch_bounds__(256) cp_h_kernel(const CpHArgs a)
 {
     const DevParams &P = *a.P;
     const size_t np = a.npad;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < (size_t)a.n; c += (size_t)gridDim.x * blockDim.x) {
-        const double TKDd = a.tk[c] * P.TSTR;
-        const R TKD = (R)TKDd;
-        const R TKD2 = TKD * TKD, TKD3 = TKD * TKD2, TKD4 = TKD * TKD3, TKD5 = TKD * TKD4;
-        const int ip = TKDd > UC_TPOL1 ? 7 : 0;
-        R TCP = 0, hs = 0;
+        const double T = a.tk[c] * P.TSTR;
+        const int r = T > UC_TPOL1 ? 1 : 0;
+        double TCP = 0.0, hs = 0.0;
+#pragma unroll 4
         for (int k = 0; k < LSP; ++k) {
-            const double *p = P.poly + k * 14 + ip;
-            const R yk = (R)a.y[k * np + c];
-            const R t = ((R)p[0] + (R)p[1] * TKD + (R)p[2] * TKD2 + (R)p[3] * TKD3 + (R)p[4] * TKD4) / (R)P.WM[k];
-            TCP = TCP + t * yk;
-            const R HSSP = ((R)p[0] * TKD + (R)p[1] * TKD2 / (R)2 + (R)p[2] * TKD3 / (R)3 + (R)p[3] * TKD4 / (R)4 +
-                            (R)p[4] * TKD5 / (R)5) / (R)P.WM[k] * (R)P.HCONVR;
-            const R H = HSSP * (R)P.WMSTR * (R)P.HSTR + (R)p[5] / (R)P.WM[k] * (R)P.GASC;
-            hs = hs + yk * H;
+            const double yk = a.y[k * np + c];
+            const double *q = P.cpc + (k * 2 + r) * 5;
+            const double *e = P.hc + (k * 2 + r) * 6;
+            const double cpk = fma(fma(fma(fma(q[4], T, q[3]), T, q[2]), T, q[1]), T, q[0]);
+            const double hk = fma(T * fma(fma(fma(fma(e[4], T, e[3]), T, e[2]), T, e[1]), T, e[0]), 1.0, e[5]);
+            TCP = TCP + cpk * yk;
+            hs = hs + yk * hk;
         }
-        if (a.cp) a.cp[c] = (double)(TCP / (R)P.WMSTR * (R)P.GASC * (R)P.TSTR / (R)P.HSTR);
-        if (a.h) a.h[c] = (double)hs;
+        if (a.cp) a.cp[c] = TCP / P.WMSTR * P.GASC * P.TSTR / P.HSTR;
+        if (a.h) a.h[c] = hs;
     }
 }
 

@@ -54,6 +54,9 @@ struct DevParams {
     double WMIK[LSP * LSP], DWMIK[LSP * LSP], WMCD[LSP * LSP];
     double ETLJ1[LSP * LSP], ETLJ2[LSP * LSP], ETLJ3[LSP * LSP], ETLJ4[LSP * LSP];
     double RETLJ1[LSP * LSP];             // 1 / ETLJ1 (the mixed form's collision-integral argument)
+    // cp/R / W and h of every species as polynomials in T for Horner evaluation, per temperature range
+    // (0: T <= TPOL1, 1: above): cp_k / W_k = sum_i cpc[i] T^i, h_k = T (sum_i hc[i] T^i) + hc[5]
+    double cpc[LSP * 2 * 5], hc[LSP * 2 * 6];
     // third-body groups 1..10 (TBODY + sum sign*coef*Y/W)
     int16_t tb_off[11], tb_len[11];
     int8_t tb_sp[64], tb_sign[64], tb_hascoef[64];

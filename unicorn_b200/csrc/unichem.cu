@@ -232,6 +232,16 @@ static void build_params(const uc_inputs &in, DevParams &P, std::vector<PairTab>
     }
     memcpy(P.poly, uc_poly, sizeof(P.poly));
     memcpy(P.elem, uc_elem_cho, sizeof(P.elem));
+    for (int k = 0; k < LSP; ++k)      // spgsolv.f:102-173 and solveh.f:39-57 as coefficient tables
+        for (int r = 0; r < 2; ++r) {
+            const double *p = uc_poly + k * 14 + 7 * r;
+            const double hs = P.HCONVR * P.WMSTR * P.HSTR / P.WM[k];
+            for (int i = 0; i < 5; ++i) {
+                P.cpc[(k * 2 + r) * 5 + i] = p[i] / P.WM[k];
+                P.hc[(k * 2 + r) * 6 + i] = p[i] / (double)(i + 1) * hs;
+            }
+            P.hc[(k * 2 + r) * 6 + 5] = p[5] / P.WM[k] * P.GASC;
+        }
     memcpy(P.om22, uc_om22, sizeof(P.om22));
     memcpy(P.ci11, uc_ci11, sizeof(P.ci11));
     for (int i = 0; i < LSP; ++i)       // main:471-483
@@ -1156,6 +1166,7 @@ extern "C" int uc_stat(uc_ctx *ctx, const char *name, double *value)
     if (!strcmp(name, "update_kind")) { *value = ctx->upd_kind; return UC_OK; }
     if (!strcmp(name, "update_chunk")) { *value = ctx->tr_chunk; return UC_OK; }
     if (!strcmp(name, "update_lockstep")) { *value = ctx->tr_lock; return UC_OK; }
+    if (!strcmp(name, "update_flops_per_cell_pass")) { *value = UC_UPDATE_FLOPS_PER_CELL_PASS; return UC_OK; }
     if (!strcmp(name, "int_sorted")) { *value = ctx->int_sorted; return UC_OK; }
     if (!strcmp(name, "int_tune_best_ms")) { *value = ctx->tune_best; return UC_OK; }
     if (!strcmp(name, "int_tune_worst_ms")) { *value = ctx->tune_worst; return UC_OK; }

@@ -358,6 +358,14 @@ def gen_tr_program(blocks, uses: dict, shadow: list[int]) -> str:
         if si + 1 < len(segs):
             out.append(f"TM_WAIT({(si + 1) % 2});")
     nld = sum(len(t) for _, t in segs)
+
+    def muls(t):
+        return 1 + muls(t.a) + muls(t.b) if isinstance(t, Mul) else 0
+    # floating-point operations per cell and pass: the multiplications of each term and its addition
+    # into the sum, and the 16 of each species' closing statements (rhs1 5, rhs2 2, ppp 1, fnew 6 with
+    # the division as one, the residual 2); the two soot scalars 19
+    flops = sum(muls(t) + 1 for b in blocks for key in ("prod", "extra", "loss") for _, t in (b[key] or [])) + \
+        16 * len(blocks) + 19
     L = ["// Generated by unicorn_b200/mech/codegen.py: the in-place species-update program",
          "// (src/lib/solvesp.f:85-2806) for a tile whose RC block is held on chip.",
          f"// RC slots 0..{len(trow) - 1} in tensor memory (slot i in columns 2i, 2i+1: low and high",
@@ -374,6 +382,7 @@ def gen_tr_program(blocks, uses: dict, shadow: list[int]) -> str:
          f"#define UC_TR_NT {len(trow)}",
          f"#define UC_TR_NS {len(srow)}",
          f"#define UC_TR_SEG {TR_SEG}",
+         f"#define UC_UPDATE_FLOPS_PER_CELL_PASS {flops}",
          "#define UC_TR_SHADOW_SAVE() do { " + " ".join(f"YOS({m}) = YO({k});" for m, k in enumerate(shadow)) + " } while (0)",
          "#define UC_UPDATE_PROGRAM_TR() do { \\",
          "    double prod = 0.0, extra, loss, rhs1, rhs2, ppp, fnew; \\"]
