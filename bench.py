@@ -619,7 +619,7 @@ def main_c3(args):
     from unicorn_b200.fields import batch_cells, nondimensional
     n = args.cells or C3_CELLS
     f = batch_cells(n, seed=0)
-    prec = unichem.FP64
+    prec = unichem.MIXED if args.precision == "mixed" else unichem.FP64
     opts = dict(isor=args.isor, relx=RELX, tol=TOL)
     u = unichem.UniChem(n)
     tk, rho = nondimensional(f, u.scales, u.wm)
@@ -663,11 +663,12 @@ def main_c3(args):
     line = {"metric": "batched stiff integration cell-updates/s (one cell over dt = 1e-5 s)",
             "value": round(n * args.steps / (ms / 1e3), 1), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded C3 generator)",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == unichem.FP64 else "f32 rates / f64 update", "data": "synthetic (seeded C3 generator)",
             "config": {"workload": f"C3: {n} independent heptane-generator cells, T~U[300,2400] K, p~U[0.8,1.2] atm, "
                                    "dt=1e-5 s, n_sub=clamp(ceil(max_k dt|w_k|/Y_k over Y_k>1e-3), 1, 200), "
                                    f"update passes to 1e-8 per sub-step (<={args.isor})",
-                       "cells": n, "precision": "fp64", "tuned": tune,
+                       "cells": n, "precision": args.precision, "tuned": tune,
                        "nsub": {"mean": round(float(ns.mean()), 2), "min": int(ns.min()), "max": int(ns.max()),
                                 "frac_1": round(float((ns == 1).mean()), 4),
                                 "frac_max": round(float((ns == ns.max()).mean()), 4)},

@@ -334,7 +334,10 @@ int uc_device_view_get(uc_ctx *ctx, uc_device_view *v);
  * the graph is captured on the first call and again when an option or the
  * tuned kernel shape changes.
  *
- * precision: UC_FP64 (everything FP64); other values return UC_E_ARG.
+ * precision: UC_FP64 (everything FP64) or UC_MIXED (the rates of every
+ * sub-step and of the start state in the mixed form of uc_rates, stored as
+ * doubles; a tile with a rate beyond the FP32 range is recomputed in FP64; the
+ * update, closure, T and rho stay FP64); other values return UC_E_ARG.
  */
 typedef struct {
     double dt;          /* non-dimensional step (DT = 1e-3 is 1e-5 s) */

@@ -65,7 +65,9 @@ def test_integrate_matches_oracle(cuda, oracle, c3):
     T1, To = tk1 * sc["TSTR"], tk_o * sc["TSTR"]
     lo, hi = sc["TSTR"] - 1.0 + 1e-6, 5000.0 - 1e-6
     ok = (T1 > lo) & (T1 < hi) & (To > lo) & (To < hi)
-    assert ok.mean() > 0.8
+    print(f"\ncells on the T clamp (not compared): device {(~((T1 > lo) & (T1 < hi))).sum()}, "
+          f"oracle {(~((To > lo) & (To < hi))).sum()}, either {(~ok).sum()} of {len(ok)}")
+    assert (~ok).sum() <= 17                       # observed: 16 of 333 (4.8 %) on the oracle
     assert np.abs(T1 - To)[ok].max() < 1e-2
     err = np.abs(y1 - y_o) - (1e-6 * np.abs(y_o) + 1e-12)
     assert (err[:, ok] <= 0).all(), f"worst Y excess {err[:, ok].max():.3g}"
@@ -94,7 +96,35 @@ def test_integrate_options_rejected(cuda):
             with pytest.raises(cuda.UniChemError):
                 u.integrate(DT, **bad)
         with pytest.raises(cuda.UniChemError):
-            u.integrate(DT, precision=cuda.MIXED)
+            u.integrate(DT, precision=7)
         u.integrate(DT, nsub_max=1)               # default pressure PBACK
         ns, _ = u.integrate_counts()
         assert (ns == 1).all()
+
+
+def test_mixed_rates_against_the_fp64_form(cuda, oracle):
+    """FP32 rates with the FP64 update against the all-FP64 form, on 4,096 cells of the C3 distribution:
+    sub-step counts (from the mixed or the FP64 omega of the start state), Y and T after dt. The stated
+    accuracy of the mixed form is 1e-3 on omega; the states after up to 200 sub-steps are compared at
+    1e-3 relative on Y above 1e-8 and 1 K on T, with the cells on the T clamp and those whose sub-step
+    count differs counted, not compared."""
+    f = batch_cells(4096, seed=12)
+    tk, rho = nondimensional(f, oracle.scales, oracle.wm)
+    pnd = f.p / oracle.scales["PSTR"]
+    a = run_gpu(cuda, f, tk, rho, pnd)
+    b = run_gpu(cuda, f, tk, rho, pnd, precision=cuda.MIXED)
+    sc = oracle.scales
+    (T64, Tmx) = (a[0] * sc["TSTR"], b[0] * sc["TSTR"])
+    lo, hi = sc["TSTR"] - 1.0 + 1e-6, 5000.0 - 1e-6
+    same_ns = a[4] == b[4]
+    ok = same_ns & (T64 > lo) & (T64 < hi) & (Tmx > lo) & (Tmx < hi)
+    y64, ymx = a[2], b[2]
+    big = y64 > 1e-8
+    rel = np.where(big, np.abs(ymx - y64) / np.maximum(y64, 1e-300), 0.0).max(axis=0)
+    print(f"\nmixed vs FP64 integration: sub-step counts equal {same_ns.mean():.4f}; compared {ok.sum()} of 4096; "
+          f"Y rel err max {rel[ok].max():.2e}, p99 {np.quantile(rel[ok], 0.99):.2e}; "
+          f"|dT| max {np.abs(Tmx - T64)[ok].max():.2e} K")
+    assert same_ns.mean() > 0.99
+    assert ok.mean() > 0.9
+    assert rel[ok].max() <= 1e-3
+    assert np.abs(Tmx - T64)[ok].max() <= 1.0

@@ -54,30 +54,15 @@ __device__ __forceinline__ double gibbs_exp(const double *a, double ELOGT, doubl
     return exp(g0);
 }
 
-// Phases 1a-2 of a tile: Gibbs functions, third bodies, soot sources and
-// the RC plane of the tile in shared memory, with NW warps (NW divides 16:
-// a warp takes the pair lists of the virtual warps w, w+NW, ...). Expects the
-// tile's Y rows in sY and the scalar rows of sC; writes sRC and sG, and the
-// six soot sources to sour[m*sstride + soff] when sour is not null. Ends
-// before the barrier that publishes sRC.
+// Phases 1b-1c of a tile: TBODY from the Y/W rows left in sRC by phase 1a, the
+// third-body groups TB001..TB010 and the soot sources (ckrates.f:643-731,
+// 1337-1352). Ends with the barrier that publishes them.
 template <int NW>
-__device__ __forceinline__ void tile_rates_fp64(const DevParams &P, const PairTab *sTab, double *sRC,
-                                                const double *sY, double *sG, double *sC, double *sour,
-                                                size_t sstride, size_t soff, int lane, int warp,
-                                                bool keep_sour = false)
+__device__ __forceinline__ void tile_tb_soot(const DevParams &P, const double *sRC, const double *sY, double *sC,
+                                             double *sour, size_t sstride, size_t soff, int lane, int warp,
+                                             bool keep_sour)
 {
-    const double C1ST = P.C1ST, C2ND = P.C2ND, C3RD = P.C3RD;
-    // ---------------- phase 1a: Gibbs functions; Y/W rows (scratch in sRC)
-    {
-        const double TKD = sC[SC_TKD * TILE + lane];
-        const double ELOGT = sC[SC_LNT * TILE + lane];
-        const int ip = TKD > UC_TPOL1 ? 7 : 0;
-        for (int k = warp; k < LSP; k += NW) {
-            sG[k * TILE + lane] = gibbs_exp(P.poly + k * 14 + ip, ELOGT, TKD);
-            sRC[k * TILE + lane] = sY[k * TILE + lane] / P.WM[k];
-        }
-    }
-    __syncthreads();
+    const double C1ST = P.C1ST;
     // ---------------- phase 1b: TBODY (ordered sum)
     if (warp == 0) {
         double tb = sRC[lane];
@@ -118,6 +103,33 @@ __device__ __forceinline__ void tile_rates_fp64(const DevParams &P, const PairTa
         }
     }
     __syncthreads();
+}
+
+// Phases 1a-2 of a tile: Gibbs functions, third bodies, soot sources and
+// the RC plane of the tile in shared memory, with NW warps (NW divides 16:
+// a warp takes the pair lists of the virtual warps w, w+NW, ...). Expects the
+// tile's Y rows in sY and the scalar rows of sC; writes sRC and sG, and the
+// six soot sources to sour[m*sstride + soff] when sour is not null. Ends
+// before the barrier that publishes sRC.
+template <int NW>
+__device__ __forceinline__ void tile_rates_fp64(const DevParams &P, const PairTab *sTab, double *sRC,
+                                                const double *sY, double *sG, double *sC, double *sour,
+                                                size_t sstride, size_t soff, int lane, int warp,
+                                                bool keep_sour = false)
+{
+    const double C1ST = P.C1ST, C2ND = P.C2ND, C3RD = P.C3RD;
+    // ---------------- phase 1a: Gibbs functions; Y/W rows (scratch in sRC)
+    {
+        const double TKD = sC[SC_TKD * TILE + lane];
+        const double ELOGT = sC[SC_LNT * TILE + lane];
+        const int ip = TKD > UC_TPOL1 ? 7 : 0;
+        for (int k = warp; k < LSP; k += NW) {
+            sG[k * TILE + lane] = gibbs_exp(P.poly + k * 14 + ip, ELOGT, TKD);
+            sRC[k * TILE + lane] = sY[k * TILE + lane] / P.WM[k];
+        }
+    }
+    __syncthreads();
+    tile_tb_soot<NW>(P, sRC, sY, sC, sour, sstride, soff, lane, warp, keep_sour);
     // ---------------- phase 2: reaction pairs -> RC plane
     {
         const double TKD = sC[SC_TKD * TILE + lane];

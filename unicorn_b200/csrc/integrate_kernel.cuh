@@ -1,4 +1,4 @@
-// Batched stiff point-implicit integration of independent cells (FP64).
+// Batched stiff point-implicit integration of independent cells (FP64, or FP32 rates with the FP64 update).
 //
 // Each cell is advanced over dt by n_sub sub-steps of dt/n_sub; every
 // sub-step is the reference's own chain for a one-cell field: the rate
@@ -22,13 +22,104 @@
 // memory.
 #pragma once
 #include "chem_kernel.cuh"
+#include "chem_mixed_kernel.cuh"
 #include "generated/update_program.cuh"
 
 namespace uc {
 
+// The rate coefficients of a tile in the mixed form of chem_mixed_kernel (FP64
+// Gibbs exponents, ln Kc and exponent assembly; FP32 exponentials, fall-off
+// blend and RC products), stored as doubles in sRC so that the FP64 update reads
+// them unchanged; third bodies and soot sources as in the FP64 form. Reads the
+// scalar rows of sC (SC_*), uses sG as scratch for the Gibbs exponents and the
+// mixed pair table in global memory. Returns, uniformly over the block, whether
+// a rate of the tile left the FP32 range (the caller then recomputes the tile
+// in FP64).
+template <int NW>
+__device__ bool tile_rates_mixed(const DevParams &P, const PairTabM *tabm, double *sRC, const double *sY, double *sG,
+                                 double *sC, double *sour, size_t sstride, size_t soff, int lane, int warp)
+{
+    {   // phase 1a: Gibbs exponents (FP64) and the Y/W rows
+        const double TKD = sC[SC_TKD * TILE + lane], ELOGT = sC[SC_LNT * TILE + lane];
+        const double IT = 1.0 / TKD;
+        const int ip = TKD > UC_TPOL1 ? 7 : 0;
+        const double T1 = TKD * 0.5, T2 = TKD * TKD * (1.0 / 6.0), T3 = T1 * T2, T4 = 1.2 * T1 * T3;
+        for (int k = warp; k < LSP; k += NW) {
+            const double *c = P.poly + k * 14 + ip;
+            sG[k * TILE + lane] = c[0] * (ELOGT - 1.0) + c[1] * T1 + c[2] * T2 + c[3] * T3 + c[4] * T4 - c[5] * IT + c[6];
+            sRC[k * TILE + lane] = sY[k * TILE + lane] / P.WM[k];
+        }
+    }
+    __syncthreads();
+    tile_tb_soot<NW>(P, sRC, sY, sC, sour, sstride, soff, lane, warp, false);
+    bool out = false;
+    {   // phase 2: reaction pairs -> RC (FP32 arithmetic, stored as doubles)
+        const double TKD = sC[SC_TKD * TILE + lane], ELOGT = sC[SC_LNT * TILE + lane], IT = 1.0 / TKD;
+        const double LNRHO = log(sC[SC_RHO * TILE + lane]), LNRUT = log(sC[SC_RUT * TILE + lane]);
+        const double LNDMOLEA = log(sC[SC_DMOLEA * TILE + lane]);
+        const float TKDf = (float)TKD;
+        for (int vw = warp; vw < CHEM_WARPS; vw += NW)
+        for (int i = 0; i < P.npair_of_warp[vw]; ++i) {
+            const int p = P.pair_of_warp[vw][i];
+            const PairTabM &T = tabm[p];
+            const double lnkf = T.lnakf + T.alf * ELOGT - T.exaf * IT;
+            double lnkr = -1.0e300;
+            if (T.has_rev) {
+                double lnq = 0.0;
+                for (int t = 0; t < T.qlen; ++t) lnq += T.qsgn[t] * sG[T.qsp[t] * TILE + lane];
+                lnkr = lnkf + T.rut * LNRUT - lnq;
+            }
+            double lafp = 0.0;
+            if (T.falloff) {
+                const double l20 = -46.051701859880914;      // ln 1e-20 (ckrates.f:770)
+                const double lden = lnkf > l20 ? lnkf + log1p(exp(l20 - lnkf)) : l20 + log1p(exp(lnkf - l20));
+                const double lnk0m = T.lnaklow + T.allow * ELOGT - T.ealow * IT +
+                                     log(sC[(SC_TB0 + T.dmole) * TILE + lane]) + LNDMOLEA - lden;
+                float RFACT;
+                if (T.troe[0] > 0.0f) {
+                    float FCLOG;
+                    if (T.troe[1] == 0.0f) FCLOG = log10f(T.troe[0]);
+                    else FCLOG = log10f((1.0f - T.troe[0]) * expf(-(TKDf / T.troe[1])) +
+                                        T.troe[0] * expf(-(TKDf / T.troe[2])) + expf(-(T.troe[3] / TKDf)));
+                    const float CPLOG = (float)(lnk0m * 0.43429448190325176) - (0.4f + 0.67f * FCLOG);
+                    const float z = CPLOG / (0.75f - 1.27f * FCLOG - 0.14f * CPLOG);
+                    RFACT = exp10f(FCLOG / (1.0f + z * z));
+                } else if (T.troe[0] == 0.0f) {
+                    RFACT = 1.0f;
+                } else {
+                    const float l = (float)(lnk0m * 0.43429448190325176);
+                    const float XFACT = 1.0f / (1.0f + l * l);
+                    RFACT = powf(-(T.troe[0] * expf(-(T.troe[1] / TKDf))) + expf(-(TKDf / T.troe[2])), XFACT);
+                }
+                lafp = (double)logf(RFACT) - (lnk0m > 0.0 ? log1p(exp(-lnk0m)) : log1p(exp(lnk0m)) - lnk0m);
+            }
+            float rc0 = 0.0f, rc1 = 0.0f;
+            const double e0 = lnkf + lafp + T.lnc0 + T.order0 * LNRHO;
+            const double e1 = lnkr + lafp + T.lnc1 + T.order1 * LNRHO;
+            if ((T.order0 && e0 > 85.0) || (T.order1 && T.has_rev && e1 > 85.0)) out = true;
+            if (T.order0) {
+                float v = exp_split(e0);
+                if (T.tb0 >= 0) v *= (float)sC[(SC_TB0 + T.tb0) * TILE + lane];
+                for (int t = 0; t < T.ny0; ++t) v *= (float)sY[T.yk0[t] * TILE + lane];
+                rc0 = v;
+            }
+            if (T.order1 && T.has_rev) {
+                float v = exp_split(e1);
+                if (T.tb1 >= 0) v *= (float)sC[(SC_TB0 + T.tb1) * TILE + lane];
+                for (int t = 0; t < T.ny1; ++t) v *= (float)sY[T.yk1[t] * TILE + lane];
+                rc1 = v;
+            }
+            sRC[(2 * p) * TILE + lane] = (double)rc0;
+            sRC[(2 * p + 1) * TILE + lane] = (double)rc1;
+        }
+    }
+    return __syncthreads_or(out) != 0;
+}
+
 struct IntArgs {
     const DevParams *P;
     const PairTab *tab;
+    const PairTabM *tabm;            // the mixed form's pair table (global memory)
     double *tk, *rho, *y, *soot;     // state, updated in place: [npad], [npad], [52][npad], [2][npad]
     const double *pnd;               // p / PSTR per cell [npad]
     const int *nsub;                 // sub-steps per cell [npad]
@@ -226,7 +317,9 @@ __global__ void sort_scatter_kernel(const int *nsub, int n, int npad, int nsub_m
         for (int c = n + lane; c < npad; c += 32) order[c] = c;
 }
 
-template <int NW>
+// MIXED: the rates of every sub-step in the mixed form (tile_rates_mixed; a tile with a rate beyond the
+// FP32 range is recomputed in FP64), the update, closure and Newton in FP64 as in the FP64 form.
+template <int NW, bool MIXED>
 __global__ void __launch_bounds__(NW * 32, 1) integrate_fp64_kernel(const IntArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -307,7 +400,8 @@ __global__ void __launch_bounds__(NW * 32, 1) integrate_fp64_kernel(const IntArg
                 sC[SC_STND * TILE + lane] = s2;
             }
             __syncthreads();
-            tile_rates_fp64<NW>(P, sTab, sRC, sY, sYN, sC, sS, TILE, lane, lane, warp);
+            if (!MIXED || tile_rates_mixed<NW>(P, a.tabm, sRC, sY, sYN, sC, sS, TILE, lane, lane, warp))
+                tile_rates_fp64<NW>(P, sTab, sRC, sY, sYN, sC, sS, TILE, lane, lane, warp);
             __syncthreads();
             if (warp == 0 && st < ns) {
                 const double dt = a.dt / (double)ns;

@@ -1713,8 +1713,10 @@ extern "C" int uc_temperature_from_held(uc_ctx *ctx)
 template <int NW>
 static bool set_integrate_attr()
 {
-    return cudaFuncSetAttribute(integrate_fp64_kernel<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INT_SMEM) ==
-           cudaSuccess;
+    return cudaFuncSetAttribute(integrate_fp64_kernel<NW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)INT_SMEM) == cudaSuccess &&
+           cudaFuncSetAttribute(integrate_fp64_kernel<NW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)INT_SMEM) == cudaSuccess;
 }
 
 // Enqueue one integration step on the context's stream (graph capture or not).
@@ -1756,17 +1758,22 @@ static int enqueue_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts
     }
     CK(cudaMemsetAsync(ctx->next_tile, 0, sizeof(int), ctx->stream));
     IntArgs a{};
-    a.P = ctx->dP; a.tab = ctx->dTab;
+    a.P = ctx->dP; a.tab = ctx->dTab; a.tabm = ctx->dTabM;
     a.tk = ctx->tk; a.rho = ctx->rho; a.y = ctx->y; a.soot = ctx->soot; a.pnd = ctx->pnd;
     a.nsub = ctx->nsub; a.order = sorted ? ctx->order : nullptr; a.next_tile = ctx->next_tile;
     a.passes = ctx->cpasses; a.status = ctx->status;
     a.dt = o.dt; a.sor1 = o.relx; a.tol = o.tol; a.isor = o.isor;
     a.n = ctx->n; a.npad = np; a.ntile = ctx->ntile;
     const int grid = std::min(ctx->ntile, ctx->nsm);
-    if (warps == 16)
-        integrate_fp64_kernel<16><<<grid, 16 * 32, INT_SMEM, ctx->stream>>>(a);
+    const bool mixed = precision == UC_MIXED;
+    if (warps == 16 && mixed)
+        integrate_fp64_kernel<16, true><<<grid, 16 * 32, INT_SMEM, ctx->stream>>>(a);
+    else if (warps == 16)
+        integrate_fp64_kernel<16, false><<<grid, 16 * 32, INT_SMEM, ctx->stream>>>(a);
+    else if (warps == 8 && mixed)
+        integrate_fp64_kernel<8, true><<<grid, 8 * 32, INT_SMEM, ctx->stream>>>(a);
     else if (warps == 8)
-        integrate_fp64_kernel<8><<<grid, 8 * 32, INT_SMEM, ctx->stream>>>(a);
+        integrate_fp64_kernel<8, false><<<grid, 8 * 32, INT_SMEM, ctx->stream>>>(a);
     else
         return set_err(ctx, UC_E_ARG, "integration kernel shape %d warps is not built", warps);
     CK(cudaGetLastError());
@@ -1776,7 +1783,8 @@ static int enqueue_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts
 static int integrate_prepare(uc_ctx *ctx, int precision, const uc_integrate_opts *o)
 {
     if (!ctx) return UC_E_ARG;
-    if (precision != UC_FP64) return set_err(ctx, UC_E_ARG, "integration precision %d is not available", precision);
+    if (precision != UC_FP64 && precision != UC_MIXED)
+        return set_err(ctx, UC_E_ARG, "integration precision %d is not available", precision);
     RET_IF(check_opts(ctx, o));
     if (!ctx->have_fields) return set_err(ctx, UC_E_STATE, "no fields uploaded");
     CK(cudaSetDevice(ctx->device));
