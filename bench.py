@@ -504,7 +504,7 @@ def main_ours(args):
     torch.cuda.synchronize(dev)
     barrier(world)
     clk = ClockSampler(dev)
-    ms, passes, kt = time_sweeps(u, st, ext, unichem.FP64, args.steps, args.warmup, clocks=clk)
+    ms, passes, kt = time_sweeps(u, st, ext, unichem.FP64, args.steps, args.warmup, isor=args.isor, clocks=clk)
     ms = max_over_ranks(ms, world)
     # ---------------- end to end through the C ABI (pinned host buffers in and out)
     pin = lambda *s: torch.empty(s, dtype=torch.float64, pin_memory=True).numpy()
@@ -519,12 +519,12 @@ def main_ours(args):
     e2e_passes = []
     for _ in range(args.steps):
         u.upload(h_tk, h_rho, h_y)
-        e2e_passes.append(u.sweep(DT, precision=unichem.FP64, isor=ISOR, relx=RELX, tol=TOL))
+        e2e_passes.append(u.sweep(DT, precision=unichem.FP64, isor=args.isor, relx=RELX, tol=TOL))
         u.download_outputs(outs)
         u.lib.uc_download_fields(u._h, None, None, unichem._p(h_yout), None, None)
     u.sync()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-    passes_run = float(np.mean([min(p, ISOR) for p in passes]))
+    passes_run = float(np.mean([min(p, args.isor) for p in passes]))
     line = None
     if rank == 0:
         line = {"metric": METRIC, "value": round(world * n * args.steps / (ms / 1e3), 1), "unit": UNIT,
