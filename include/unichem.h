@@ -369,8 +369,8 @@ int uc_integrate_counts(uc_ctx *ctx, int *nsub, int *passes);
  * reference counterpart; the surrogate is not part of the reference):
  * c[M][N] (FP32) = a[M][K] * b[N][K]^T with a, b BF16 bit patterns, row-major.
  * kernel 0: the tiled GEMM (N a multiple of 16, K of 64); kernel 1: the
- * layer kernel with b resident in shared memory (N a multiple of 64 up to 256,
- * K in 64, 128, 256). Allocates and frees its own device buffers; meant for checking the
+ * layer kernel with b resident in shared memory (N and K multiples of 64 up
+ * to 256). Allocates and frees its own device buffers; meant for checking the
  * kernels, not for speed. */
 int uc_gemm_bf16(int device, int kernel, int M, int N, int K, const uint16_t *a, const uint16_t *b, float *c);
 

@@ -49,6 +49,16 @@ def gelu_grad(z):
     return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * C_GELU * (1.0 + 3 * 0.044715 * z * z)
 
 
+def forward(w, x):
+    """x [M][64] (BF16 values) -> the network's output z [M][64] (before decoding), float64."""
+    h = x.astype(np.float64)
+    layers = unpack(w)
+    for li, (W, b) in enumerate(layers):
+        z = h @ bf16(W).T + b
+        h = bf16(gelu(z)) if li < len(layers) - 1 else z
+    return h
+
+
 def forward_backward(w, x, t):
     """x [M][64] (BF16 values), t [M][64]; returns (loss, flat gradient)."""
     layers = unpack(w)

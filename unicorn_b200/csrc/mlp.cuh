@@ -49,15 +49,21 @@ __global__ void mlp_features_kernel(const DevParams *Pp, const MlpNorm *N, const
         const double T = tk[c] * P.TSTR;
         const double lnp = log(pnd[c] / P.PBACK);      // ln(p / reference pressure)
         int out = 0;
-        __nv_bfloat16 *xr = X + (size_t)(r0 + i) * MLP_IN;
-        for (int f = 0; f < MLP_IN; ++f) {
-            float v = 0.0f;
-            if (f < MLP_NF) {
-                const float raw = mlp_raw_feature(f, T, lnp, y, npad, c);
-                out |= !(raw >= N->hull_lo[f] && raw <= N->hull_hi[f]);
-                v = (raw - N->feat_mu[f]) / N->feat_sd[f];
+        uint4 *xr = reinterpret_cast<uint4 *>(X + (size_t)(r0 + i) * MLP_IN);
+        for (int f0 = 0; f0 < MLP_IN; f0 += 8) {          // eight features -> one 16-byte store
+            __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int f = f0 + j;
+                float v = 0.0f;
+                if (f < MLP_NF) {
+                    const float raw = mlp_raw_feature(f, T, lnp, y, npad, c);
+                    out |= !(raw >= N->hull_lo[f] && raw <= N->hull_hi[f]);
+                    v = (raw - N->feat_mu[f]) / N->feat_sd[f];
+                }
+                o[j] = __float2bfloat16_rn(v);
             }
-            xr[f] = __float2bfloat16_rn(v);
+            xr[f0 / 8] = *reinterpret_cast<const uint4 *>(o);
         }
         if (outside) outside[i] = out;
     }
@@ -75,17 +81,6 @@ __global__ void mlp_targets_kernel(const MlpNorm *N, const double *qdsp, int npa
             v = ((float)asinh(q / N->tgt_scale[k]) - N->tgt_mu[k]) / N->tgt_sd[k];
         }
         Tg[(size_t)(r0 + r) * MLP_OUT + k] = v;
-    }
-}
-
-// Network output rows [0, rows) -> QDSP of cells [c0, c0+rows) ([52][npad], FP64)
-__global__ void mlp_decode_kernel(const MlpNorm *N, const float *Out, int rows, double *qdsp, int npad, int c0)
-{
-    const int nthreads = gridDim.x * blockDim.x;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows * MLP_NO; i += nthreads) {
-        const int k = i / rows, r = i % rows;     // consecutive threads -> consecutive cells of a row
-        const float t = Out[(size_t)r * MLP_OUT + k] * N->tgt_sd[k] + N->tgt_mu[k];
-        qdsp[(size_t)k * npad + c0 + r] = (double)N->tgt_scale[k] * sinh((double)t);
     }
 }
 
@@ -153,21 +148,28 @@ __global__ void transpose_bf16_kernel(const __nv_bfloat16 *in, int R, int C, __n
     }
 }
 
-// db[j] = sum over rows of G[m][j] (fixed order per column)
-__global__ void bias_grad_kernel(const __nv_bfloat16 *G, int M, int N, float *db)
+// db[j] = sum over the batch of Gt[j][m] (the transposed output gradient, rows contiguous): one warp per
+// j, 16-byte loads, each lane's partial in a fixed order, then a fixed shuffle tree
+__global__ void bias_grad_kernel(const __nv_bfloat16 *Gt, int M, int N, float *db)
 {
-    __shared__ float s[8][33];
-    const int j = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (j >= N) return;
+    const __nv_bfloat16 *row = Gt + (size_t)j * M;
     float acc = 0.0f;
-    if (j < N)
-        for (int m = threadIdx.y; m < M; m += blockDim.y) acc += __bfloat162float(G[(size_t)m * N + j]);
-    s[threadIdx.y][threadIdx.x] = acc;
-    __syncthreads();
-    if (threadIdx.y == 0 && j < N) {
-        float t = 0.0f;
-        for (int r = 0; r < (int)blockDim.y; ++r) t += s[r][threadIdx.x];
-        db[j] = t;
+    int m = lane * 8;
+    for (; m + 8 <= M; m += 256) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(row + m);
+        const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 f = __bfloat1622float2(h[i]);
+            acc += f.x + f.y;
+        }
     }
+    for (int r = m; r < M && r < m + 8; ++r) acc += __bfloat162float(row[r]);    // ragged tail
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) db[j] = acc;
 }
 
 struct AdamArgs {

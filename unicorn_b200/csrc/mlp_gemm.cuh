@@ -1,24 +1,27 @@
-// BF16 tensor-core GEMM for the surrogate network (sm_100a, tcgen05).
+// BF16 tensor-core GEMMs of the surrogate network (sm_100a, tcgen05, TMA).
 //
 //   C[M, N] = A[M, K] * B[N, K]^T      (A, B bf16, row-major, K contiguous; FP32 accumulate)
 //
-// One CTA of 4 warps computes a 128 x Nt tile (Nt <= 256, a multiple of 16)
-// with the accumulator in tensor memory (TMEM, Nt columns of 128 lanes):
-//   1. all threads copy (cp.async, 16 B each) a 128 x 64 chunk of A and an
-//      Nt x 64 chunk of B from global memory into shared memory in the canonical K-major layout
-//      without swizzle (8 x 8 "core matrices" of 128 contiguous bytes; core
-//      matrices adjacent in K are 128 B apart, 8-row groups 1024 B apart);
-//   2. one thread issues four tcgen05.mma (K = 16 each) and commits them to an
-//      mbarrier; the CTA waits (bounded) before the chunk's shared memory is
-//      rewritten;
-//   3. after the last chunk each warp reads its 32 TMEM lanes (rows) with
-//      tcgen05.ld and applies the epilogue (bias, GELU, its derivative,
-//      conversions) on the way to global memory.
+// gemm_bf16_tc_kernel: one CTA of 4 warps computes a 128 x Nt tile (Nt <= 256,
+// a multiple of 16) over a range of K (the whole K, or one of gridDim.z
+// split-K ranges whose FP32 partial tiles splitk_reduce_kernel adds in a fixed
+// order), with the accumulator in tensor memory (TMEM, Nt columns of 128 lanes):
+//   * thread 0 loads the 128 x 64 chunk of A and the Nt x 64 chunk of B of each
+//     K step with TMA (cp.async.bulk.tensor from this GPU's memory, no
+//     multicast) into one of two shared-memory stages, in the 128-byte-swizzled
+//     K-major layout, once the MMAs that read the stage before have completed;
+//   * thread 32 issues four tcgen05.mma (K = 16) per chunk as it lands and
+//     commits them to the stage's "empty" barrier, so the copy of chunk k + 1
+//     overlaps the MMAs of chunk k;
+//   * after the last chunk each warp reads its 32 TMEM lanes (rows) with
+//     tcgen05.ld and applies the epilogue (bias, GELU, its derivative,
+//     conversions) on the way to global memory.
 // The epilogues are those the network needs: forward layers (bias + GELU,
 // keeping the pre-activation for the backward pass), the output layer (bias,
 // FP32 out), the input gradient of a hidden layer (times GELU'(z)) and the
 // weight gradient (FP32 out).
 #pragma once
+#include <cuda.h>          // CUtensorMap (the type only)
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -30,10 +33,14 @@ constexpr int GM = 128;          // rows of a CTA tile (TMEM lanes)
 constexpr int GK = 64;           // K chunk staged in shared memory
 constexpr int GN_MAX = 256;      // columns of a CTA tile (TMEM columns)
 constexpr int GEMM_THREADS = 128;
-constexpr size_t GEMM_SMEM = (size_t)(GM + GN_MAX) * GK * 2 + 64;
-// dynamic shared memory asked at launch: above the tile's need, so that at most two
-// CTAs (2 x 256 TMEM columns) share an SM
+constexpr uint32_t GEMM_A_BYTES = (uint32_t)GM * GK * 2;          // one K chunk of A: 128 rows x 128 B
+constexpr uint32_t GEMM_B_BYTES = (uint32_t)GN_MAX * GK * 2;      // one K chunk of B: up to 256 rows x 128 B
+constexpr size_t GEMM_STAGE = GEMM_A_BYTES + GEMM_B_BYTES;
+constexpr size_t GEMM_SMEM = 1024 + 2 * GEMM_STAGE + 64;           // align slack, two stages, five mbarriers
+// dynamic shared memory asked at launch: at least the two stages, and enough that at most
+// two CTAs (2 x 256 TMEM columns) share an SM
 constexpr size_t GEMM_SMEM_LAUNCH = 100 * 1024;
+static_assert(GEMM_SMEM <= GEMM_SMEM_LAUNCH, "GEMM stages");
 
 enum GemmEpi : int {
     EPI_F32 = 0,        // C as FP32 (out_f32, ldo)
@@ -41,6 +48,7 @@ enum GemmEpi : int {
     EPI_BIAS_F32 = 2,   // C + bias -> out_f32
     EPI_DGELU = 3,      // C * gelu'(z_in) -> out_bf16 (gradient w.r.t. a hidden pre-activation)
     EPI_BIAS_BF16 = 4,  // C + bias -> out_bf16 (no activation)
+    EPI_DECODE = 5,     // layer kernel only: t = C * dec_sd + (bias * dec_sd + dec_mu) -> dec_out[k][dec_ld] = dec_scale sinh(t), k < dec_n
 };
 
 struct GemmArgs {
@@ -56,6 +64,10 @@ struct GemmArgs {
     float *out_f32;               // [M][ldo]
     __nv_bfloat16 *out_bf16;      // [M][ldo]
     int ldo;
+    size_t split_stride;          // split-K: CTA z writes its FP32 partial tile at out_f32 + z * split_stride
+    const float *dec_sd, *dec_mu, *dec_scale;   // EPI_DECODE: per-output scaling
+    double *dec_out;              // EPI_DECODE: [dec_n][dec_ld] FP64, row r of the layer -> column r
+    int dec_ld, dec_n;
     int *status;
 };
 
@@ -81,108 +93,136 @@ __device__ __forceinline__ float gelu_grad_f(float x)
     return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * du;
 }
 
-// shared-memory matrix descriptor: K-major, no swizzle
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
-{
-    uint64_t d = 0;
-    d |= (uint64_t)((addr >> 4) & 0x3FFF);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-    d |= (uint64_t)1 << 46;                        // descriptor version of sm_100
-    return d;                                      // base offset 0, layout type 0 (no swizzle)
-}
-
 // instruction descriptor of kind::f16: BF16 x BF16 -> FP32, both K-major, M x N
 __host__ __device__ constexpr uint32_t mma_idesc(int m, int n)
 {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
-// 16-byte asynchronous global -> shared copy (zero-filled when !valid)
-__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 16 : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all()
-{
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
-}
-
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__global__ void __launch_bounds__(GEMM_THREADS) gemm_bf16_tc_kernel(const GemmArgs g)
+// shared-memory matrix descriptor: K-major, 128-byte swizzle (8-row atoms 1024 B apart)
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr)
 {
-    extern __shared__ __align__(1024) unsigned char gsm[];
-    unsigned char *sA = gsm;                                  // 128 x 64 bf16 = 16 KB
-    unsigned char *sB = gsm + GM * GK * 2;                    // Nt x 64 bf16 <= 32 KB
-    uint64_t *bar = reinterpret_cast<uint64_t *>(gsm + (GM + GN_MAX) * GK * 2);
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                        // leading byte offset: not used by a swizzled K-major operand
+    d |= (uint64_t)(1024 >> 4) << 32;              // stride byte offset: 8-row atoms
+    d |= (uint64_t)1 << 46;                        // descriptor version of sm_100
+    d |= (uint64_t)2 << 61;                        // layout type: 128-byte swizzle
+    return d;
+}
+
+// 2-D TMA tile load (this GPU's memory, no multicast), completion on the mbarrier
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// bounded wait that also gives up when another role has aborted; on giving up it records the timeout
+__device__ __forceinline__ bool lw_wait(uint64_t *bar, uint32_t parity, volatile int *abort, int *status)
+{
+    for (int round = 0; round < 64; ++round) {
+        if (mbar_wait_bounded(bar, parity, 1 << 16)) return true;
+        if (*abort) return false;
+    }
+    atomicExch(status, ST_MMA_TIMEOUT);
+    *abort = 1;
+    return false;
+}
+
+__global__ void __launch_bounds__(GEMM_THREADS)
+    gemm_bf16_tc_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap map_a,
+                        const __grid_constant__ CUtensorMap map_b)
+{
+    extern __shared__ __align__(1024) unsigned char gsm_raw[];
+    unsigned char *gsm = gsm_raw + ((1024 - (smem_u32(gsm_raw) & 1023)) & 1023);
+    uint64_t *full = reinterpret_cast<uint64_t *>(gsm + 2 * GEMM_STAGE);   // [2] chunk landed
+    uint64_t *empty = full + 2;                                             // [2] its MMAs completed
+    uint64_t *done = empty + 2;                                             // every MMA of the CTA completed
     __shared__ uint32_t s_tmem;
+    __shared__ volatile int s_abort;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * GM, n0 = blockIdx.y * GN_MAX;
     const int nt = min(GN_MAX, g.N - n0);                     // multiple of 16
     const uint32_t ncols = nt <= 32 ? 32 : nt <= 64 ? 64 : nt <= 128 ? 128 : 256;
+    const uint32_t b_bytes = (uint32_t)min(g.N, GN_MAX) * GK * 2;     // the B box (rows past N read as zeros)
+    // this CTA's K chunks
+    const int nk_all = g.K / GK, per = (nk_all + gridDim.z - 1) / gridDim.z;
+    const int c_beg = blockIdx.z * per, nck = min(nk_all, c_beg + per) - c_beg;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                      "r"(ncols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    if (tid == 0) mbar_init(bar, 1);
+    if (tid == 0) {
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(full + i, 1);
+            mbar_init(empty + i, 1);
+        }
+        mbar_init(done, 1);
+        s_abort = 0;
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
-    const uint32_t idesc = mma_idesc(GM, nt);
-    const int nchunk = g.K / GK;
-    bool ok = true;
 
-    for (int kc = 0; kc < nchunk; ++kc) {
-        const int k0 = kc * GK;
-        // ---- stage A (128 x 64) and B (nt x 64), 16-byte pieces, canonical K-major layout
-        for (int i = tid; i < GM * (GK / 8); i += GEMM_THREADS) {
-            const int r = i >> 3, kb = i & 7;
-            const bool in = m0 + r < g.M;
-            cp_async16(sA + ((r >> 3) * (GK / 8) + kb) * 128 + (r & 7) * 16,
-                       g.A + (size_t)(in ? m0 + r : 0) * g.lda + k0 + kb * 8, in);
+    if (tid == 0) {
+        // ---- TMA producer: chunk j into stage j & 1
+        int j = 0;
+        for (; j < nck; ++j) {
+            const int s = j & 1;
+            if (j >= 2 && !lw_wait(empty + s, (uint32_t)(((j >> 1) + 1) & 1), &s_abort, g.status)) break;
+            unsigned char *sA = gsm + (size_t)s * GEMM_STAGE;
+            mbar_expect_tx(full + s, GEMM_A_BYTES + b_bytes);
+            tma_load_2d(sA, &map_a, (c_beg + j) * GK, m0, full + s);
+            tma_load_2d(sA + GEMM_A_BYTES, &map_b, (c_beg + j) * GK, n0, full + s);
         }
-        for (int i = tid; i < nt * (GK / 8); i += GEMM_THREADS) {
-            const int r = i >> 3, kb = i & 7;
-            cp_async16(sB + ((r >> 3) * (GK / 8) + kb) * 128 + (r & 7) * 16, g.B + (size_t)(n0 + r) * g.ldb + k0 + kb * 8,
-                       true);
-        }
-        cp_async_wait_all();
-        // generic-proxy writes -> visible to the tensor core (async proxy)
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        if (tid == 0) {
-            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+        // every copy issued has landed before the CTA can exit
+        for (int i = (j > 2 ? j - 2 : 0); i < j; ++i) mbar_wait_bounded(full + (i & 1), (uint32_t)((i >> 1) & 1), 1 << 22);
+    } else if (tid == 32) {
+        // ---- MMA issuer
+        const uint32_t idesc = mma_idesc(GM, nt);
+        for (int j = 0; j < nck; ++j) {
+            const int s = j & 1;
+            if (!lw_wait(full + s, (uint32_t)((j >> 1) & 1), &s_abort, g.status)) break;
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(gsm + (size_t)s * GEMM_STAGE), b0 = a0 + GEMM_A_BYTES;
 #pragma unroll
             for (int kk = 0; kk < GK / 16; ++kk) {
-                const uint64_t ad = smem_desc(a0 + kk * 256, 128, (GK / 8) * 128);
-                const uint64_t bd = smem_desc(b0 + kk * 256, 128, (GK / 8) * 128);
-                const uint32_t acc = (kc > 0 || kk > 0) ? 1u : 0u;
+                const uint32_t accum = (j > 0 || kk > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+                    "l"(smem_desc_sw128(a0 + kk * 32)), "l"(smem_desc_sw128(b0 + kk * 32)), "r"(idesc), "r"(accum));
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(bar))
-                         : "memory");
+            tc_commit(empty + s);
         }
-        // the chunk's shared memory is read by the MMAs until they complete
-        const bool done = mbar_wait_bounded(bar, (uint32_t)(kc & 1), 1 << 22);
-        if (!done) {
-            if (tid == 0) atomicExch(g.status, ST_MMA_TIMEOUT);
-            mbar_wait_bounded(bar, (uint32_t)(kc & 1), 1 << 22);   // let work in flight land
-        }
-        tc_fence_after();
-        if (!__syncthreads_and(done)) { ok = false; break; }    // the same decision in every thread
+        tc_commit(done);
     }
+    __syncwarp();
+    bool ok = lw_wait(done, 0, &s_abort, g.status);
+    ok = __syncthreads_and(ok && !s_abort) != 0;
+    tc_fence_after();
+    float *out_f32 = g.out_f32 ? g.out_f32 + (size_t)blockIdx.z * g.split_stride : nullptr;
 
     // ---- epilogue: warp w reads TMEM lanes 32w..32w+31 (rows), 16 columns at a time
     const int row = m0 + warp * 32 + lane;
@@ -202,29 +242,49 @@ __global__ void __launch_bounds__(GEMM_THREADS) gemm_bf16_tc_kernel(const GemmAr
                 float x[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) x[j] = __uint_as_float(v[j]);
-                if (g.epi == EPI_F32) {
+                // each thread owns a row: 16-byte loads and stores along it (n, ldo, ldz multiples of 16)
+                if (g.epi == EPI_F32 || g.epi == EPI_BIAS_F32) {
+                    float4 *o4 = reinterpret_cast<float4 *>(out_f32 + (size_t)row * g.ldo + n);
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) g.out_f32[(size_t)row * g.ldo + n + j] = x[j];
-                } else if (g.epi == EPI_BIAS_F32) {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) g.out_f32[(size_t)row * g.ldo + n + j] = x[j] + g.bias[n + j];
-                } else if (g.epi == EPI_BIAS_GELU) {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const float z = x[j] + g.bias[n + j];
-                        if (g.z_save) g.z_save[(size_t)row * g.ldz + n + j] = z;
-                        g.out_bf16[(size_t)row * g.ldo + n + j] = __float2bfloat16_rn(gelu_f(z));
-                    }
-                } else if (g.epi == EPI_DGELU) {
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const float z = g.z_in[(size_t)row * g.ldz + n + j];
-                        g.out_bf16[(size_t)row * g.ldo + n + j] = __float2bfloat16_rn(x[j] * gelu_grad_f(z));
+                    for (int q = 0; q < 4; ++q) {
+                        float4 o = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+                        if (g.epi == EPI_BIAS_F32) {
+                            o.x += g.bias[n + 4 * q]; o.y += g.bias[n + 4 * q + 1];
+                            o.z += g.bias[n + 4 * q + 2]; o.w += g.bias[n + 4 * q + 3];
+                        }
+                        o4[q] = o;
                     }
                 } else {
+                    float y[16];
+                    if (g.epi == EPI_BIAS_GELU) {
 #pragma unroll
-                    for (int j = 0; j < 16; ++j)
-                        g.out_bf16[(size_t)row * g.ldo + n + j] = __float2bfloat16_rn(x[j] + g.bias[n + j]);
+                        for (int j = 0; j < 16; ++j) {
+                            const float z = x[j] + g.bias[n + j];
+                            if (g.z_save) g.z_save[(size_t)row * g.ldz + n + j] = z;
+                            y[j] = gelu_f(z);
+                        }
+                    } else if (g.epi == EPI_DGELU) {
+                        const float4 *z4 = reinterpret_cast<const float4 *>(g.z_in + (size_t)row * g.ldz + n);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float4 z = z4[q];
+                            y[4 * q] = x[4 * q] * gelu_grad_f(z.x);
+                            y[4 * q + 1] = x[4 * q + 1] * gelu_grad_f(z.y);
+                            y[4 * q + 2] = x[4 * q + 2] * gelu_grad_f(z.z);
+                            y[4 * q + 3] = x[4 * q + 3] * gelu_grad_f(z.w);
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) y[j] = x[j] + g.bias[n + j];
+                    }
+                    uint4 *ob = reinterpret_cast<uint4 *>(g.out_bf16 + (size_t)row * g.ldo + n);
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        __align__(16) __nv_bfloat162 h[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) h[j] = __floats2bfloat162_rn(y[8 * q + 2 * j], y[8 * q + 2 * j + 1]);
+                        ob[q] = *reinterpret_cast<uint4 *>(h);
+                    }
                 }
             }
         }
@@ -234,34 +294,157 @@ __global__ void __launch_bounds__(GEMM_THREADS) gemm_bf16_tc_kernel(const GemmAr
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
 }
 
+// out[m][n] = sum over s of part[s][m][n], s in order (the split-K partial tiles, [splits][M][N])
+__global__ void splitk_reduce_kernel(const float *part, int splits, int M, int N, float *out, int ldo)
+{
+    const size_t mn = (size_t)M * N;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < mn; i += (size_t)gridDim.x * blockDim.x) {
+        float acc = 0.0f;
+        for (int z = 0; z < splits; ++z) acc += part[(size_t)z * mn + i];
+        out[(i / N) * ldo + i % N] = acc;
+    }
+}
+
 }  // namespace uc
 
 namespace uc {
 
 // ---------------------------------------------------------------------------
 // One layer of the network over many rows, weights resident in shared memory:
-//   out[M, N] = epi(A[M, K] * W[N, K]^T + bias),   N <= 256, K in {64, 128, 256}
-// A persistent CTA per SM (8 warps) stages W once in the canonical K-major
-// layout, then walks 128-row tiles of A: it stages the tile, one thread
-// issues K/16 tcgen05.mma into one of two TMEM accumulators (2 x 256 columns)
-// and commits them to that accumulator's mbarrier, and while they run the
-// warps drain the previous tile's accumulator through tcgen05.ld (32 columns
-// at a time) into the epilogue (bias from shared memory, GELU -> BF16, or
-// bias -> FP32, 16-byte stores). Warp w reads TMEM lanes 32 (w % 4) .. +31
-// and half w / 4 of the columns (N / 2 a multiple of 32).
-constexpr int LW_THREADS = 256;
-constexpr size_t LW_SMEM = (size_t)256 * 256 * 2 + (size_t)128 * 256 * 2 + 64;
+//   out[M, N] = epi(A[M, K] * W[N, K]^T + bias),   N in {64, 128, 192, 256}, K in {64, 128, 192, 256}
+// A persistent CTA per SM, warp-specialised:
+//   warp 8 (one thread): TMA loads. W once (K/64 boxes of N rows x 128 B), then
+//     the 128 x 64 chunks of the CTA's row tiles, in order, into a ring of
+//     LW_SLOTS 16 KB slots; a slot is refilled once the MMAs that read it have
+//     completed (their commit arrives on the slot's "empty" barrier);
+//   warp 9 (one thread): for each tile, once the epilogue has drained the
+//     accumulator it is about to use (two accumulators of 256 TMEM columns),
+//     four tcgen05.mma (K = 16) per chunk as each chunk lands, a commit per
+//     chunk (frees the slot) and one per tile (the accumulator is full);
+//   warps 0-7: drain the full accumulator through tcgen05.ld, 32 columns at a
+//     time, into the epilogue (bias from shared
+//     memory, then GELU -> BF16 with the pre-activation kept if asked, bias ->
+//     FP32, or the surrogate's decoding into FP64 omega; 16-byte stores) and
+//     mark it empty. Warp w reads TMEM lanes 32 (w % 4) .. +31 and half w / 4
+//     of the columns.
+// So the loads of the next tiles, the MMAs of this one and the epilogue of the
+// previous one overlap. Operands are in the 128-byte-swizzled K-major layout
+// that TMA writes with CU_TENSOR_MAP_SWIZZLE_128B (rows of 64 BF16, 16-byte
+// pieces of row r at piece ^ (r % 8), 1024-byte atoms of 8 rows). Every wait
+// is bounded; a wait that gives up sets the status and an abort flag that the
+// other roles see, and the CTA retires its copies and MMAs in flight before it
+// frees TMEM.
+constexpr int LW_EPI_WARPS = 8;
+constexpr int LW_THREADS = (LW_EPI_WARPS + 2) * 32;
+constexpr int LW_SLOTS = 5;                                    // A chunks in flight per CTA
+constexpr uint32_t LW_CHUNK_BYTES = (uint32_t)GM * GK * 2;     // 128 rows x 64 BF16
+constexpr size_t LW_W_BYTES = (size_t)256 * 256 * 2;
+constexpr size_t LW_SMEM = 1024 + LW_W_BYTES + (size_t)LW_SLOTS * LW_CHUNK_BYTES + 256;   // align slack, W, ring, barriers
 
-__global__ void __launch_bounds__(LW_THREADS, 1) gemm_w_resident_kernel(const GemmArgs g)
+// 32 consecutive TMEM columns of the warp's 32 lanes into v (asynchronous until tm_wait32(v))
+__device__ __forceinline__ void tm_ld32(uint32_t (&v)[32], uint32_t taddr)
 {
-    extern __shared__ __align__(1024) unsigned char lsm[];
-    const int N = g.N, K = g.K;
-    unsigned char *sW = lsm;                                   // N x K bf16
-    unsigned char *sA = lsm + (size_t)N * K * 2;               // 128 x K bf16
-    uint64_t *bar = reinterpret_cast<uint64_t *>(lsm + LW_SMEM - 64);   // two mbarriers
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                 : "r"(taddr));
+}
+// wait for the warp's TMEM loads; v is tied to the wait so that no use of it moves above it
+__device__ __forceinline__ void tm_wait32(uint32_t (&v)[32])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]), "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15]), "+r"(v[16]), "+r"(v[17]), "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]), "+r"(v[22]), "+r"(v[23]), "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]), "+r"(v[29]), "+r"(v[30]), "+r"(v[31])
+                 :
+                 : "memory");
+}
+
+// omega_k = scale_k sinh(t). In FP32, branch-free: sinh(t) = (e - 1/e) / 2 with e = 2^(t log2 e) from the
+// hardware exponential (relative error ~1e-6 at |t| = 80, far below the network's own error), and the
+// Taylor series t + t^3/6 + t^5/120 below |t| = 0.25 where the difference cancels (truncation < 3e-8
+// relative); beyond |t| = 80, where e would overflow FP32, sinh in FP64.
+__device__ __noinline__ double lw_decode_wide(float t, float scale) { return (double)scale * sinh((double)t); }
+
+__device__ __forceinline__ double lw_decode(float t, float scale)
+{
+    const float at = fabsf(t);
+    if (at >= 80.0f) return lw_decode_wide(t, scale);      // out of line: rare, and keeps the unrolled epilogue small
+    const float e = exp2f(t * 1.4426950408889634f);
+    const float big = 0.5f * (e - __frcp_rn(e));
+    const float t2 = t * t;
+    const float small = t * fmaf(t2, fmaf(t2, 1.0f / 120.0f, 1.0f / 6.0f), 1.0f);
+    return (double)scale * (double)(at < 0.25f ? small : big);
+}
+
+// epilogue of 32 accumulator columns [c, c + 32) of one row (bias read as float4 broadcasts)
+__device__ __forceinline__ void lw_store32(const GemmArgs &g, const uint32_t (&v)[32], int row, int c,
+                                           const float *s_bias, const float (*s_dec)[64])
+{
+    if (row >= g.M) return;
+    const float4 *b4 = reinterpret_cast<const float4 *>(s_bias + c);
+    if (g.epi == EPI_BIAS_GELU) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            __align__(16) __nv_bfloat162 o[4];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const float4 bb = b4[q * 2 + j];
+                const int i = q * 8 + j * 4;
+                const float z0 = __uint_as_float(v[i]) + bb.x, z1 = __uint_as_float(v[i + 1]) + bb.y;
+                const float z2 = __uint_as_float(v[i + 2]) + bb.z, z3 = __uint_as_float(v[i + 3]) + bb.w;
+                if (g.z_save) {
+                    float4 zz;
+                    zz.x = z0; zz.y = z1; zz.z = z2; zz.w = z3;
+                    *reinterpret_cast<float4 *>(g.z_save + (size_t)row * g.ldz + c + i) = zz;
+                }
+                o[j * 2] = __floats2bfloat162_rn(gelu_f(z0), gelu_f(z1));
+                o[j * 2 + 1] = __floats2bfloat162_rn(gelu_f(z2), gelu_f(z3));
+            }
+            *reinterpret_cast<uint4 *>(g.out_bf16 + (size_t)row * g.ldo + c + q * 8) = *reinterpret_cast<uint4 *>(o);
+        }
+    } else if (g.epi == EPI_DECODE) {
+        // straight into the [k][ld] FP64 output: the lanes are consecutive rows
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const int k = c + j;
+            if (k < g.dec_n) {
+                const float t = fmaf(__uint_as_float(v[j]), s_dec[0][k], s_dec[1][k]);
+                g.dec_out[(size_t)k * g.dec_ld + row] = lw_decode(t, s_dec[2][k]);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float4 bb = b4[q];
+            float4 o;
+            o.x = __uint_as_float(v[q * 4 + 0]) + bb.x;
+            o.y = __uint_as_float(v[q * 4 + 1]) + bb.y;
+            o.z = __uint_as_float(v[q * 4 + 2]) + bb.z;
+            o.w = __uint_as_float(v[q * 4 + 3]) + bb.w;
+            *reinterpret_cast<float4 *>(g.out_f32 + (size_t)row * g.ldo + c + q * 4) = o;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(LW_THREADS, 1)
+    gemm_w_resident_kernel(const GemmArgs g, const __grid_constant__ CUtensorMap map_a,
+                           const __grid_constant__ CUtensorMap map_w)
+{
+    extern __shared__ __align__(1024) unsigned char lsm_raw[];
+    // 1024-byte alignment of the swizzle atoms, whatever the base of dynamic shared memory
+    unsigned char *lsm = lsm_raw + ((1024 - (smem_u32(lsm_raw) & 1023)) & 1023);
+    const int N = g.N, K = g.K, nck = K / GK;
+    unsigned char *sW = lsm;                                           // K/64 chunks of N x 128 B
+    unsigned char *sA = lsm + LW_W_BYTES;                              // LW_SLOTS chunks of 128 x 128 B
+    uint64_t *full = reinterpret_cast<uint64_t *>(sA + (size_t)LW_SLOTS * LW_CHUNK_BYTES);
+    uint64_t *empty = full + LW_SLOTS;
+    uint64_t *accf = empty + LW_SLOTS;       // [2] accumulator full (MMA commit)
+    uint64_t *acce = accf + 2;               // [2] accumulator drained (one arrive per epilogue warp)
+    uint64_t *wbar = acce + 2;               // W landed
+    uint64_t *done = wbar + 1;               // every MMA of the CTA completed
     __shared__ uint32_t s_tmem;
+    __shared__ __align__(16) float s_bias[256];
+    __shared__ float s_dec[3][64];           // EPI_DECODE: t = acc * sd + (bias * sd + mu), scale
+    __shared__ volatile int s_abort;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int kb8 = K / 8;                                     // core matrices along K
     const int ntiles = (g.M + GM - 1) / GM;
 
     if (warp == 0) {
@@ -270,128 +453,113 @@ __global__ void __launch_bounds__(LW_THREADS, 1) gemm_w_resident_kernel(const Ge
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        mbar_init(bar, 1);
-        mbar_init(bar + 1, 1);
+        for (int i = 0; i < LW_SLOTS; ++i) {
+            mbar_init(full + i, 1);
+            mbar_init(empty + i, 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(accf + b, 1);
+            mbar_init(acce + b, LW_EPI_WARPS);
+        }
+        mbar_init(wbar, 1);
+        mbar_init(done, 1);
+        s_abort = 0;
     }
-    // weights, once per CTA
-    for (int i = tid; i < N * kb8; i += LW_THREADS) {
-        const int r = i / kb8, kb = i % kb8;
-        cp_async16(sW + ((size_t)(r >> 3) * kb8 + kb) * 128 + (r & 7) * 16, g.B + (size_t)r * g.ldb + kb * 8, true);
-    }
-    cp_async_wait_all();
+    for (int i = tid; i < N; i += LW_THREADS) s_bias[i] = g.bias[i];
+    if (g.epi == EPI_DECODE)
+        for (int k = tid; k < g.dec_n; k += LW_THREADS) {
+            s_dec[0][k] = g.dec_sd[k];
+            s_dec[1][k] = g.bias[k] * g.dec_sd[k] + g.dec_mu[k];
+            s_dec[2][k] = g.dec_scale[k];
+        }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
-    const uint32_t idesc = mma_idesc(GM, N);
-    bool ok = true;
-    int it = 0;
 
-    // bias of the layer in shared memory (read by every row)
-    __shared__ float s_bias[256];
-    for (int i = tid; i < N; i += LW_THREADS) s_bias[i] = g.bias[i];
-    __syncthreads();
-
-    auto epilogue = [&](int tile, int buf) {
-        const int row = tile * GM + (warp & 3) * 32 + lane;
-        const int half = N / 2;                                // 128 or 32 columns per warp
-        const int cbeg = (warp >> 2) * half, cend = cbeg + half;
-        for (int c0 = cbeg; c0 < cend; c0 += 32) {
-            uint32_t v[32];
-            const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(buf * 256 + c0);
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-                  "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-                  "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < g.M) {
-                if (g.epi == EPI_BIAS_GELU) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        __align__(16) __nv_bfloat16 o[8];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const int c = q * 8 + j;
-                            const float z = __uint_as_float(v[c]) + s_bias[c0 + c];
-                            if (g.z_save) g.z_save[(size_t)row * g.ldz + c0 + c] = z;
-                            o[j] = __float2bfloat16_rn(gelu_f(z));
-                        }
-                        *reinterpret_cast<uint4 *>(g.out_bf16 + (size_t)row * g.ldo + c0 + q * 8) =
-                            *reinterpret_cast<uint4 *>(o);
+    if (warp == LW_EPI_WARPS) {
+        // ---- TMA producer
+        if (lane == 0) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(&map_a) : "memory");
+            mbar_expect_tx(wbar, (uint32_t)(N * K * 2));
+            for (int c = 0; c < nck; ++c) tma_load_2d(sW + (size_t)c * N * 128, &map_w, c * GK, 0, wbar);
+            int q = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x) {
+                for (int c = 0; c < nck; ++c, ++q) {
+                    const int s = q % LW_SLOTS;
+                    if (q >= LW_SLOTS && !lw_wait(empty + s, (uint32_t)((q / LW_SLOTS + 1) & 1), &s_abort, g.status)) {
+                        ok = false;
+                        break;
                     }
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        float4 o;
-                        o.x = __uint_as_float(v[q * 4 + 0]) + s_bias[c0 + q * 4 + 0];
-                        o.y = __uint_as_float(v[q * 4 + 1]) + s_bias[c0 + q * 4 + 1];
-                        o.z = __uint_as_float(v[q * 4 + 2]) + s_bias[c0 + q * 4 + 2];
-                        o.w = __uint_as_float(v[q * 4 + 3]) + s_bias[c0 + q * 4 + 3];
-                        *reinterpret_cast<float4 *>(g.out_f32 + (size_t)row * g.ldo + c0 + q * 4) = o;
-                    }
+                    mbar_expect_tx(full + s, LW_CHUNK_BYTES);
+                    tma_load_2d(sA + (size_t)s * LW_CHUNK_BYTES, &map_a, c * GK, tile * GM, full + s);
                 }
             }
+            // every copy issued has landed before the CTA can exit (bounded; nothing else to do on failure)
+            for (int j = (q > LW_SLOTS ? q - LW_SLOTS : 0); j < q; ++j)
+                mbar_wait_bounded(full + j % LW_SLOTS, (uint32_t)((j / LW_SLOTS) & 1), 1 << 22);
+            mbar_wait_bounded(wbar, 0, 1 << 22);
         }
-    };
-
-    int prev_tile = -1;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-        const int buf = it & 1;
-        // the previous tile's MMAs read sA: wait for them before restaging it
-        if (prev_tile >= 0) {
-            const bool done = mbar_wait_bounded(bar + (buf ^ 1), (uint32_t)(((it - 1) >> 1) & 1), 1 << 22);
-            if (!done) {
-                if (tid == 0) atomicExch(g.status, ST_MMA_TIMEOUT);
-                mbar_wait_bounded(bar + (buf ^ 1), (uint32_t)(((it - 1) >> 1) & 1), 1 << 22);
-            }
+    } else if (warp == LW_EPI_WARPS + 1) {
+        // ---- MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = mma_idesc(GM, N);
+            bool ok = lw_wait(wbar, 0, &s_abort, g.status);
             tc_fence_after();
-            if (!__syncthreads_and(done)) { ok = false; break; }
-        }
-        const int m0 = tile * GM;
-        for (int i = tid; i < GM * kb8; i += LW_THREADS) {
-            const int r = i / kb8, kb = i % kb8;
-            const bool in = m0 + r < g.M;
-            cp_async16(sA + ((size_t)(r >> 3) * kb8 + kb) * 128 + (r & 7) * 16,
-                       g.A + (size_t)(in ? m0 + r : 0) * g.lda + kb * 8, in);
-        }
-        cp_async_wait_all();
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        tc_fence_before();
-        __syncthreads();                 // also: the epilogue of tile it-2 (same accumulator) is finished
-        tc_fence_after();
-        if (tid == 0) {
-            const uint32_t a0 = smem_u32(sA), w0 = smem_u32(sW);
-            for (int kk = 0; kk < K / 16; ++kk) {
-                const uint64_t ad = smem_desc(a0 + kk * 256, 128, kb8 * 128);
-                const uint64_t bd = smem_desc(w0 + kk * 256, 128, kb8 * 128);
-                const uint32_t acc = kk > 0 ? 1u : 0u;
-                asm volatile(
-                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + (uint32_t)(buf * 256)),
-                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            int q = 0, it = 0;
+            for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x, ++it) {
+                const int b = it & 1;
+                if (it >= 2 && !lw_wait(acce + b, (uint32_t)(((it >> 1) - 1) & 1), &s_abort, g.status)) break;
+                tc_fence_after();
+                const uint32_t acc_addr = tmem + (uint32_t)(b * 256);
+                for (int c = 0; c < nck; ++c, ++q) {
+                    const int s = q % LW_SLOTS;
+                    if (!lw_wait(full + s, (uint32_t)((q / LW_SLOTS) & 1), &s_abort, g.status)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a0 = smem_u32(sA + (size_t)s * LW_CHUNK_BYTES);
+                    const uint32_t w0 = smem_u32(sW + (size_t)c * N * 128);
+#pragma unroll
+                    for (int kk = 0; kk < GK / 16; ++kk) {
+                        const uint32_t accum = (c > 0 || kk > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(acc_addr),
+                            "l"(smem_desc_sw128(a0 + kk * 32)), "l"(smem_desc_sw128(w0 + kk * 32)), "r"(idesc),
+                            "r"(accum));
+                    }
+                    tc_commit(empty + s);                // the slot may be refilled once these MMAs are done
+                }
+                if (!ok) break;
+                tc_commit(accf + b);                     // the accumulator holds the tile
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(bar + buf))
-                         : "memory");
+            tc_commit(done);
+            mbar_wait_bounded(done, 0, 1 << 22);         // no MMA in flight when TMEM is freed
         }
-        // drain the previous accumulator while these MMAs run
-        if (prev_tile >= 0) epilogue(prev_tile, buf ^ 1);
-        tc_fence_before();
-        prev_tile = tile;
-    }
-    if (ok && prev_tile >= 0) {
-        const int buf = (it - 1) & 1;
-        const bool done = mbar_wait_bounded(bar + buf, (uint32_t)(((it - 1) >> 1) & 1), 1 << 22);
-        if (!done) {
-            if (tid == 0) atomicExch(g.status, ST_MMA_TIMEOUT);
-            mbar_wait_bounded(bar + buf, (uint32_t)(((it - 1) >> 1) & 1), 1 << 22);
+    } else {
+        // ---- epilogue warps: warp w drains TMEM lanes 32 (w % 4) .. +31 (rows), columns [w / 4 * N / 2, +N / 2),
+        // 32 at a time
+        const int ncw = N / 2, cbeg = (warp >> 2) * ncw;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+            const int b = it & 1;
+            if (!lw_wait(accf + b, (uint32_t)((it >> 1) & 1), &s_abort, g.status)) break;
+            tc_fence_after();
+            const int row = tile * GM + (warp & 3) * 32 + lane;
+            const uint32_t tbase = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(b * 256);
+            for (int c = cbeg; c < cbeg + ncw; c += 32) {
+                uint32_t v[32];
+                tm_ld32(v, tbase + (uint32_t)c);
+                tm_wait32(v);
+                lw_store32(g, v, row, c, s_bias, s_dec);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acce + b);        // the MMAs of tile it + 2 may overwrite this accumulator
         }
-        tc_fence_after();
-        if (__syncthreads_and(done)) epilogue(prev_tile, buf);
     }
     tc_fence_before();
     __syncthreads();

@@ -487,18 +487,23 @@ static void ip_kernel(bool mixed, const void **fn, size_t *sm)
 typedef CUresult (*uc_encode_tiled_fn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                        const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                        CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-static int encode_rc_map(uc_ctx *ctx)
+static uc_encode_tiled_fn tensor_map_encoder()
 {
-    if (ctx->tr_map_base == ctx->rc) return UC_OK;
     static uc_encode_tiled_fn encode = nullptr;
     if (!encode) {
         void *fn = nullptr;
         cudaDriverEntryPointQueryResult q;
         cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
-        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
-            return set_err(ctx, UC_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-        encode = (uc_encode_tiled_fn)fn;
+        if (e == cudaSuccess && q == cudaDriverEntryPointSuccess && fn) encode = (uc_encode_tiled_fn)fn;
     }
+    return encode;
+}
+
+static int encode_rc_map(uc_ctx *ctx)
+{
+    if (ctx->tr_map_base == ctx->rc) return UC_OK;
+    uc_encode_tiled_fn encode = tensor_map_encoder();
+    if (!encode) return set_err(ctx, UC_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
     const cuuint64_t dims[2] = {(cuuint64_t)ctx->npad, (cuuint64_t)LRX};
     const cuuint64_t strides[1] = {(cuuint64_t)ctx->npad * sizeof(double)};
     const cuuint32_t estr[2] = {1, 1};
@@ -1901,8 +1906,51 @@ extern "C" int uc_integrate_counts(uc_ctx *ctx, int *nsub, int *passes)
 
 // ------------------------------------------------------------------ tensor-core GEMM
 
-// Launch C = A * B^T on the stream (see mlp_gemm.cuh for the shapes it takes).
-static cudaError_t launch_gemm(const GemmArgs &g, cudaStream_t st)
+// A row-major BF16 matrix [rows][ld] (its first `cols` columns) as a TMA tensor map: boxes of 64 columns
+// (128 B) x box_rows rows, 128-byte swizzle (the K-major operand layout of the tensor-core kernels), rows
+// beyond `rows` read as zeros.
+static bool encode_bf16_map(CUtensorMap *m, const void *base, int cols, int rows, int ld, int box_rows)
+{
+    uc_encode_tiled_fn encode = tensor_map_encoder();
+    if (!encode || ((uintptr_t)base & 15) || ld % 8 || cols % GK || box_rows < 1 || box_rows > 256) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)GK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// multiprocessors of the current device (cached per device)
+static int device_sms()
+{
+    static thread_local int nsm = 0, nsm_dev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (nsm_dev != dev) {
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        nsm_dev = dev;
+    }
+    return nsm;
+}
+
+// split-K factor of the tiled GEMM: FP32 outputs only, enough CTAs to cover the SMs, at least four K
+// chunks per split, and no more partial tiles than `ws_floats` holds
+static int gemm_splits(const GemmArgs &g, size_t ws_floats)
+{
+    if (g.epi != EPI_F32 || !ws_floats) return 1;
+    const int tiles = ((g.M + GM - 1) / GM) * ((g.N + GN_MAX - 1) / GN_MAX), nk = g.K / GK;
+    int sp = std::min(nk / 4, (device_sms() + tiles - 1) / tiles);
+    sp = (int)std::min<size_t>((size_t)sp, ws_floats / ((size_t)g.M * g.N));
+    if (sp <= 1) return 1;
+    const int per = (nk + sp - 1) / sp;
+    return (nk + per - 1) / per;                 // no empty split
+}
+
+// Launch C = A * B^T on the stream (mlp_gemm.cuh gives the shapes it takes); FP32 outputs are split
+// along K over the workspace `ws` ([splits][M][N]) when that fills more SMs, then reduced in order.
+static cudaError_t launch_gemm(const GemmArgs &g, cudaStream_t st, float *ws, size_t ws_floats)
 {
     static thread_local int attr_done = -1;
     int dev = 0;
@@ -1913,14 +1961,33 @@ static cudaError_t launch_gemm(const GemmArgs &g, cudaStream_t st)
         if (e != cudaSuccess) return e;
         attr_done = dev;
     }
-    dim3 grid((g.M + GM - 1) / GM, (g.N + GN_MAX - 1) / GN_MAX);
-    gemm_bf16_tc_kernel<<<grid, GEMM_THREADS, GEMM_SMEM_LAUNCH, st>>>(g);
+    CUtensorMap map_a, map_b;
+    if (!encode_bf16_map(&map_a, g.A, g.K, g.M, g.lda, GM) ||
+        !encode_bf16_map(&map_b, g.B, g.K, g.N, g.ldb, std::min(g.N, GN_MAX)))
+        return cudaErrorInvalidValue;
+    const int sp = gemm_splits(g, ws_floats);
+    dim3 grid((g.M + GM - 1) / GM, (g.N + GN_MAX - 1) / GN_MAX, sp);
+    if (sp == 1) {
+        gemm_bf16_tc_kernel<<<grid, GEMM_THREADS, GEMM_SMEM_LAUNCH, st>>>(g, map_a, map_b);
+        return cudaGetLastError();
+    }
+    GemmArgs gs = g;
+    gs.out_f32 = ws;
+    gs.ldo = g.N;
+    gs.split_stride = (size_t)g.M * g.N;
+    gemm_bf16_tc_kernel<<<grid, GEMM_THREADS, GEMM_SMEM_LAUNCH, st>>>(gs, map_a, map_b);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    splitk_reduce_kernel<<<device_sms() * 2, 256, 0, st>>>(ws, sp, g.M, g.N, g.out_f32, g.ldo);
     return cudaGetLastError();
 }
 
-// One network layer over M rows with the weights resident in shared memory (mlp_gemm.cuh).
+// One network layer over M rows with the weights resident in shared memory (mlp_gemm.cuh):
+// N and K multiples of 64 up to 256.
 static cudaError_t launch_layer(const GemmArgs &g, int nsm, cudaStream_t st)
 {
+    if (g.N % 64 || g.N > 256 || g.K % GK || g.K > 256 || g.M <= 0) return cudaErrorInvalidValue;
+    if (g.epi == EPI_DECODE && (!g.dec_out || g.dec_n > g.N || g.dec_n > 64)) return cudaErrorInvalidValue;
     static thread_local int attr_done = -1;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -1930,8 +1997,11 @@ static cudaError_t launch_layer(const GemmArgs &g, int nsm, cudaStream_t st)
         if (e != cudaSuccess) return e;
         attr_done = dev;
     }
+    CUtensorMap map_a, map_w;
+    if (!encode_bf16_map(&map_a, g.A, g.K, g.M, g.lda, GM) || !encode_bf16_map(&map_w, g.B, g.K, g.N, g.ldb, g.N))
+        return cudaErrorInvalidValue;
     const int ntiles = (g.M + GM - 1) / GM;
-    gemm_w_resident_kernel<<<std::min(ntiles, nsm), LW_THREADS, LW_SMEM, st>>>(g);
+    gemm_w_resident_kernel<<<std::min(ntiles, nsm), LW_THREADS, LW_SMEM, st>>>(g, map_a, map_w);
     return cudaGetLastError();
 }
 
@@ -1944,7 +2014,7 @@ static bool gemm_shape_ok(int M, int N, int K, int lda, int ldb)
 extern "C" int uc_gemm_bf16(int device, int kernel, int M, int N, int K, const uint16_t *a, const uint16_t *b, float *c)
 {
     if (!a || !b || !c || !gemm_shape_ok(M, N, K, K, K)) return UC_E_ARG;
-    if (kernel != 0 && (kernel != 1 || N > 256 || N % 64 != 0 || (K != 64 && K != 128 && K != 256))) return UC_E_ARG;
+    if (kernel != 0 && (kernel != 1 || N > 256 || N % 64 != 0 || K > 256)) return UC_E_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return UC_E_CUDA;
     __nv_bfloat16 *dA = nullptr, *dB = nullptr;
     float *dC = nullptr;
@@ -1970,7 +2040,12 @@ extern "C" int uc_gemm_bf16(int device, int kernel, int M, int N, int K, const u
             cudaGetDeviceProperties(&prop, device);
             e = rc == UC_OK ? launch_layer(g, prop.multiProcessorCount, 0) : cudaSuccess;
         } else {
-            e = launch_gemm(g, 0);
+            const size_t wsf = (size_t)M * N * std::max(1, K / GK / 4);   // the largest split gemm_splits may take
+            float *ws = nullptr;
+            if (cudaMalloc((void **)&ws, wsf * sizeof(float)) != cudaSuccess) rc = UC_E_NOMEM;
+            e = rc == UC_OK ? launch_gemm(g, 0, ws, wsf) : cudaSuccess;
+            if (rc == UC_OK && e == cudaSuccess) e = cudaDeviceSynchronize();
+            cudaFree(ws);
         }
         if (rc == UC_OK && (e != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)) rc = UC_E_CUDA;
         cudaFree(zb);
@@ -1985,6 +2060,9 @@ extern "C" int uc_gemm_bf16(int device, int kernel, int M, int N, int K, const u
 }
 
 // ------------------------------------------------------------------ learned surrogate
+
+// split-K workspace of the weight-gradient GEMMs: 32 partial tiles of the largest layer (256 x 256)
+constexpr size_t MLP_WS_FLOATS = (size_t)32 * MLP_H * MLP_H;
 
 struct uc_mlp {
     int device = 0;
@@ -2006,6 +2084,7 @@ struct uc_mlp {
     int bcap = 0;
     __nv_bfloat16 *H[MLP_LAYERS] = {}, *G[MLP_LAYERS] = {}, *Ht = nullptr, *Gt = nullptr;
     float *Z[MLP_LAYERS - 1] = {}, *Out = nullptr, *T = nullptr;
+    float *ws = nullptr;           // split-K partial tiles of the weight gradients (MLP_WS_FLOATS)
     double *partial = nullptr;
     int *d_iter = nullptr, *d_t = nullptr, *idx = nullptr;
     long idx_cap = 0;
@@ -2016,7 +2095,6 @@ struct uc_mlp {
     // inference buffers
     long icap = 0;
     __nv_bfloat16 *IX = nullptr, *IH0 = nullptr, *IH1 = nullptr;
-    float *IOut = nullptr;
     int *outside = nullptr, *list = nullptr, *count = nullptr, *tlist = nullptr, *tcount = nullptr, *pass_s = nullptr;
     double *pred_s = nullptr, *err_s = nullptr;
     uc_ctx *sample = nullptr;      // compact field of the cells recomputed exactly
@@ -2204,7 +2282,7 @@ static int mlp_gemm(uc_mlp *mlp, cudaStream_t st, const __nv_bfloat16 *A, int ld
     g.A = A; g.B = B; g.lda = lda; g.ldb = ldb; g.M = M; g.N = N; g.K = K; g.epi = epi;
     g.bias = bias; g.z_in = z_in; g.z_save = z_save; g.ldz = ldz; g.out_f32 = of; g.out_bf16 = ob; g.ldo = ldo;
     g.status = mlp->status;
-    MCK(launch_gemm(g, st));
+    MCK(launch_gemm(g, st, mlp->ws, MLP_WS_FLOATS));
     return UC_OK;
 }
 
@@ -2216,28 +2294,31 @@ static void mlp_free_batch(uc_mlp *mlp)
         mlp->H[l] = mlp->G[l] = nullptr;
         if (l < MLP_LAYERS - 1) { cudaFree(mlp->Z[l]); mlp->Z[l] = nullptr; }
     }
-    void **bufs[] = {(void **)&mlp->Ht, (void **)&mlp->Gt, (void **)&mlp->Out, (void **)&mlp->T, (void **)&mlp->partial};
+    void **bufs[] = {(void **)&mlp->Ht, (void **)&mlp->Gt, (void **)&mlp->Out, (void **)&mlp->T, (void **)&mlp->partial,
+                     (void **)&mlp->ws};
     for (auto b : bufs) { cudaFree(*b); *b = nullptr; }
     mlp->bcap = 0;
 }
 
 // forward layer l over M rows (weights resident in shared memory)
 static int mlp_layer(uc_mlp *mlp, cudaStream_t st, const __nv_bfloat16 *A, int lda, int l, int M, int epi,
-                     float *z_save, float *of, __nv_bfloat16 *ob)
+                     float *z_save, float *of, __nv_bfloat16 *ob, double *dec_out = nullptr, int dec_ld = 0)
 {
     GemmArgs g{};
+    if (epi == EPI_DECODE) {           // the output layer decoded into omega [52][dec_ld] (FP64)
+        const char *nb = reinterpret_cast<const char *>(mlp->dnorm);
+        g.dec_sd = reinterpret_cast<const float *>(nb + offsetof(MlpNorm, tgt_sd));
+        g.dec_mu = reinterpret_cast<const float *>(nb + offsetof(MlpNorm, tgt_mu));
+        g.dec_scale = reinterpret_cast<const float *>(nb + offsetof(MlpNorm, tgt_scale));
+        g.dec_out = dec_out;
+        g.dec_ld = dec_ld;
+        g.dec_n = MLP_NO;
+    }
     g.A = A; g.lda = lda; g.B = mlp->wb + mlp->bfoff[l]; g.ldb = mlp->in[l];
     g.M = M; g.N = mlp->out[l]; g.K = mlp->in[l]; g.epi = epi; g.bias = mlp->w + mlp->boff[l];
     g.z_save = z_save; g.ldz = MLP_H; g.out_f32 = of; g.out_bf16 = ob; g.ldo = mlp->out[l];
     g.status = mlp->status;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    static thread_local int nsm = 0, nsm_dev = -1;
-    if (nsm_dev != dev) {
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        nsm_dev = dev;
-    }
-    MCK(launch_layer(g, nsm, st));
+    MCK(launch_layer(g, device_sms(), st));
     return UC_OK;
 }
 
@@ -2254,7 +2335,7 @@ static int mlp_batch_buffers(uc_mlp *mlp, int B)
     }
     if ((rc = mlp_alloc(mlp, &mlp->Ht, (size_t)B * MLP_H)) || (rc = mlp_alloc(mlp, &mlp->Gt, (size_t)B * MLP_H)) ||
         (rc = mlp_alloc(mlp, &mlp->Out, (size_t)B * MLP_OUT)) || (rc = mlp_alloc(mlp, &mlp->T, (size_t)B * MLP_OUT)) ||
-        (rc = mlp_alloc(mlp, &mlp->partial, 1024)))
+        (rc = mlp_alloc(mlp, &mlp->partial, 1024)) || (rc = mlp_alloc(mlp, &mlp->ws, MLP_WS_FLOATS)))
         return rc;
     mlp->bcap = B;
     return UC_OK;
@@ -2285,7 +2366,7 @@ static int mlp_enqueue_fwd_bwd(uc_mlp *mlp, int B, float *loss_hist)
         // dW[out][in] = G^T H over the batch
         RET_IF(mlp_gemm(mlp, st, mlp->Gt, B, mlp->Ht, B, out, in, B, EPI_F32, nullptr, nullptr, nullptr, 0,
                         mlp->g + mlp->woff[l], nullptr, in));
-        bias_grad_kernel<<<(out + 31) / 32, dim3(32, 8), 0, st>>>(mlp->G[l], B, out, mlp->g + mlp->boff[l]);
+        bias_grad_kernel<<<(out + 7) / 8, 256, 0, st>>>(mlp->Gt, B, out, mlp->g + mlp->boff[l]);
         MCK(cudaGetLastError());
         if (l > 0)   // gradient w.r.t. the previous pre-activation: (G W) * gelu'(z)
             RET_IF(mlp_gemm(mlp, st, mlp->G[l], out, mlp->wbt + mlp->bfoff[l], out, B, in, out, EPI_DGELU, nullptr,
@@ -2421,18 +2502,17 @@ extern "C" int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats)
     if (mlp->icap < np) {
         // grown to the largest field seen (the buffers of a smaller one are released first)
         CK(cudaStreamSynchronize(ctx->stream));
-        void *old[] = {mlp->IX, mlp->IH0, mlp->IH1, mlp->IOut, mlp->outside, mlp->list, mlp->count, mlp->tlist,
+        void *old[] = {mlp->IX, mlp->IH0, mlp->IH1, mlp->outside, mlp->list, mlp->count, mlp->tlist,
                        mlp->tcount, mlp->pass_s, mlp->pred_s, mlp->err_s};
         for (void *b : old)
             if (b) cudaFree(b);
         mlp->IX = mlp->IH0 = mlp->IH1 = nullptr;
-        mlp->IOut = nullptr;
         mlp->outside = mlp->list = mlp->count = mlp->tlist = mlp->tcount = mlp->pass_s = nullptr;
         mlp->pred_s = mlp->err_s = nullptr;
         if (mlp->sample) { uc_destroy(mlp->sample); mlp->sample = nullptr; }
         mlp->icap = 0;
         if ((rc = mlp_alloc(mlp, &mlp->IX, (size_t)np * MLP_IN)) || (rc = mlp_alloc(mlp, &mlp->IH0, (size_t)np * MLP_H)) ||
-            (rc = mlp_alloc(mlp, &mlp->IH1, (size_t)np * MLP_H)) || (rc = mlp_alloc(mlp, &mlp->IOut, (size_t)np * MLP_OUT)) ||
+            (rc = mlp_alloc(mlp, &mlp->IH1, (size_t)np * MLP_H)) ||
             (rc = mlp_alloc(mlp, &mlp->outside, (size_t)np)) || (rc = mlp_alloc(mlp, &mlp->list, (size_t)np)) ||
             (rc = mlp_alloc(mlp, &mlp->count, 1)) || (rc = mlp_alloc(mlp, &mlp->tlist, (size_t)nt)) ||
             (rc = mlp_alloc(mlp, &mlp->tcount, 1)) || (rc = mlp_alloc(mlp, &mlp->pass_s, (size_t)ns)) ||
@@ -2453,12 +2533,10 @@ extern "C" int uc_mlp_omega(uc_mlp *mlp, uc_ctx *ctx, double tol, double *stats)
     __nv_bfloat16 *hin = mlp->IX, *hb[2] = {mlp->IH0, mlp->IH1};
     for (int l = 0; l < MLP_LAYERS; ++l) {
         const bool last = l == MLP_LAYERS - 1;
-        RET_IF(mlp_layer(mlp, st, hin, mlp->in[l], l, np, last ? EPI_BIAS_F32 : EPI_BIAS_GELU, nullptr,
-                         last ? mlp->IOut : nullptr, last ? nullptr : hb[l & 1]));
+        RET_IF(mlp_layer(mlp, st, hin, mlp->in[l], l, np, last ? EPI_DECODE : EPI_BIAS_GELU, nullptr, nullptr,
+                         last ? nullptr : hb[l & 1], last ? ctx->qdsp : nullptr, np));
         if (!last) hin = hb[l & 1];
     }
-    mlp_decode_kernel<<<grid, 256, 0, st>>>(mlp->dnorm, mlp->IOut, np, ctx->qdsp, np, 0);
-    CK(cudaGetLastError());
     if (std::isinf(tol)) {          // the network alone: no checks, no fallback
         if (stats) {
             CK(cudaStreamSynchronize(st));
@@ -2563,7 +2641,7 @@ extern "C" void uc_mlp_destroy(uc_mlp *mlp)
     if (mlp->train_exec) cudaGraphExecDestroy(mlp->train_exec);
     if (mlp->train_graph) cudaGraphDestroy(mlp->train_graph);
     void *bufs[] = {mlp->dnorm, mlp->w, mlp->g, mlp->m, mlp->v, mlp->wb, mlp->wbt, mlp->Xall, mlp->Tall,
-                    mlp->d_iter, mlp->d_t, mlp->idx, mlp->loss_hist, mlp->IX, mlp->IH0, mlp->IH1, mlp->IOut,
+                    mlp->d_iter, mlp->d_t, mlp->idx, mlp->loss_hist, mlp->IX, mlp->IH0, mlp->IH1,
                     mlp->outside, mlp->list, mlp->count, mlp->tlist, mlp->tcount, mlp->pass_s, mlp->pred_s,
                     mlp->err_s, mlp->status};
     for (void *b : bufs)
