@@ -41,6 +41,11 @@ extern "C" {
 #define UC_E_STATE -3      /* call order: e.g. update before fields were uploaded */
 #define UC_E_TIMEOUT -4    /* a device-side bounded wait gave up */
 #define UC_E_NOCONV -5     /* a bounded iteration did not converge (reported, not fatal) */
+/* The device kernels record UC_E_NOCONV (a cell's T Newton ran out of its 100
+ * steps, as the reference reports and carries on from) in a status word that
+ * the next call which synchronises the stream reads and clears: a call that
+ * returns UC_E_NOCONV has completed its own work, the non-convergence may come
+ * from an earlier asynchronous call (e.g. uc_temperature_from_held). */
 #define UC_E_NOMEM -6      /* device allocation failed */
 
 typedef struct uc_ctx uc_ctx;

@@ -65,6 +65,7 @@ struct GemmArgs {
     __nv_bfloat16 *out_bf16;      // [M][ldo]
     int ldo;
     size_t split_stride;          // split-K: CTA z writes its FP32 partial tile at out_f32 + z * split_stride
+    int ntile;                    // tiled GEMM: columns per CTA tile (0: GN_MAX)
     const float *dec_sd, *dec_mu, *dec_scale;   // EPI_DECODE: per-output scaling
     double *dec_out;              // EPI_DECODE: [dec_n][dec_ld] FP64, row r of the layer -> column r
     int dec_ld, dec_n;
@@ -159,10 +160,11 @@ __global__ void __launch_bounds__(GEMM_THREADS)
     __shared__ uint32_t s_tmem;
     __shared__ volatile int s_abort;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * GM, n0 = blockIdx.y * GN_MAX;
-    const int nt = min(GN_MAX, g.N - n0);                     // multiple of 16
+    const int ntile = g.ntile > 0 ? g.ntile : GN_MAX;        // columns per CTA tile (multiple of 16, <= 256)
+    const int m0 = blockIdx.x * GM, n0 = blockIdx.y * ntile;
+    const int nt = min(ntile, g.N - n0);                      // multiple of 16
     const uint32_t ncols = nt <= 32 ? 32 : nt <= 64 ? 64 : nt <= 128 ? 128 : 256;
-    const uint32_t b_bytes = (uint32_t)min(g.N, GN_MAX) * GK * 2;     // the B box (rows past N read as zeros)
+    const uint32_t b_bytes = (uint32_t)min(g.N, ntile) * GK * 2;      // the B box (rows past N read as zeros)
     // this CTA's K chunks
     const int nk_all = g.K / GK, per = (nk_all + gridDim.z - 1) / gridDim.z;
     const int c_beg = blockIdx.z * per, nck = min(nk_all, c_beg + per) - c_beg;

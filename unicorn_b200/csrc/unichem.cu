@@ -1961,17 +1961,24 @@ static cudaError_t launch_gemm(const GemmArgs &g, cudaStream_t st, float *ws, si
         if (e != cudaSuccess) return e;
         attr_done = dev;
     }
+    const int sp = gemm_splits(g, ws_floats);
+    // without a split, narrower column tiles where 256-column ones would leave SMs idle (one row per
+    // thread in the epilogue: more CTAs, more rows in flight)
+    GemmArgs gt = g;
+    gt.ntile = GN_MAX;
+    const int mt = (g.M + GM - 1) / GM;
+    while (sp == 1 && gt.ntile > 64 && mt * ((g.N + gt.ntile - 1) / gt.ntile) < device_sms() && gt.ntile / 2 < g.N)
+        gt.ntile /= 2;
     CUtensorMap map_a, map_b;
     if (!encode_bf16_map(&map_a, g.A, g.K, g.M, g.lda, GM) ||
-        !encode_bf16_map(&map_b, g.B, g.K, g.N, g.ldb, std::min(g.N, GN_MAX)))
+        !encode_bf16_map(&map_b, g.B, g.K, g.N, g.ldb, std::min(g.N, gt.ntile)))
         return cudaErrorInvalidValue;
-    const int sp = gemm_splits(g, ws_floats);
-    dim3 grid((g.M + GM - 1) / GM, (g.N + GN_MAX - 1) / GN_MAX, sp);
+    dim3 grid(mt, (g.N + gt.ntile - 1) / gt.ntile, sp);
     if (sp == 1) {
-        gemm_bf16_tc_kernel<<<grid, GEMM_THREADS, GEMM_SMEM_LAUNCH, st>>>(g, map_a, map_b);
+        gemm_bf16_tc_kernel<<<grid, GEMM_THREADS, GEMM_SMEM_LAUNCH, st>>>(gt, map_a, map_b);
         return cudaGetLastError();
     }
-    GemmArgs gs = g;
+    GemmArgs gs = gt;
     gs.out_f32 = ws;
     gs.ldo = g.N;
     gs.split_stride = (size_t)g.M * g.N;

@@ -178,7 +178,13 @@ class UniChem:
 
     # ------------------------------------------------------------ plumbing
     def _ck(self, rc: int):
-        if rc != 0:
+        # UC_E_NOCONV (-5): a T Newton ran out of steps in some cell, recorded by an asynchronous
+        # kernel and reported at the next synchronising call, whose own work has completed; the
+        # reference prints a message and carries on, so it is a warning here
+        if rc == -5:
+            import warnings
+            warnings.warn(self.lib.uc_last_error(self._h).decode())
+        elif rc != 0:
             raise UniChemError(rc, self.lib.uc_last_error(self._h).decode())
 
     def close(self):
@@ -273,18 +279,20 @@ class UniChem:
         fs = _in(face_sum, (LSP - 1, self.n))
         fn = _in(face_nbr, (LSP - 1, self.n))
         passes = ctypes.c_int(0)
-        self._ck(self.lib.uc_species_update(self._h, dt, int(isor), relx, tol, spnorm, _p(fs), _p(fn),
-                                            ctypes.byref(passes)))
+        self._ck_warn(self.lib.uc_species_update(self._h, dt, int(isor), relx, tol, spnorm, _p(fs), _p(fn),
+                                                 ctypes.byref(passes)))
         return passes.value
 
     def sweep(self, dt: float, precision: int = FP64, isor: int = 100, relx: float = 0.99, tol: float = 1e-8,
               spnorm: float = 0.0, face_sum=None, face_nbr=None) -> int:
-        """One species sweep: props, cp/h, rates + omega, point-implicit update."""
+        """One species sweep: props, cp/h, rates + omega, point-implicit update. A T Newton of an
+        earlier asynchronous call that ran out of steps (reported when this call synchronises) is a
+        warning, as the reference prints one and carries on; the sweep itself has completed."""
         fs = _in(face_sum, (LSP - 1, self.n))
         fn = _in(face_nbr, (LSP - 1, self.n))
         passes = ctypes.c_int(0)
-        self._ck(self.lib.uc_sweep(self._h, precision, dt, int(isor), relx, tol, spnorm, _p(fs), _p(fn),
-                                   ctypes.byref(passes)))
+        self._ck_warn(self.lib.uc_sweep(self._h, precision, dt, int(isor), relx, tol, spnorm, _p(fs), _p(fn),
+                                        ctypes.byref(passes)))
         return passes.value
 
     def chem_props(self, precision: int = FP64):
