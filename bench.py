@@ -15,9 +15,10 @@ runs the same sweep on chunks of the same field.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 ``value`` is device-resident FP64 throughput (fields already on the GPU);
-``e2e`` is the same sweep through the C ABI with the step's inputs copied
-from pinned host memory and its outputs copied back, inside the timed
-region. ``forms`` compares, on the same field, the FP64 form with the mixed
+``e2e`` is the same sweep through the C ABI (uc_sweep_host) with the step's
+inputs copied from pinned host memory and its outputs copied back, inside
+the timed region; the outputs of the properties and rates are copied while
+the species update runs. ``forms`` compares, on the same field, the FP64 form with the mixed
 form and with the learned surrogate plus per-cell fallback, with the error
 of each against FP64; ``c2`` is the FP64 sweep of the 601x301 heptane jet
 field. ``--impl reference`` times the reference's own routines (translated
@@ -518,10 +519,9 @@ def main_ours(args):
     t0 = time.perf_counter()
     e2e_passes = []
     for _ in range(args.steps):
-        u.upload(h_tk, h_rho, h_y)
-        e2e_passes.append(u.sweep(DT, precision=unichem.FP64, isor=args.isor, relx=RELX, tol=TOL))
-        u.download_outputs(outs)
-        u.lib.uc_download_fields(u._h, None, None, unichem._p(h_yout), None, None)
+        # uc_sweep_host: upload, sweep, outputs copied back while the species update runs, updated Y
+        e2e_passes.append(u.sweep_host(h_tk, h_rho, h_y, out=outs, y_out=h_yout, dt=DT, precision=unichem.FP64,
+                                       isor=args.isor, relx=RELX, tol=TOL))
     u.sync()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     passes_run = float(np.mean([min(p, args.isor) for p in passes]))

@@ -161,6 +161,25 @@ int uc_temperature_from_h(uc_ctx *ctx, const double *ht);
 int uc_sweep(uc_ctx *ctx, int precision, double dt, int isor, double relx, double tol, double spnorm,
              const double *face_sum, const double *face_nbr, int *passes);
 
+/* Host buffers of one uc_sweep_host call (each [n] or [52][n] like the
+ * upload and download calls; any output may be NULL = not copied; stmf/stnd
+ * in may be NULL = zero). */
+typedef struct {
+    const double *tk, *rho, *fsp, *stmf, *stnd;             /* state in */
+    double *qdsp, *qdot, *domega_dy, *vmu, *vtc, *vdf, *cp, *h;   /* outputs of the sweep's first steps */
+    double *fsp_out, *stmf_out, *stnd_out;                  /* state after the update */
+} uc_host_io;
+
+/* One species sweep on host buffers: uc_upload_fields(tk, rho, fsp, stmf,
+ * stnd), uc_sweep(...), uc_download_outputs(...) and the updated Y and soot,
+ * with the same results as those calls in that order. The outputs of the
+ * properties, cp/h and the rates are final before the species update starts,
+ * so they are copied to the host on a second stream while the update runs;
+ * only the updated state is copied after it. The host buffers may be pinned
+ * (copies asynchronous) or pageable. Returns when every copy has landed. */
+int uc_sweep_host(uc_ctx *ctx, int precision, double dt, int isor, double relx, double tol, double spnorm,
+                  const double *face_sum, const double *face_nbr, const uc_host_io *io, int *passes);
+
 /* The chemistry and properties of the device-resident state without the
  * update: the Y clip with transport properties, cp and h, then omega and
  * d(omega)/dY (the first three steps of uc_sweep, in its order; no RC plane is

@@ -47,6 +47,8 @@ struct RelaxBuffers {
 struct uc_ctx {
     int device = 0, n = 0, npad = 0, ntile = 0, nsm = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t io_stream = nullptr;  // uc_sweep_host: copies of the outputs while the update runs
+    cudaEvent_t io_event = nullptr;
     uc_scales sc{};
     uc_inputs inputs{};               // the input-card values of uc_init
     DevParams *hP = nullptr;          // host copy
@@ -396,6 +398,8 @@ static void free_ctx(uc_ctx *c)
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     c->ev_pool.clear();
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->io_stream) cudaStreamDestroy(c->io_stream);
+    if (c->io_event) cudaEventDestroy(c->io_event);
     delete c->hP;
 }
 
@@ -1119,6 +1123,60 @@ extern "C" int uc_sweep(uc_ctx *ctx, int precision, double dt, int isor, double 
     ctx->have_rc = true;
     ctx->rc_start = false;
     return uc_species_update(ctx, dt, isor, relx, tol, spnorm, face_sum, face_nbr, passes);
+}
+
+extern "C" int uc_sweep_host(uc_ctx *ctx, int precision, double dt, int isor, double relx, double tol,
+                             double spnorm, const double *face_sum, const double *face_nbr, const uc_host_io *io,
+                             int *passes)
+{
+    if (!ctx) return UC_E_ARG;
+    if (!io) return set_err(ctx, UC_E_ARG, "uc_sweep_host: io is required");
+    if (precision != UC_FP64 && precision != UC_MIXED) return set_err(ctx, UC_E_ARG, "unknown precision %d", precision);
+    RET_IF(uc_upload_fields(ctx, io->tk, io->rho, io->fsp, io->stmf, io->stnd));
+    RET_IF(props_impl(ctx, precision, nullptr, nullptr, nullptr));
+    if (ctx->have_grid && ctx->have_flow && !face_sum && !face_nbr)
+        RET_IF(uc_assemble_faces(ctx, dt, nullptr, nullptr, nullptr, nullptr));
+    RET_IF(cp_h_impl(ctx, precision, nullptr, nullptr));
+    CK(cudaSetDevice(ctx->device));
+    RET_IF(launch_chem(ctx, precision, true, true));
+    ctx->have_rc = true;
+    ctx->rc_start = false;
+    if (!ctx->io_stream) {
+        CK(cudaStreamCreateWithFlags(&ctx->io_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->io_event, cudaEventDisableTiming));
+    }
+    // the properties, cp/h, omega and d(omega)/dY are final here: the side stream copies them after this
+    // point while the update (which writes only Y and soot) runs on the context's stream
+    CK(cudaEventRecord(ctx->io_event, ctx->stream));
+    RET_IF(uc_species_update(ctx, dt, isor, relx, tol, spnorm, face_sum, face_nbr, nullptr));
+    CK(cudaStreamWaitEvent(ctx->io_stream, ctx->io_event, 0));
+    struct { double *dst; const double *src; int rows; } o[] = {
+        {io->qdsp, ctx->qdsp, LSP}, {io->qdot, ctx->qdot, 1}, {io->domega_dy, ctx->dwdy, LSP}, {io->vmu, ctx->vmu, 1},
+        {io->vtc, ctx->vtc, 1}, {io->vdf, ctx->vdf, LSP}, {io->cp, ctx->cp, 1}, {io->h, ctx->h, 1}};
+    cudaError_t ce = cudaSuccess;
+    for (auto &x : o)
+        if (x.dst && x.src && ce == cudaSuccess)
+            ce = cudaMemcpy2DAsync(x.dst, (size_t)ctx->n * sizeof(double), x.src, (size_t)ctx->npad * sizeof(double),
+                                   (size_t)ctx->n * sizeof(double), x.rows, cudaMemcpyDeviceToHost, ctx->io_stream);
+    // the updated state and the pass count after the update, on the context's stream
+    if (ce == cudaSuccess) {
+        if (io->fsp_out) ce = cudaMemcpy2DAsync(io->fsp_out, (size_t)ctx->n * sizeof(double), ctx->y,
+                                                (size_t)ctx->npad * sizeof(double), (size_t)ctx->n * sizeof(double), LSP,
+                                                cudaMemcpyDeviceToHost, ctx->stream);
+        if (ce == cudaSuccess && io->stmf_out)
+            ce = cudaMemcpyAsync(io->stmf_out, ctx->soot, (size_t)ctx->n * sizeof(double), cudaMemcpyDeviceToHost,
+                                 ctx->stream);
+        if (ce == cudaSuccess && io->stnd_out)
+            ce = cudaMemcpyAsync(io->stnd_out, ctx->soot + ctx->npad, (size_t)ctx->n * sizeof(double),
+                                 cudaMemcpyDeviceToHost, ctx->stream);
+        if (ce == cudaSuccess && passes)
+            ce = cudaMemcpyAsync(passes, ctx->passes, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    }
+    // both streams drained before returning, also after an error (the host buffers must not be written later)
+    const cudaError_t e1 = cudaStreamSynchronize(ctx->io_stream), e2 = cudaStreamSynchronize(ctx->stream);
+    if (ce == cudaSuccess) ce = e1 != cudaSuccess ? e1 : e2;
+    if (ce != cudaSuccess) return set_err(ctx, UC_E_CUDA, "uc_sweep_host: %s", cudaGetErrorString(ce));
+    return check_status(ctx);
 }
 
 extern "C" int uc_download_outputs(uc_ctx *ctx, double *qdsp, double *qdot, double *domega_dy, double *vmu,

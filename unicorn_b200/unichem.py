@@ -76,6 +76,13 @@ class EnthalpyOpts(ctypes.Structure):
                 ("hnorm", ctypes.c_double), ("sigh", ctypes.c_double)]
 
 
+class HostIO(ctypes.Structure):
+    """uc_host_io: the host buffers of one uc_sweep_host call (NULL = not copied)."""
+    _fields_ = [(k, ctypes.POINTER(ctypes.c_double)) for k in
+                ("tk", "rho", "fsp", "stmf", "stnd", "qdsp", "qdot", "domega_dy", "vmu", "vtc", "vdf", "cp", "h",
+                 "fsp_out", "stmf_out", "stnd_out")]
+
+
 def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     """Load libunichem.so; raises if it is missing (no CPU fallback exists)."""
     global _lib
@@ -101,6 +108,8 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
     lib.uc_sweep.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                              ctypes.c_double, P, P, ctypes.POINTER(ctypes.c_int)]
     lib.uc_download_outputs.argtypes = [vp, P, P, P, P, P, P, P, P]
+    lib.uc_sweep_host.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, P, P, ctypes.POINTER(HostIO), ctypes.POINTER(ctypes.c_int)]
     lib.uc_chem_props.argtypes = [vp, ctypes.c_int]
     lib.uc_set_iskip.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     lib.uc_profile.argtypes = [vp, ctypes.c_int]
@@ -134,6 +143,13 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _host(a, shape):
+    """A host array used in place by a call (no copy): float64, C-contiguous, of the given shape."""
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous or a.shape != shape:
+        raise ValueError(f"expected a C-contiguous float64 array of shape {shape}")
+    return a
 
 
 def _in(a, shape=None):
@@ -293,6 +309,33 @@ class UniChem:
         passes = ctypes.c_int(0)
         self._ck_warn(self.lib.uc_sweep(self._h, precision, dt, int(isor), relx, tol, spnorm, _p(fs), _p(fn),
                                         ctypes.byref(passes)))
+        return passes.value
+
+    def sweep_host(self, tk, rho, y, out: dict | None = None, y_out=None, soot=None, soot_out=None, dt: float = 1e-5,
+                   precision: int = FP64, isor: int = 100, relx: float = 0.99, tol: float = 1e-8, spnorm: float = 0.0,
+                   face_sum=None, face_nbr=None) -> int:
+        """uc_sweep_host: upload (tk, rho, y[, soot = (stmf, stnd)]), one sweep, and the outputs (keys of
+        download_outputs) and the updated Y (and soot) into the given host arrays; the output copies
+        overlap the species update. The arrays are used in place (pinned ones make the copies
+        asynchronous): float64, C-contiguous, of the shapes of upload/download_outputs."""
+        n = self.n
+        chk = lambda a, shape: None if a is None else _host(a, shape)
+        io = HostIO()
+        io.tk, io.rho, io.fsp = _p(chk(tk, (n,))), _p(chk(rho, (n,))), _p(chk(y, (LSP, n)))
+        if soot is not None:
+            io.stmf, io.stnd = _p(chk(soot[0], (n,))), _p(chk(soot[1], (n,)))
+        out = out or {}
+        shapes = dict(qdsp=(LSP, n), qdot=(n,), domega_dy=(LSP, n), vmu=(n,), vtc=(n,), vdf=(LSP, n), cp=(n,), h=(n,))
+        for k, shape in shapes.items():
+            setattr(io, k, _p(chk(out.get(k), shape)))
+        io.fsp_out = _p(chk(y_out, (LSP, n)))
+        if soot_out is not None:
+            io.stmf_out, io.stnd_out = _p(chk(soot_out[0], (n,))), _p(chk(soot_out[1], (n,)))
+        fs = _in(face_sum, (LSP - 1, n))
+        fn = _in(face_nbr, (LSP - 1, n))
+        passes = ctypes.c_int(0)
+        self._ck(self.lib.uc_sweep_host(self._h, precision, dt, int(isor), relx, tol, spnorm, _p(fs), _p(fn),
+                                        ctypes.byref(io), ctypes.byref(passes)))
         return passes.value
 
     def chem_props(self, precision: int = FP64):
