@@ -467,6 +467,22 @@ class Oracle:
                              _dptr(out))
         return out
 
+    def enthalpy_total(self, tk, y):
+        """Total enthalpy per cell at its own T (the quantity uc_hold_enthalpy holds)."""
+        enth = np.empty(len(tk))
+        self.lib.orc_enthalpy_total(len(tk), _dptr(_c(tk)), _dptr(_c(y)), _dptr(enth))
+        return enth
+
+    def temperature_held(self, tk_guess, y, pnd, enth, with_conv=False):
+        """(tk, rho) from the held total enthalpy and new Y, rho at the cell pressure; with_conv adds
+        per cell whether the Newton met its step rule."""
+        tk = np.array(tk_guess, dtype=np.float64, copy=True)
+        rho = np.empty(len(tk))
+        conv = np.zeros(len(tk), dtype=np.int32)
+        self.lib.orc_temperature_held(len(tk), _dptr(tk), _dptr(rho), _dptr(_c(y)), _dptr(_c(pnd)), _dptr(_c(enth)),
+                                      _iptr(conv))
+        return (tk, rho, conv.astype(bool)) if with_conv else (tk, rho)
+
     def temperature(self, tk_guess, y, ht):
         tk = np.array(tk_guess, dtype=np.float64, copy=True)
         self.lib.orc_temperature(len(tk), _dptr(tk), _dptr(_c(y)), _dptr(_c(ht)))

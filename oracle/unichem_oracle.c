@@ -742,7 +742,14 @@ int orc_species_update(int n, const double *rho, const double *y0, double *y, co
  * enthalpy ht (FPZ) and the mass fractions; tk holds the guess on entry. */
 /* Newton for T at the total enthalpy ENTH (solveh.f:1186-1234); y has
  * stride ys between species. Returns the new non-dimensional tk. */
+static double temperature_cell_conv(double tk, const double *y, size_t ys, double ENTH, int *conv);
 static double temperature_cell(double tk, const double *y, size_t ys, double ENTH)
+{
+    return temperature_cell_conv(tk, y, ys, ENTH, NULL);
+}
+
+/* conv (optional) receives 1 when the Newton met its step rule within 100 steps */
+static double temperature_cell_conv(double tk, const double *y, size_t ys, double ENTH, int *conv)
 {
     const double TKDMIN = S.TSTR - 1.0;
     int IPL = 0;
@@ -770,11 +777,15 @@ static double temperature_cell(double tk, const double *y, size_t ys, double ENT
         if (TKD <= TPOLY) TKD = T.tpol2 / 2.0;
         TPOLY = T.tpol2;
     }
+    if (conv) *conv = 0;
     for (int it = 1; it <= 100; ++it) {
         double DTKD = ((A1 + (A2 + (A3 + (A4 + A5 * TKD) * TKD) * TKD) * TKD) * TKD + A6
                        - ENTH * S.WMSTR / S.GASC)
                       / (A1 + (2.0 * A2 + (3.0 * A3 + (4.0 * A4 + 5.0 * A5 * TKD) * TKD) * TKD) * TKD);
-        if (fabs(DTKD) <= F(0.001)) break;
+        if (fabs(DTKD) <= F(0.001)) {
+            if (conv) *conv = 1;
+            break;
+        }
         TKD = TKD - DTKD;
     }
     if (TKD > T.tpol2) TKD = T.tpol2;
@@ -812,6 +823,31 @@ static double enthalpy_total(double tk, const double *y, size_t ys)
         A6 = A6 + a[5] * yk / S.WM[k];
     }
     return ((A1 + (A2 + (A3 + (A4 + A5 * TKD) * TKD) * TKD) * TKD) * TKD + A6) * S.GASC / S.WMSTR;
+}
+
+/* The in-loop T update of the sweep loop (uc_hold_enthalpy, uc_temperature_from_held):
+ * each cell's total enthalpy at its own T is held; after the species update T
+ * follows from the held enthalpy and the new mass fractions by the Newton of
+ * solveh.f:1186-1234 (T clamped to [TSTR-1, TPOL2] as there), and rho from the
+ * ideal gas at the cell pressure (main:1056-1062, RHO = P/(BETA1 TK sum Y/W)).
+ * The same step that orc_integrate takes per sub-step; conv (optional) [n]
+ * receives 1 where the Newton met its step rule (the reference prints a
+ * message where it did not, and carries on). */
+void orc_enthalpy_total(int n, const double *tk, const double *y, double *enth)
+{
+    for (int c = 0; c < n; ++c) enth[c] = enthalpy_total(tk[c], y + c, (size_t)n);
+}
+
+void orc_temperature_held(int n, double *tk, double *rho, const double *y, const double *pnd, const double *enth,
+                          int *conv)
+{
+    for (int c = 0; c < n; ++c) {
+        const double t = temperature_cell_conv(tk[c], y + c, (size_t)n, enth[c], conv ? conv + c : NULL);
+        double rbar = 0.0;
+        for (int k = 0; k < LSP; ++k) rbar = rbar + y[(size_t)k * n + c] / S.WM[k];
+        tk[c] = t;
+        rho[c] = pnd[c] / (S.BETA1 * t * rbar);
+    }
 }
 
 /* Sub-step count of each cell from its chemical time scale:
