@@ -45,6 +45,7 @@ UNIT = "cell-updates/s"
 DT = 1e-3            # non-dimensional: 1e-5 s / TMSTR (0.01 s)
 ISOR, RELX, TOL = 100, 0.99, 1e-8     # docs/input.uni:25-27
 NZ, NR, FUEL, TPEAK = 601, 301, 11, 2300.0
+C5_HEAD_SWEEPS = 100   # in-loop sweeps reported in the headline line (the full run: --workload c5)
 HEAD_CELLS, HEAD_SEED = 1 << 20, 7
 TRAIN_STATES, TRAIN_STEPS = 4 << 20, 6000
 MLP_TOLS = (1e-3, 1e-2, 1e-1)
@@ -545,6 +546,8 @@ def main_ours(args):
         u.close()
         if not args.no_c2:
             line["c2"] = run_c2(args, dev, pk)
+        if not args.no_c5:
+            line["c5"] = run_c5(args, C5_HEAD_SWEEPS)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_port(tk, rho, f.y)
         print(json.dumps(line), flush=True)
@@ -763,7 +766,9 @@ def main_c4(args):
 
 
 # ---------------------------------------------------------------- C5: in-loop sweeps
-def main_c5(args):
+def run_c5(args, sweeps):
+    """The in-loop C5 run over `sweeps` sweeps: timing and checkpoint report of the FP64 and mixed forms
+    (with the omega errors of the mixed kernel and the surrogate at the checkpoints)."""
     import torch
     from unicorn_b200 import unichem
     from unicorn_b200.fields import jet_field, nondimensional
@@ -771,7 +776,7 @@ def main_c5(args):
     from unicorn_b200.surrogate import Surrogate, raw_features
     f = jet_field(NZ, NR, fuel=FUEL, t_peak=TPEAK, seed=0)
     n = f.n
-    checkpoints = sorted({c for c in (100, 500, 1000, args.sweeps) if c <= args.sweeps})
+    checkpoints = sorted({c for c in (100, 500, 1000, sweeps) if c <= sweeps})
     # ---- surrogate trained on four other seeded fields of the same generator
     s = Surrogate(capacity=4 * n, seed=1)
     u = unichem.UniChem(n)
@@ -808,7 +813,7 @@ def main_c5(args):
         ext = torch.cuda.ExternalStream(view["stream"])
         rep = {}
         ms_total, passes = 0.0, []
-        for sw in range(1, args.sweeps + 1):
+        for sw in range(1, sweeps + 1):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(ext)
             passes.append(u.sweep(DT, precision=prec, isor=ISOR, relx=RELX, tol=TOL, face_sum=fs, face_nbr=fn))
@@ -846,21 +851,26 @@ def main_c5(args):
                               "omega_err_mlp_p50": float(np.median(e_ml)), "omega_err_mlp_p99": float(np.quantile(e_ml, 0.99)),
                               "mlp_cells_exact_at_1e-3": round(fb["cells_exact"], 4)})
                 rep[f"sweep_{sw}"] = entry
-        timing[name] = {"ms_per_sweep": round(ms_total / args.sweeps, 3),
-                        "cell_updates_per_s": round(n * args.sweeps / (ms_total / 1e3), 1)}
+        timing[name] = {"ms_per_sweep": round(ms_total / sweeps, 3),
+                        "cell_updates_per_s": round(n * sweeps / (ms_total / 1e3), 1)}
         report[name] = rep
         u.close()
     probe.close()
     s.close()
+    return {"workload": f"C5: 601x301 heptane field, {sweeps} sweeps of dt=1e-5 s, transport frozen "
+                        "(diffusion faces from the initial field), T from held enthalpy each sweep",
+            "timing": timing, "report": report,
+            "surrogate": {"train_steps": args.train_steps, "train_states": 4 * n,
+                          "loss_first": float(loss[:10].mean()), "loss_last": float(loss[-50:].mean())}}
+
+
+def main_c5(args):
+    c5 = run_c5(args, args.sweeps)
+    fp = c5["timing"]["fp64"]
     line = {"metric": "in-loop heptane sweeps: peak-T drift, sum-Y drift and omega error at sweeps 100/500/1000",
-            "value": timing["fp64"]["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.sweeps, "warmup": 0,
-            "ms_per_step": timing["fp64"]["ms_per_sweep"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64 (and mixed)", "data": "synthetic (seeded C2 generator)",
-            "config": {"workload": f"C5: 601x301 heptane field, {args.sweeps} sweeps of dt=1e-5 s, transport frozen "
-                                   "(diffusion faces from the initial field), T from held enthalpy each sweep",
-                       "timing": timing, "report": report,
-                       "surrogate": {"train_steps": args.train_steps, "train_states": 4 * n,
-                                     "loss_first": float(loss[:10].mean()), "loss_last": float(loss[-50:].mean())}}}
+            "value": fp["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.sweeps, "warmup": 0,
+            "ms_per_step": fp["ms_per_sweep"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (and mixed)", "data": "synthetic (seeded C2 generator)", "config": c5}
     print(json.dumps(line), flush=True)
 
 
@@ -997,6 +1007,7 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="head: skip the mixed / surrogate comparison")
     ap.add_argument("--no-mlp", action="store_true", help="head: skip the surrogate")
     ap.add_argument("--no-c2", action="store_true", help="head: skip the 601x301 field")
+    ap.add_argument("--no-c5", action="store_true", help="head: skip the in-loop sweeps of the 601x301 field")
     args = ap.parse_args()
     if args.workload == "c3":
         main_c3(args)
