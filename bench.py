@@ -151,11 +151,13 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """The largest x over the ranks (a device tensor under NCCL, a host one under gloo)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
