@@ -596,6 +596,7 @@ def main_reference(args):
 
 # ---------------------------------------------------------------- C3: batched stiff integration
 C3_CELLS = 1 << 20
+NSUB_MAX = 200                       # the sub-step cap of the C3 options (UniChem.integrate default)
 
 
 def cpu_baseline_c3(f, ncells=2048):
@@ -678,10 +679,17 @@ def main_c3(args):
                                 "frac_1": round(float((ns == 1).mean()), 4),
                                 "frac_max": round(float((ns == ns.max()).mean()), 4)},
                        "passes_per_substep": round(float(pa.sum()) / substeps, 2),
-                       "l2": "state 470 MB > L2; all sub-step work on chip"},
+                       "shape": ("rounds form (field kernels per sub-step round, cells in n_sub order)"
+                                 if tune["int_warps"] == 3 else
+                                 f"persistent work-queue kernel, {int(tune['int_warps'])} warps"),
+                       "l2": ("state 470 MB > L2; RC plane 4.6 GB written and read back per round"
+                              if tune["int_warps"] == 3 else "state 470 MB > L2; all sub-step work on chip")},
             "e2e": {"value": round(n * args.steps / e2e, 1), "unit": UNIT, "h2d_bytes_per_step": (2 + 52) * 8 * n,
                     "d2h_bytes_per_step": (2 + 52) * 8 * n},
-            "gpu_launches": kt["integrate"][1] * (6 if tune["int_sorted"] else 3),
+            # per step: rates of the start state, n_sub, the sort (3), then the persistent kernel, or the round
+            # counts, gather, held enthalpy, 3 kernels per round (one round per possible sub-step) and scatter
+            "gpu_launches": kt["integrate"][1] * ((9 + 3 * NSUB_MAX) if tune["int_warps"] == 3 else
+                                                  (6 if tune["int_sorted"] else 3)),
             "clocks": clk.summary(),
             "roofline": {"kernel": "integrate", "bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64, 2),
                          "peak_source": "measured in this run: FP64 FMA loop (bench.py fp64_fma_peak)" if fp64_m else

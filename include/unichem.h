@@ -354,9 +354,15 @@ int uc_device_view_get(uc_ctx *ctx, uc_device_view *v);
  * n_sub = clamp(ceil(x / c_tau), 1, nsub_max), x = max over species with
  * Y_k > y_tau of dt*|QDSP_k| / (RCONV*rho*Y_k), QDSP of the start state.
  * The whole step (rates of the start state, n_sub, a stable sort of the
- * cells by n_sub, the persistent work-queue kernel) is one CUDA graph launch;
- * the graph is captured on the first call and again when an option or the
- * tuned kernel shape changes.
+ * cells by n_sub, then the sub-steps) is one CUDA graph launch; the graph is
+ * captured on the first call and again when an option or the tuned kernel
+ * shape changes. Two shapes run the sub-steps: the persistent work-queue
+ * kernel (each CTA advances one 32-cell tile through all its sub-steps) and,
+ * for UC_FP64, the rounds form (the cells gathered in n_sub order; round r
+ * advances the cells with n_sub > r by one sub-step with the field kernels:
+ * rates, a per-cell form of the tile-resident species update, T and rho).
+ * The rounds form holds a copy of the state in n_sub order on the device
+ * (58 doubles and 2 ints per cell) and uses the context's RC plane.
  *
  * precision: UC_FP64 (everything FP64) or UC_MIXED (the rates of every
  * sub-step and of the start state in the mixed form of uc_rates, stored as
@@ -382,8 +388,9 @@ int uc_hold_enthalpy(uc_ctx *ctx);
 int uc_temperature_from_held(uc_ctx *ctx);
 int uc_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts *o);
 /* Times each kernel shape on the current state (restored after each trial)
- * and keeps the fastest for uc_integrate; uc_stat "int_warps", "int_sorted",
- * "int_tune_best_ms", "int_tune_worst_ms" report the outcome. */
+ * and keeps the fastest for uc_integrate; uc_stat "int_warps" (16 or 8: the
+ * persistent kernel with that many warps per CTA; 3: the rounds form),
+ * "int_sorted", "int_tune_best_ms", "int_tune_worst_ms" report the outcome. */
 int uc_integrate_tune(uc_ctx *ctx, int precision, const uc_integrate_opts *o);
 /* Per-cell sub-step counts and update passes of the last uc_integrate (host [n], either may be NULL). */
 int uc_integrate_counts(uc_ctx *ctx, int *nsub, int *passes);

@@ -28,13 +28,21 @@ def cuda():
     return unichem
 
 
-def run_gpu(cuda, f, tk, rho, pnd, tune=False, **kw):
+SHAPES = {"persistent": 16, "rounds": 3}
+
+
+def run_gpu(cuda, f, tk, rho, pnd, tune=False, shape=None, monkeypatch=None, **kw):
+    if shape is not None:
+        monkeypatch.setenv("UNICHEM_INT_WARPS", str(shape))
     with cuda.UniChem(f.n) as u:
+        if shape is not None:
+            assert u.stat("int_warps") == shape
         u.upload(tk, rho, f.y)
         u.set_pressure(pnd)
         if tune:
             info = u.integrate_tune(DT, **kw)
-            assert info["int_warps"] in (8, 16) and info["int_sorted"] in (0, 1)
+            assert info["int_warps"] in (3, 8, 16) and info["int_sorted"] in (0, 1)
+            print(f"\ntuned shape: {info}")
         u.integrate(DT, **kw)
         tk1, rho1, y1, s1, s2 = u.download()
         ns, pa = u.integrate_counts()
@@ -48,9 +56,11 @@ def c3(oracle):
     return f, tk, rho, f.p / oracle.scales["PSTR"]
 
 
-def test_integrate_matches_oracle(cuda, oracle, c3):
+@pytest.mark.parametrize("form", list(SHAPES))
+def test_integrate_matches_oracle(cuda, oracle, c3, form, monkeypatch):
+    """Both shapes: the persistent work-queue kernel and the rounds form (field kernels per sub-step)."""
     f, tk, rho, pnd = c3
-    tk1, rho1, y1, s1, ns, pa = run_gpu(cuda, f, tk, rho, pnd)
+    tk1, rho1, y1, s1, ns, pa = run_gpu(cuda, f, tk, rho, pnd, shape=SHAPES[form], monkeypatch=monkeypatch)
     q = oracle.omega(tk, rho, f.y)[0]
     ns_o, x = oracle.nsub(rho, f.y, q, DT)
     near = np.abs(x - np.round(x)) <= 1e-9 * np.maximum(x, 1.0)
@@ -76,13 +86,41 @@ def test_integrate_matches_oracle(cuda, oracle, c3):
     assert (np.abs(pa - pa_o)[ok] <= ns[ok]).mean() > 0.95
 
 
-def test_kernel_shapes_agree_bitwise(cuda, oracle, c3):
-    """Every tuned shape (8 or 16 warps, sorted or natural queue order) computes each cell the same way."""
+def test_kernel_shapes_agree_bitwise(cuda, oracle, c3, monkeypatch):
+    """The persistent kernel's shapes (8 or 16 warps) compute each cell the same way; the tuner (which
+    also times the natural queue order and the rounds form) restores the state after each trial."""
     f, tk, rho, pnd = c3
-    a = run_gpu(cuda, f, tk, rho, pnd)
-    b = run_gpu(cuda, f, tk, rho, pnd, tune=True)
+    a = run_gpu(cuda, f, tk, rho, pnd, shape=16, monkeypatch=monkeypatch)
+    b = run_gpu(cuda, f, tk, rho, pnd, shape=8, monkeypatch=monkeypatch)
     for u, v in zip(a, b):
         assert np.array_equal(u, v)
+    c = run_gpu(cuda, f, tk, rho, pnd, tune=True)
+    assert np.array_equal(c[4], a[4])                    # sub-step counts of the restored start state
+
+
+def test_rounds_form_against_the_persistent_kernel(cuda, oracle, monkeypatch):
+    """4,096 cells (128 tiles, rounds whose last tile is partly live): the rounds form against the
+    persistent kernel, at the tolerances of the oracle test (the two run the same arithmetic per cell
+    except for the update's program form, two Y sets against Y in place, whose compiled contractions may
+    differ in the last bit; a per-cell pass loop stopping on 1e-8 can then move by one pass)."""
+    f = batch_cells(4096, seed=13)
+    tk, rho = nondimensional(f, oracle.scales, oracle.wm)
+    pnd = f.p / oracle.scales["PSTR"]
+    a = run_gpu(cuda, f, tk, rho, pnd, shape=16, monkeypatch=monkeypatch)
+    b = run_gpu(cuda, f, tk, rho, pnd, shape=3, monkeypatch=monkeypatch)
+    sc = oracle.scales
+    assert np.array_equal(a[4], b[4])                     # the same sub-step counts (same start-state rates)
+    Ta, Tb = a[0] * sc["TSTR"], b[0] * sc["TSTR"]
+    lo, hi = sc["TSTR"] - 1.0 + 1e-6, 5000.0 - 1e-6
+    ok = (Ta > lo) & (Ta < hi) & (Tb > lo) & (Tb < hi)
+    print(f"\nrounds vs persistent: cells on the T clamp {(~ok).sum()} of 4096; passes equal "
+          f"{(a[5] == b[5]).mean():.4f}; Y bit-equal cells {np.all(a[2] == b[2], axis=0).mean():.4f}")
+    assert (~ok).mean() < 0.08
+    assert np.abs(Ta - Tb)[ok].max() < 1e-2
+    err = np.abs(b[2] - a[2]) - (1e-6 * np.abs(a[2]) + 1e-12)
+    assert (err[:, ok] <= 0).all(), f"worst Y excess {err[:, ok].max():.3g}"
+    assert np.abs(b[3] - a[3])[:, ok].max() <= 1e-12 + 1e-6 * np.abs(a[3]).max()
+    assert (np.abs(a[5] - b[5])[ok] <= a[4][ok]).mean() > 0.95
 
 
 def test_integrate_options_rejected(cuda):

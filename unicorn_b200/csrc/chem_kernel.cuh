@@ -270,6 +270,7 @@ __global__ void __launch_bounds__(CHEM_THREADS, 1) chem_fp64_kernel(const ChemAr
                     sRC[r * TILE + lane] = a.rc_stale ? a.rc_stale[(size_t)r * a.npad + cell] : 0.0;
             __syncthreads();
         }
+        if (!a.qdsp && !a.qdot && !a.dwdy) continue;      // RC and SOUR only: no species sums (uniform branch)
         const bool put = cls < 2;
         {
             const double TKD = sC[SC_TKD * TILE + lane];

@@ -225,12 +225,14 @@ __global__ void hold_enthalpy_kernel(const DevParams *Pp, const double *tk, cons
 }
 
 // T from the held total enthalpy and the current Y (solveh.f:1186-1234), then rho
-// from the ideal gas at the cell pressure (main:1056-1062)
+// from the ideal gas at the cell pressure (main:1056-1062); the first *nlive cells when nlive is given,
+// else all npad
 __global__ void temperature_held_kernel(const DevParams *Pp, const double *enth, const double *y, const double *pnd,
-                                        int npad, double *tk, double *rho, int *status)
+                                        int npad, double *tk, double *rho, int *status, const int *nlive = nullptr)
 {
     const DevParams &P = *Pp;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < npad; c += gridDim.x * blockDim.x) {
+    const int nc = nlive ? *nlive : npad;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
         bool conv;
         const double t = temperature_at(P, tk[c], y + c, npad, enth[c], &conv);
         if (!conv && status) atomicCAS(status, ST_OK, ST_NEWTON_NOCONV);
@@ -315,6 +317,61 @@ __global__ void sort_scatter_kernel(const int *nsub, int n, int npad, int nsub_m
     // positions n..npad-1 keep the padding cells
     if (j == 0)
         for (int c = n + lane; c < npad; c += 32) order[c] = c;
+}
+
+// ---- rounds form: the cells in n_sub order (longest first) advance one sub-step per round; round r
+// (0-based) advances the cells with n_sub > r, a prefix of that order. After the sort's scan, hist[b * nchunk]
+// counts the cells whose key nsub_max - n_sub is below b, so round r has hist[(nsub_max - r) * nchunk] cells.
+__global__ void round_counts_kernel(const int *hist, int nchunk, int nsub_max, int *cells, int *tiles)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nsub_max; r += gridDim.x * blockDim.x) {
+        const int c = hist[(size_t)(nsub_max - r) * nchunk];
+        cells[r] = c;
+        tiles[r] = (c + TILE - 1) / TILE;
+    }
+}
+
+__global__ void iota_kernel(int *v, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
+// The state in n_sub order: dst position pos holds cell order[pos] (pos < n; the padding cells keep their
+// place). Layout of the dense block: y [52][npad], tk, rho, pnd, soot [2][npad]; ints: nsub, passes (zeroed).
+struct RoundState {
+    double *y, *tk, *rho, *pnd, *soot, *enth;
+    int *nsub, *passes;
+};
+__global__ void gather_state_kernel(const int *order, int n, int npad, const double *y, const double *tk,
+                                    const double *rho, const double *pnd, const double *soot, const int *nsub,
+                                    RoundState d)
+{
+    for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < npad; pos += gridDim.x * blockDim.x) {
+        const int c = pos < n ? order[pos] : pos;
+        for (int k = 0; k < LSP; ++k) d.y[(size_t)k * npad + pos] = y[(size_t)k * npad + c];
+        d.tk[pos] = tk[c];
+        d.rho[pos] = rho[c];
+        d.pnd[pos] = pnd[c];
+        d.soot[pos] = soot[c];
+        d.soot[npad + pos] = soot[(size_t)npad + c];
+        d.nsub[pos] = nsub[c];
+        d.passes[pos] = 0;
+    }
+}
+
+// back to cell order (the first n positions)
+__global__ void scatter_state_kernel(const int *order, int n, int npad, RoundState s, double *y, double *tk,
+                                     double *rho, double *soot, int *passes)
+{
+    for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += gridDim.x * blockDim.x) {
+        const int c = order[pos];
+        for (int k = 0; k < LSP; ++k) y[(size_t)k * npad + c] = s.y[(size_t)k * npad + pos];
+        tk[c] = s.tk[pos];
+        rho[c] = s.rho[pos];
+        soot[c] = s.soot[pos];
+        soot[(size_t)npad + c] = s.soot[npad + pos];
+        passes[c] = s.passes[pos];
+    }
 }
 
 // MIXED: the rates of every sub-step in the mixed form (tile_rates_mixed; a tile with a rate beyond the

@@ -104,7 +104,9 @@ struct uc_ctx {
     cudaGraphExec_t int_exec = nullptr;
     uc_integrate_opts int_opts{};
     int int_prec = -1, int_gwarps = 0, int_gsorted = -1;   // what the captured graph was built for
-    int int_warps = 16, int_sorted = 1;                     // kernel shape in use (tuned)
+    int int_warps = 16, int_sorted = 1;                     // kernel shape in use (tuned); 3 warps: rounds form
+    double *rnd_state = nullptr;       // rounds form: y [52], tk, rho, pnd, soot [2], enth rows in n_sub order
+    int *rnd_int = nullptr;            // ... nsub and passes in that order, cells and tiles per round, tiles 0..ntile-1
     double tune_best = 0.0, tune_worst = 0.0;
     // tracing: CUDA event pairs around launches
     bool prof = false;
@@ -385,6 +387,8 @@ static void free_ctx(uc_ctx *c)
             if (*b) { cudaFree(*b); *b = nullptr; }
         if (c->pnd) cudaFree(c->pnd);
         if (c->enth) cudaFree(c->enth);
+        if (c->rnd_state) cudaFree(c->rnd_state);
+        if (c->rnd_int) cudaFree(c->rnd_int);
         void *fb[] = {c->g_xxs, c->g_xxc, c->g_yys, c->g_yyc, c->g_yr, c->f_u, c->f_v, c->f_tmu,
                       c->fe, c->fw, c->fn, c->fs, c->hold, c->skip, c->skip_hold, c->hold_comb, c->fd_x, c->fd_y, c->fd_u, c->fd_v, c->fd_out,
                       c->e_w, c->e_ekt, c->e_rdhsp, c->e_prod, c->e_fpz, c->e_ze, c->e_zw, c->e_zn, c->e_zs,
@@ -608,6 +612,14 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
             else if (!strcmp(k, "inplace")) ctx->upd_kind = 1;
         }
         if (const char *k = getenv("UNICHEM_TR_CHUNK")) ctx->tr_chunk = std::max(1, std::min(TR_CHUNK_MAX, atoi(k)));
+        // shape of the batched integration until uc_integrate_tune picks one: 16 or 8 (persistent kernel), 3 (rounds).
+        // By default the rounds form once every SM has four tiles or more (1M cells: 4.1 s per step against 7.4 s
+        // for the persistent kernel; 333 cells: the persistent kernel is faster)
+        if (ctx->ntile >= 4 * ctx->nsm) ctx->int_warps = 3;
+        if (const char *k = getenv("UNICHEM_INT_WARPS")) {
+            const int v = atoi(k);
+            if (v == 3 || v == 8 || v == 16) ctx->int_warps = v;
+        }
         if (ctx->upd_kind == 0) {
             if (const char *k = getenv("UNICHEM_TR_LOCKSTEP")) ctx->tr_lock = atoi(k) != 0;
             for (int f = 0; f < 2 && e == cudaSuccess; ++f) {
@@ -1782,10 +1794,80 @@ static bool set_integrate_attr()
                                 (int)INT_SMEM) == cudaSuccess;
 }
 
-// Enqueue one integration step on the context's stream (graph capture or not).
+// The rounds form's arrays inside rnd_state / rnd_int
+static RoundState round_state(uc_ctx *ctx)
+{
+    const size_t np = ctx->npad;
+    RoundState r;
+    r.y = ctx->rnd_state;
+    r.tk = r.y + (size_t)LSP * np;
+    r.rho = r.tk + np;
+    r.pnd = r.rho + np;
+    r.soot = r.pnd + np;
+    r.enth = r.soot + 2 * np;
+    r.nsub = ctx->rnd_int;
+    r.passes = r.nsub + np;
+    return r;
+}
+static int *round_cells(uc_ctx *ctx) { return ctx->rnd_int + 2 * (size_t)ctx->npad; }
+static int *round_tiles(uc_ctx *ctx) { return round_cells(ctx) + SORT_MAXBIN; }
+static int *round_tile_list(uc_ctx *ctx) { return round_tiles(ctx) + SORT_MAXBIN; }
+
+// Rounds form of the integration step (FP64; after the sub-step counts and the sort): the state is gathered
+// in n_sub order, then round r advances the cells with n_sub > r by one sub-step with the field kernels --
+// chem_fp64_kernel for RC and SOUR of those tiles, the per-cell tile-resident update (own dt, own stop,
+// closure), T from the held enthalpy and rho -- and the state is scattered back. Every kernel reads its
+// round's cell or tile count from device memory, so the step is one graph whatever the counts are.
+static int enqueue_rounds(uc_ctx *ctx, const uc_integrate_opts &o)
+{
+    const int np = ctx->npad;
+    const int nchunk = (ctx->n + SORT_CHUNK - 1) / SORT_CHUNK;
+    const RoundState rs = round_state(ctx);
+    int *cells = round_cells(ctx), *tiles = round_tiles(ctx);
+    const int eg = std::max(1, std::min((np + 255) / 256, ctx->nsm * 8));
+    round_counts_kernel<<<(o.nsub_max + 255) / 256, 256, 0, ctx->stream>>>(ctx->hist, nchunk, o.nsub_max, cells, tiles);
+    CK(cudaGetLastError());
+    gather_state_kernel<<<eg, 256, 0, ctx->stream>>>(ctx->order, ctx->n, np, ctx->y, ctx->tk, ctx->rho, ctx->pnd,
+                                                     ctx->soot, ctx->nsub, rs);
+    CK(cudaGetLastError());
+    hold_enthalpy_kernel<<<ctx->nsm * 4, 256, 0, ctx->stream>>>(ctx->dP, rs.tk, rs.y, np, rs.enth);
+    CK(cudaGetLastError());
+    ChemArgs c{};
+    c.P = ctx->dP; c.tab = ctx->dTab;
+    c.tk = rs.tk; c.rho = rs.rho; c.y = rs.y; c.stmf = rs.soot; c.stnd = rs.soot + np;
+    c.rc = ctx->rc; c.sour = ctx->sour;
+    c.n = ctx->n; c.npad = np; c.ntile = ctx->ntile; c.status = ctx->status;
+    c.tile_list = round_tile_list(ctx);
+    UpdArgs u{};
+    u.P = ctx->dP; u.rc = ctx->rc; u.sour = ctx->sour; u.rho = rs.rho;
+    u.y0 = rs.y; u.soot0 = rs.soot; u.y = rs.y; u.soot = rs.soot;     // old level = the sub-step's start state
+    u.dt = o.dt; u.sor1 = o.relx; u.tol = o.tol; u.isor = o.isor;
+    u.n = ctx->n; u.npad = np; u.ntile = ctx->ntile;
+    for (int r = 0; r < o.nsub_max; ++r) {
+        c.tile_count = tiles + r;
+        chem_fp64_kernel<<<std::min(ctx->ntile, ctx->nsm), CHEM_THREADS, CHEM_SMEM, ctx->stream>>>(c);
+        CK(cudaGetLastError());
+        update_cells_kernel<<<ctx->nsm, TR_WARPS * 32, TR_SMEM, ctx->stream>>>(u, cells + r, rs.nsub, rs.passes,
+                                                                               ctx->status, ctx->tr_map[0],
+                                                                               ctx->tr_map[1]);
+        CK(cudaGetLastError());
+        temperature_held_kernel<<<ctx->nsm * 4, 128, 0, ctx->stream>>>(ctx->dP, rs.enth, rs.y, rs.pnd, np, rs.tk,
+                                                                        rs.rho, ctx->status, cells + r);
+        CK(cudaGetLastError());
+    }
+    scatter_state_kernel<<<eg, 256, 0, ctx->stream>>>(ctx->order, ctx->n, np, rs, ctx->y, ctx->tk, ctx->rho,
+                                                      ctx->soot, ctx->cpasses);
+    CK(cudaGetLastError());
+    return UC_OK;
+}
+
+// Enqueue one integration step on the context's stream (graph capture or not). warps 16 or 8: the
+// persistent kernel with that many warps; 3: the rounds form (FP64; the mixed form takes 16 warps).
 static int enqueue_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts &o, int warps, int sorted)
 {
     const int np = ctx->npad;
+    if (warps == 3 && precision != UC_FP64) warps = 16;
+    if (warps == 3) sorted = 1;
     // omega of the start state (QDSP rows) for the sub-step counts
     if (precision == UC_MIXED) {
         ChemMArgs m{};
@@ -1819,6 +1901,7 @@ static int enqueue_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts
                                                            ctx->order);
         CK(cudaGetLastError());
     }
+    if (warps == 3) return enqueue_rounds(ctx, o);
     CK(cudaMemsetAsync(ctx->next_tile, 0, sizeof(int), ctx->stream));
     IntArgs a{};
     a.P = ctx->dP; a.tab = ctx->dTab; a.tabm = ctx->dTabM;
@@ -1860,6 +1943,29 @@ static int integrate_prepare(uc_ctx *ctx, int precision, const uc_integrate_opts
     }
     if (!set_integrate_attr<16>() || !set_integrate_attr<8>())
         return set_err(ctx, UC_E_CUDA, "integration kernel shared-memory attribute");
+    if (precision == UC_FP64) {
+        // the rounds form: its state copy in n_sub order, the RC plane and its tensor maps
+        const size_t np = ctx->npad;
+        if (!ctx->rnd_state) RET_IF(dalloc(ctx, &ctx->rnd_state, (size_t)(LSP + 6) * np));
+        if (!ctx->rnd_int) {
+            cudaError_t e = cudaMalloc((void **)&ctx->rnd_int, (2 * np + 2 * SORT_MAXBIN + ctx->ntile) * sizeof(int));
+            if (e != cudaSuccess) {
+                ctx->rnd_int = nullptr;
+                return set_err(ctx, UC_E_NOMEM, "integration rounds buffers: %s", cudaGetErrorString(e));
+            }
+            iota_kernel<<<std::max(1, std::min((ctx->ntile + 255) / 256, ctx->nsm * 4)), 256, 0, ctx->stream>>>(
+                round_tile_list(ctx), ctx->ntile);
+            CK(cudaGetLastError());
+        }
+        if (!ctx->rc) RET_IF(dalloc(ctx, &ctx->rc, (size_t)LRX * np));
+        RET_IF(encode_rc_map(ctx));
+        if (cudaFuncSetAttribute(update_cells_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TR_SMEM) !=
+            cudaSuccess)
+            return set_err(ctx, UC_E_CUDA, "integration rounds: update kernel shared-memory attribute");
+        if (cudaFuncSetAttribute(chem_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CHEM_SMEM) !=
+            cudaSuccess)
+            return set_err(ctx, UC_E_CUDA, "integration rounds: rate kernel shared-memory attribute");
+    }
     return UC_OK;
 }
 
@@ -1867,6 +1973,7 @@ extern "C" int uc_integrate(uc_ctx *ctx, int precision, const uc_integrate_opts 
 {
     RET_IF(integrate_prepare(ctx, precision, o));
     ctx->rc_start = false;
+    ctx->have_rc = false;          // the state moves on (and the rounds form uses the RC plane)
     const bool fresh = ctx->int_exec && ctx->int_prec == precision && ctx->int_gwarps == ctx->int_warps &&
                        ctx->int_gsorted == ctx->int_sorted && same_opts(ctx->int_opts, *o);
     if (!fresh) {
@@ -1919,14 +2026,16 @@ extern "C" int uc_integrate_tune(uc_ctx *ctx, int precision, const uc_integrate_
         }
         return cudaSuccess;
     };
-    const int shapes[4][2] = {{16, 1}, {8, 1}, {16, 0}, {8, 0}};
+    // persistent kernel (16 or 8 warps, sorted or natural queue order); the rounds form (FP64)
+    const int shapes[5][2] = {{16, 1}, {8, 1}, {16, 0}, {8, 0}, {3, 1}};
+    const int nshape = precision == UC_FP64 ? 5 : 4;
     double best = 1e300, worst = 0.0;
     int bw = 16, bs = 1, rc = UC_OK;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     if (copy_state(true) != cudaSuccess) rc = set_err(ctx, UC_E_CUDA, "tuning: state copy failed");
-    for (int i = 0; i < 4 && rc == UC_OK; ++i) {
+    for (int i = 0; i < nshape && rc == UC_OK; ++i) {
         cudaEventRecord(e0, ctx->stream);
         rc = enqueue_integrate(ctx, precision, *o, shapes[i][0], shapes[i][1]);
         cudaEventRecord(e1, ctx->stream);

@@ -103,6 +103,59 @@ __device__ __forceinline__ void tr_box_load(double *dst, const CUtensorMap *map,
         : "memory");
 }
 
+// Stage one 32-cell tile's RC block on chip, all rows by bulk copies (bandwidth-bound, not latency-bound):
+// first the tensor-memory rows (slots 0..NT-1) into the warp's shared-memory slot, moved on into the warp's
+// lane quarter of tensor memory by tcgen05.st, then the shared-memory rows (slots NT..543) into the slot.
+// The second copy is still in flight on return: tr_stage_wait completes it (the caller loads the cells'
+// state meanwhile). Bounded waits: on a timeout the status is set and the copies in flight are waited for.
+__device__ __forceinline__ void tr_stage_begin(double *slot, uint32_t tbase, const CUtensorMap *map_t,
+                                               const CUtensorMap *map_s, int tile, uint64_t *bar, uint32_t &phase,
+                                               int lane, int *status)
+{
+    __syncwarp();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) {
+        mbar_expect_tx(bar, (uint32_t)(UC_TR_NT * TILE * sizeof(double)));
+        tr_box_load(slot, map_t, tile * TILE, 0, bar);            // slots 0 .. NT-1
+    }
+    __syncwarp();
+    if (!mbar_wait_bounded(bar, phase, UC_TR_WAIT_TRIES)) {
+        if (lane == 0) atomicExch(status, ST_TMA_TIMEOUT);
+        mbar_wait_bounded(bar, phase, UC_TR_WAIT_TRIES);   // let copies in flight land
+    }
+    phase ^= 1u;
+    for (int i0 = 0; i0 < UC_TR_NT; i0 += 16) {
+        uint32_t v[32];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const double d = slot[(size_t)(i0 + q) * TILE + lane];
+            v[2 * q] = (uint32_t)__double2loint(d);
+            v[2 * q + 1] = (uint32_t)__double2hiint(d);
+        }
+        tr_tmem_st16(tbase + (uint32_t)(2 * i0), v);
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    __syncwarp();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) {
+        mbar_expect_tx(bar, (uint32_t)(UC_TR_NS * TILE * sizeof(double)));
+        tr_box_load(slot, map_s, tile * TILE, UC_TR_NT, bar);     // slots NT .. NT+NS/2-1
+        tr_box_load(slot + (size_t)TR_BOX_S * TILE, map_s, tile * TILE, UC_TR_NT + TR_BOX_S, bar);
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void tr_stage_wait(uint64_t *bar, uint32_t &phase, int lane, int *status)
+{
+    if (!mbar_wait_bounded(bar, phase, UC_TR_WAIT_TRIES)) {
+        if (lane == 0) atomicExch(status, ST_TMA_TIMEOUT);
+        mbar_wait_bounded(bar, phase, UC_TR_WAIT_TRIES);   // let copies in flight land
+    }
+    phase ^= 1u;
+}
+
 template <bool FACES, bool LOCK>
 __global__ void __launch_bounds__(TR_WARPS * 32, 1)
 update_tr_kernel(const UpdArgs a, const TrArgs t, const __grid_constant__ CUtensorMap map_t,
@@ -152,42 +205,7 @@ update_tr_kernel(const UpdArgs a, const TrArgs t, const __grid_constant__ CUtens
             if (!own) tile = a.ntile - 1;             // one (nothing stored) to keep the barriers matched
             const size_t cell = (size_t)tile * TILE + lane;
             const bool live = own && cell < (size_t)a.n && !(a.hold && a.hold[cell]);
-            // ---- stage the tile's RC block, all rows by bulk copies (bandwidth-bound, not latency-bound):
-            // first the tensor-memory rows into the shared-memory slot, moved on by tcgen05.st, then
-            // the shared-memory rows into the slot
-            __syncwarp();
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) {
-                mbar_expect_tx(&s_bar[w], (uint32_t)(UC_TR_NT * TILE * sizeof(double)));
-                tr_box_load(slot, &map_t, tile * TILE, 0, &s_bar[w]);            // slots 0 .. NT-1
-            }
-            __syncwarp();
-            if (!mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES)) {
-                if (lane == 0) atomicExch(t.status, ST_TMA_TIMEOUT);
-                mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES);   // let copies in flight land
-            }
-            phase ^= 1u;
-            for (int i0 = 0; i0 < UC_TR_NT; i0 += 16) {
-                uint32_t v[32];
-#pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const double d = slot[(size_t)(i0 + q) * TILE + lane];
-                    v[2 * q] = (uint32_t)__double2loint(d);
-                    v[2 * q + 1] = (uint32_t)__double2hiint(d);
-                }
-                tr_tmem_st16(tbase + (uint32_t)(2 * i0), v);
-            }
-            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-            __syncwarp();
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) {
-                mbar_expect_tx(&s_bar[w], (uint32_t)(UC_TR_NS * TILE * sizeof(double)));
-                tr_box_load(slot, &map_s, tile * TILE, UC_TR_NT, &s_bar[w]);     // slots NT .. NT+NS/2-1
-                tr_box_load(slot + (size_t)TR_BOX_S * TILE, &map_s, tile * TILE, UC_TR_NT + TR_BOX_S, &s_bar[w]);
-            }
-            __syncwarp();
+            tr_stage_begin(slot, tbase, &map_t, &map_s, tile, &s_bar[w], phase, lane, t.status);
             // ---- the cell's state (Y in registers)
             double yv[LSP], ysh[UC_IP_NSHADOW];
 #pragma unroll
@@ -200,11 +218,7 @@ update_tr_kernel(const UpdArgs a, const TrArgs t, const __grid_constant__ CUtens
             sc[7 * TILE] = a.soot0[np + cell];
             double st1 = a.soot[cell], st2 = a.soot[np + cell];
             double y0s0, y0s1, fss0 = 0.0, fss1 = 0.0, fns0 = 0.0, fns1 = 0.0;
-            if (!mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES)) {
-                if (lane == 0) atomicExch(t.status, ST_TMA_TIMEOUT);
-                mbar_wait_bounded(&s_bar[w], phase, UC_TR_WAIT_TRIES);   // let copies in flight land
-            }
-            phase ^= 1u;
+            tr_stage_wait(&s_bar[w], phase, lane, t.status);
             for (int j = 0; j < C; ++j) {
                 double crsd = 0.0;
                 {
@@ -346,6 +360,158 @@ update_tr_kernel(const UpdArgs a, const TrArgs t, const __grid_constant__ CUtens
             n2 = 0.0;
         }
         a.y[(LSP - 1) * np + cell] = n2;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (w == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(512));
+}
+
+// Per-cell form of the tile-resident update, for the batched integration (uc_integrate, rounds form):
+// every cell runs its own pass loop with its own step a.dt / nsub[cell] and stops on its own residual
+// (SPNORM = LSP - 1: solvesp.f:2833-2838 for a one-cell field), then the N2 closure and renormalisation
+// (solvesp.f:2839-2915), all in registers. Only the first *nlive cells of the arrays are live (the caller
+// orders the cells so that the ones still integrating come first); tiles beyond them are not touched.
+// The old time level (a.y0, a.soot0) is the state at the sub-step start, and the caller may pass the
+// state arrays themselves: each warp reads its tile's rows before it writes them. passes[cell] is
+// incremented by the passes the cell ran. No grid barrier: warps take tiles gwarp, gwarp + nwarp, ...
+// The arithmetic of a pass is that of update_tr_kernel; a lane that has converged keeps its Y while the
+// others of its warp run on (its values are computed and dropped).
+__global__ void __launch_bounds__(TR_WARPS * 32, 1)
+update_cells_kernel(const UpdArgs a, const int *nlive, const int *nsub, int *passes, int *status,
+                    const __grid_constant__ CUtensorMap map_t, const __grid_constant__ CUtensorMap map_s)
+{
+    extern __shared__ __align__(128) double s_rc[];          // [TR_WARPS][UC_TR_NS][32]
+    __shared__ double s_wm[LSP];
+    __shared__ double s_cell[TR_WARPS][8][TILE];            // SOUR 1..6 and the two soot values of the old level
+    __shared__ __align__(8) uint64_t s_bar[TR_WARPS];
+    __shared__ uint32_t s_tmem;
+    const int n = *nlive;
+    if (n <= 0) return;                                     // uniform over the grid
+    const DevParams &P = *a.P;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const size_t np = a.npad;
+    const double sor1 = a.sor1, sor2 = 1.0 - a.sor1;
+    const int ntile = (n + TILE - 1) / TILE;
+
+    if (w == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x < TR_WARPS) mbar_init(&s_bar[threadIdx.x], 1);
+    for (int k = threadIdx.x; k < LSP; k += blockDim.x) s_wm[k] = P.WM[k];
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tbase = s_tmem + ((uint32_t)(32 * w) << 16);   // this warp's lane quarter
+    double *slot = s_rc + (size_t)w * TR_SLOT_DOUBLES;
+    uint32_t phase = 0;
+    const int nwarp = gridDim.x * TR_WARPS;
+    uint32_t bank0[2 * UC_TR_SEG], bank1[2 * UC_TR_SEG];
+#pragma unroll
+    for (int i = 0; i < 2 * UC_TR_SEG; ++i) bank0[i] = bank1[i] = 0u;
+
+    for (int tile = blockIdx.x * TR_WARPS + w; tile < ntile; tile += nwarp) {
+        const size_t cell = (size_t)tile * TILE + lane;
+        const bool live = cell < (size_t)n;
+        tr_stage_begin(slot, tbase, &map_t, &map_s, tile, &s_bar[w], phase, lane, status);
+        double yv[LSP], ysh[UC_IP_NSHADOW];
+#pragma unroll
+        for (int k = 0; k < LSP; ++k) yv[k] = a.y[k * np + cell];
+        const double rho = a.rho[cell];
+        const double dt = a.dt / (double)max(1, nsub[cell]);
+        double *sc = &s_cell[w][0][lane];        // sc[m * TILE]: SOUR(m), m < 6; old soot at 6, 7
+#pragma unroll
+        for (int m = 0; m < 6; ++m) sc[m * TILE] = a.sour[m * np + cell];
+        sc[6 * TILE] = a.soot0[cell];
+        sc[7 * TILE] = a.soot0[np + cell];
+        double st1 = a.soot[cell], st2 = a.soot[np + cell];
+        double y0s0, y0s1;
+        tr_stage_wait(&s_bar[w], phase, lane, status);
+        bool done = !live;
+        int npass = 0;
+        for (int pass = 1; pass <= a.isor; ++pass) {
+            if (__all_sync(0xffffffffu, done)) break;
+            double crsd = 0.0;
+            {
+                double &rsd = crsd;
+#define YO(k) yv[k]
+#define YN(k) yv[k]
+#define YOS(m) ysh[m]
+#define SOUR(m) sc[(m) * TILE]
+#define WM(k) s_wm[k]
+#define UC_TR_PF(s, k) do { y0s##s = __ldg(a.y0 + (size_t)(k) * np + cell); } while (0)
+#define Y0S(s) y0s##s
+#define FSS(s) 0.0
+#define FNS(s) 0.0
+#define UC_TR_SYNC() do { } while (0)
+#define UC_UPDATE_TAIL(k) do { if (fnew < 0.0) fnew = 0.0; if (!done) yv[k] = fnew; } while (0)
+#define RCS(i) slot[(i) * TILE + lane]
+#define TM_LD(b, q, col)                                                                              \
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];"                             \
+                 : "=r"(bank##b[2 * (q)]), "=r"(bank##b[2 * (q) + 1])                                \
+                 : "r"(tbase + (uint32_t)(col)))
+#define TM_WAIT(b) UC_TR_WAIT_BANK(bank##b)
+#define RCT(b, q) __hiloint2double((int)bank##b[2 * (q) + 1], (int)bank##b[2 * (q)])
+                UC_TR_SHADOW_SAVE();
+                UC_UPDATE_PROGRAM_TR();
+#undef YO
+#undef YN
+#undef YOS
+#undef SOUR
+#undef WM
+#undef UC_TR_PF
+#undef Y0S
+#undef FSS
+#undef FNS
+#undef UC_TR_SYNC
+#undef UC_UPDATE_TAIL
+#undef RCS
+#undef TM_LD
+#undef TM_WAIT
+#undef RCT
+            }
+            // soot mass fraction and number density (solvesp.f:2807-2832)
+            const double y2 = yv[1], y4 = yv[3], y5 = yv[4], y22 = yv[21];
+            const double so0 = sc[0], so1 = sc[TILE], so2 = sc[2 * TILE], so3 = sc[3 * TILE], so4 = sc[4 * TILE],
+                         so5 = sc[5 * TILE];
+            double rhs1 = rho * sc[6 * TILE] + dt * ((double)0.012011f / P.WMSTR) *
+                                               (2.0 * so0 * y22 - so2 * y2 - so3 * y5 - so4 * y4);
+            double fnew = sor2 * st1 + rhs1 * sor1 / ((rho - 0.0) - 0.0);
+            crsd += fabs(st1 - fnew);
+            if (fnew < 0.0) fnew = 0.0;
+            const double n1 = fnew;
+            rhs1 = rho * sc[7 * TILE] + dt * so1 * y22;
+            const double rhs2 = -(dt * so5);
+            fnew = sor2 * st2 + rhs1 * sor1 / ((rho - 0.0) - rhs2);
+            if (fnew < 0.0) fnew = 0.0;
+            if (!done) {
+                st1 = n1;
+                st2 = fnew;
+                ++npass;
+                if (crsd / (double)(LSP - 1) <= a.tol) done = true;
+            }
+        }
+        if (live) {
+            // N2 closure and renormalisation (solvesp.f:2839-2915)
+            double ft = yv[0];
+#pragma unroll
+            for (int k = 1; k < LSP - 1; ++k) ft = ft + yv[k];
+            ft = ft + st1;
+            double n2 = 1.0 - ft;
+            if (ft > 1.0) {
+#pragma unroll
+                for (int k = 0; k < LSP - 1; ++k) yv[k] = yv[k] / ft;
+                st1 = st1 / ft;
+                n2 = 0.0;
+            }
+            yv[LSP - 1] = n2;
+#pragma unroll
+            for (int k = 0; k < LSP; ++k) a.y[k * np + cell] = yv[k];
+            a.soot[cell] = st1;
+            a.soot[np + cell] = st2;
+            passes[cell] += npass;
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
