@@ -679,7 +679,8 @@ def main_c3(args):
                                 "frac_1": round(float((ns == 1).mean()), 4),
                                 "frac_max": round(float((ns == ns.max()).mean()), 4)},
                        "passes_per_substep": round(float(pa.sum()) / substeps, 2),
-                       "shape": ("rounds form (field kernels per sub-step round, cells in n_sub order)"
+                       "shape": ("rounds form (field kernels per sub-step round; cells in n_sub order, "
+                                 "re-sorted by the passes of their last sub-step between rounds)"
                                  if tune["int_warps"] == 3 else
                                  f"persistent work-queue kernel, {int(tune['int_warps'])} warps"),
                        "l2": ("state 470 MB > L2; RC plane 4.6 GB written and read back per round"
@@ -687,8 +688,9 @@ def main_c3(args):
             "e2e": {"value": round(n * args.steps / e2e, 1), "unit": UNIT, "h2d_bytes_per_step": (2 + 52) * 8 * n,
                     "d2h_bytes_per_step": (2 + 52) * 8 * n},
             # per step: rates of the start state, n_sub, the sort (3), then the persistent kernel, or the round
-            # counts, gather, held enthalpy, 3 kernels per round (one round per possible sub-step) and scatter
-            "gpu_launches": kt["integrate"][1] * ((9 + 3 * NSUB_MAX) if tune["int_warps"] == 3 else
+            # counts, gather, held enthalpy, 3 kernels per round (one round per possible sub-step), 5 for the
+            # re-sort between rounds, and the scatter
+            "gpu_launches": kt["integrate"][1] * ((4 + 8 * NSUB_MAX) if tune["int_warps"] == 3 else
                                                   (6 if tune["int_sorted"] else 3)),
             "clocks": clk.summary(),
             "roofline": {"kernel": "integrate", "bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64, 2),

@@ -360,9 +360,11 @@ int uc_device_view_get(uc_ctx *ctx, uc_device_view *v);
  * kernel (each CTA advances one 32-cell tile through all its sub-steps) and,
  * for UC_FP64, the rounds form (the cells gathered in n_sub order; round r
  * advances the cells with n_sub > r by one sub-step with the field kernels:
- * rates, a per-cell form of the tile-resident species update, T and rho).
- * The rounds form holds a copy of the state in n_sub order on the device
- * (58 doubles and 2 ints per cell) and uses the context's RC plane.
+ * rates, a per-cell form of the tile-resident species update, T and rho;
+ * between rounds the cells that go on are re-ordered by the passes of their
+ * last sub-step). The rounds form holds two copies of the state in its own
+ * order on the device (116 doubles and 10 ints per cell) and uses the
+ * context's RC plane.
  *
  * precision: UC_FP64 (everything FP64) or UC_MIXED (the rates of every
  * sub-step and of the start state in the mixed form of uc_rates, stored as

@@ -336,12 +336,15 @@ __global__ void iota_kernel(int *v, int n)
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
 }
 
-// The state in n_sub order: dst position pos holds cell order[pos] (pos < n; the padding cells keep their
-// place). Layout of the dense block: y [52][npad], tk, rho, pnd, soot [2][npad]; ints: nsub, passes (zeroed).
+// The state of the rounds form, position by position: y [52][npad], tk, rho, pnd, soot [2][npad], enth in
+// doubles; nsub, passes (summed over the sub-steps), last (passes of the last sub-step) and ord (the cell at
+// the position) in ints. Two such buffers alternate: between rounds the live cells are re-ordered.
 struct RoundState {
     double *y, *tk, *rho, *pnd, *soot, *enth;
-    int *nsub, *passes;
+    int *nsub, *passes, *last, *ord;
 };
+
+// The state in n_sub order: position pos holds cell order[pos] (pos < n; the padding cells keep their place)
 __global__ void gather_state_kernel(const int *order, int n, int npad, const double *y, const double *tk,
                                     const double *rho, const double *pnd, const double *soot, const int *nsub,
                                     RoundState d)
@@ -356,15 +359,86 @@ __global__ void gather_state_kernel(const int *order, int n, int npad, const dou
         d.soot[npad + pos] = soot[(size_t)npad + c];
         d.nsub[pos] = nsub[c];
         d.passes[pos] = 0;
+        d.last[pos] = 0;
+        d.ord[pos] = c;
+    }
+}
+
+// Sort key of the positions of round r for round r + 1: the cells that go on (n_sub > r + 1) by the passes
+// their last sub-step took, most first (a cell's pass count changes little from one sub-step to the next,
+// so warps then hold cells that stop together), the others after them.
+constexpr int ROUND_KEYS = 102;            // 0..99: 100 - min(passes, 100) of a live cell; 101: done
+__global__ void round_key_kernel(const int *nsub, const int *last, const int *nlive, int r, int *key)
+{
+    const int n = *nlive;
+    for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += gridDim.x * blockDim.x)
+        key[pos] = nsub[pos] > r + 1 ? 100 - min(max(last[pos], 1), 100) : ROUND_KEYS - 1;
+}
+
+// Stable counting sort of the first *nlive keys (chunks of SORT_CHUNK; hist [nbins][nchunk], scanned by
+// sort_scan_kernel in between): perm[new position] = old position.
+__global__ void key_count_kernel(const int *key, const int *nlive, int nbins, int nchunk, int *hist)
+{
+    __shared__ int h[SORT_MAXBIN];
+    const int j = blockIdx.x, n = *nlive;
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    const int c0 = j * SORT_CHUNK, c1 = min(n, c0 + SORT_CHUNK);
+    for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) atomicAdd(&h[key[c]], 1);
+    __syncthreads();
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x) hist[(size_t)b * nchunk + j] = h[b];
+}
+
+__global__ void key_scatter_kernel(const int *key, const int *nlive, int nbins, int nchunk, const int *offs,
+                                   int *perm)
+{
+    __shared__ int off[SORT_MAXBIN];
+    const int j = blockIdx.x, lane = threadIdx.x, n = *nlive;
+    for (int b = lane; b < nbins; b += 32) off[b] = offs[(size_t)b * nchunk + j];
+    __syncwarp();
+    const int c0 = j * SORT_CHUNK, c1 = min(n, c0 + SORT_CHUNK);
+    for (int base = c0; base < c1; base += 32) {
+        const int c = base + lane;
+        const bool v = c < c1;
+        const int k = v ? key[c] : -1;
+        const unsigned act = __ballot_sync(0xffffffffu, v);
+        const unsigned peers = __match_any_sync(0xffffffffu, k) & act;
+        const int rank = __popc(peers & ((1u << lane) - 1));
+        int pos = 0;
+        if (v) pos = off[k] + rank;
+        __syncwarp();
+        if (v && rank == 0) off[k] += __popc(peers);
+        __syncwarp();
+        if (v) perm[pos] = c;
+    }
+}
+
+// d[pos] = s[perm[pos]] for the first *nlive positions, d[pos] = s[pos] beyond
+__global__ void permute_state_kernel(const int *perm, const int *nlive, int npad, RoundState s, RoundState d)
+{
+    const int n = *nlive;
+    for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < npad; pos += gridDim.x * blockDim.x) {
+        const int q = pos < n ? perm[pos] : pos;
+        for (int k = 0; k < LSP; ++k) d.y[(size_t)k * npad + pos] = s.y[(size_t)k * npad + q];
+        d.tk[pos] = s.tk[q];
+        d.rho[pos] = s.rho[q];
+        d.pnd[pos] = s.pnd[q];
+        d.soot[pos] = s.soot[q];
+        d.soot[npad + pos] = s.soot[npad + q];
+        d.enth[pos] = s.enth[q];
+        d.nsub[pos] = s.nsub[q];
+        d.passes[pos] = s.passes[q];
+        d.last[pos] = s.last[q];
+        d.ord[pos] = s.ord[q];
     }
 }
 
 // back to cell order (the first n positions)
-__global__ void scatter_state_kernel(const int *order, int n, int npad, RoundState s, double *y, double *tk,
-                                     double *rho, double *soot, int *passes)
+__global__ void scatter_state_kernel(int n, int npad, RoundState s, double *y, double *tk, double *rho,
+                                     double *soot, int *passes)
 {
     for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += gridDim.x * blockDim.x) {
-        const int c = order[pos];
+        const int c = s.ord[pos];
         for (int k = 0; k < LSP; ++k) y[(size_t)k * npad + c] = s.y[(size_t)k * npad + pos];
         tk[c] = s.tk[pos];
         rho[c] = s.rho[pos];

@@ -1794,39 +1794,49 @@ static bool set_integrate_attr()
                                 (int)INT_SMEM) == cudaSuccess;
 }
 
-// The rounds form's arrays inside rnd_state / rnd_int
-static RoundState round_state(uc_ctx *ctx)
+// The rounds form's arrays inside rnd_state / rnd_int: two state buffers b = 0, 1, then (ints) the sort
+// keys and permutation of a round, the cells and tiles of each round and the tile list 0..ntile-1
+static RoundState round_state(uc_ctx *ctx, int b)
 {
     const size_t np = ctx->npad;
     RoundState r;
-    r.y = ctx->rnd_state;
+    r.y = ctx->rnd_state + (size_t)b * (LSP + 6) * np;
     r.tk = r.y + (size_t)LSP * np;
     r.rho = r.tk + np;
     r.pnd = r.rho + np;
     r.soot = r.pnd + np;
     r.enth = r.soot + 2 * np;
-    r.nsub = ctx->rnd_int;
+    r.nsub = ctx->rnd_int + (size_t)b * 4 * np;
     r.passes = r.nsub + np;
+    r.last = r.passes + np;
+    r.ord = r.last + np;
     return r;
 }
-static int *round_cells(uc_ctx *ctx) { return ctx->rnd_int + 2 * (size_t)ctx->npad; }
+static size_t round_state_doubles(uc_ctx *ctx) { return 2 * (size_t)(LSP + 6) * ctx->npad; }
+static size_t round_ints(uc_ctx *ctx) { return 10 * (size_t)ctx->npad + 2 * SORT_MAXBIN + ctx->ntile; }
+static int *round_key(uc_ctx *ctx) { return ctx->rnd_int + 8 * (size_t)ctx->npad; }
+static int *round_perm(uc_ctx *ctx) { return round_key(ctx) + ctx->npad; }
+static int *round_cells(uc_ctx *ctx) { return round_perm(ctx) + ctx->npad; }
 static int *round_tiles(uc_ctx *ctx) { return round_cells(ctx) + SORT_MAXBIN; }
 static int *round_tile_list(uc_ctx *ctx) { return round_tiles(ctx) + SORT_MAXBIN; }
 
 // Rounds form of the integration step (FP64; after the sub-step counts and the sort): the state is gathered
-// in n_sub order, then round r advances the cells with n_sub > r by one sub-step with the field kernels --
-// chem_fp64_kernel for RC and SOUR of those tiles, the per-cell tile-resident update (own dt, own stop,
-// closure), T from the held enthalpy and rho -- and the state is scattered back. Every kernel reads its
-// round's cell or tile count from device memory, so the step is one graph whatever the counts are.
+// in n_sub order, then round r advances the cells with n_sub > r (a prefix of the positions) by one sub-step
+// with the field kernels -- chem_fp64_kernel for RC and SOUR of those tiles, the per-cell tile-resident
+// update (own dt, own stop, closure), T from the held enthalpy and rho -- and re-orders the prefix for the
+// next round (the cells that go on first, by the passes of their last sub-step; a stable counting sort and
+// a permutation into the other state buffer); at the end the state is scattered back to cell order. Every
+// kernel reads its round's cell or tile count from device memory, so the step is one graph whatever the
+// counts are.
 static int enqueue_rounds(uc_ctx *ctx, const uc_integrate_opts &o)
 {
     const int np = ctx->npad;
     const int nchunk = (ctx->n + SORT_CHUNK - 1) / SORT_CHUNK;
-    const RoundState rs = round_state(ctx);
-    int *cells = round_cells(ctx), *tiles = round_tiles(ctx);
+    int *cells = round_cells(ctx), *tiles = round_tiles(ctx), *key = round_key(ctx), *perm = round_perm(ctx);
     const int eg = std::max(1, std::min((np + 255) / 256, ctx->nsm * 8));
     round_counts_kernel<<<(o.nsub_max + 255) / 256, 256, 0, ctx->stream>>>(ctx->hist, nchunk, o.nsub_max, cells, tiles);
     CK(cudaGetLastError());
+    RoundState rs = round_state(ctx, 0), other = round_state(ctx, 1);
     gather_state_kernel<<<eg, 256, 0, ctx->stream>>>(ctx->order, ctx->n, np, ctx->y, ctx->tk, ctx->rho, ctx->pnd,
                                                      ctx->soot, ctx->nsub, rs);
     CK(cudaGetLastError());
@@ -1834,29 +1844,42 @@ static int enqueue_rounds(uc_ctx *ctx, const uc_integrate_opts &o)
     CK(cudaGetLastError());
     ChemArgs c{};
     c.P = ctx->dP; c.tab = ctx->dTab;
-    c.tk = rs.tk; c.rho = rs.rho; c.y = rs.y; c.stmf = rs.soot; c.stnd = rs.soot + np;
     c.rc = ctx->rc; c.sour = ctx->sour;
     c.n = ctx->n; c.npad = np; c.ntile = ctx->ntile; c.status = ctx->status;
     c.tile_list = round_tile_list(ctx);
     UpdArgs u{};
-    u.P = ctx->dP; u.rc = ctx->rc; u.sour = ctx->sour; u.rho = rs.rho;
-    u.y0 = rs.y; u.soot0 = rs.soot; u.y = rs.y; u.soot = rs.soot;     // old level = the sub-step's start state
+    u.P = ctx->dP; u.rc = ctx->rc; u.sour = ctx->sour;
     u.dt = o.dt; u.sor1 = o.relx; u.tol = o.tol; u.isor = o.isor;
     u.n = ctx->n; u.npad = np; u.ntile = ctx->ntile;
     for (int r = 0; r < o.nsub_max; ++r) {
+        c.tk = rs.tk; c.rho = rs.rho; c.y = rs.y; c.stmf = rs.soot; c.stnd = rs.soot + np;
         c.tile_count = tiles + r;
         chem_fp64_kernel<<<std::min(ctx->ntile, ctx->nsm), CHEM_THREADS, CHEM_SMEM, ctx->stream>>>(c);
         CK(cudaGetLastError());
+        u.rho = rs.rho;
+        u.y0 = rs.y; u.soot0 = rs.soot; u.y = rs.y; u.soot = rs.soot;     // old level = the sub-step's start state
         update_cells_kernel<<<ctx->nsm, TR_WARPS * 32, TR_SMEM, ctx->stream>>>(u, cells + r, rs.nsub, rs.passes,
-                                                                               ctx->status, ctx->tr_map[0],
+                                                                               rs.last, ctx->status, ctx->tr_map[0],
                                                                                ctx->tr_map[1]);
         CK(cudaGetLastError());
         temperature_held_kernel<<<ctx->nsm * 4, 128, 0, ctx->stream>>>(ctx->dP, rs.enth, rs.y, rs.pnd, np, rs.tk,
                                                                         rs.rho, ctx->status, cells + r);
         CK(cudaGetLastError());
+        if (r + 1 == o.nsub_max) break;
+        round_key_kernel<<<eg, 256, 0, ctx->stream>>>(rs.nsub, rs.last, cells + r, r, key);
+        CK(cudaGetLastError());
+        key_count_kernel<<<nchunk, 256, 0, ctx->stream>>>(key, cells + r, ROUND_KEYS, nchunk, ctx->hist);
+        CK(cudaGetLastError());
+        sort_scan_kernel<<<1, 1024, 0, ctx->stream>>>(ctx->hist, ROUND_KEYS * nchunk);
+        CK(cudaGetLastError());
+        key_scatter_kernel<<<nchunk, 32, 0, ctx->stream>>>(key, cells + r, ROUND_KEYS, nchunk, ctx->hist, perm);
+        CK(cudaGetLastError());
+        permute_state_kernel<<<eg, 256, 0, ctx->stream>>>(perm, cells + r, np, rs, other);
+        CK(cudaGetLastError());
+        std::swap(rs, other);
     }
-    scatter_state_kernel<<<eg, 256, 0, ctx->stream>>>(ctx->order, ctx->n, np, rs, ctx->y, ctx->tk, ctx->rho,
-                                                      ctx->soot, ctx->cpasses);
+    scatter_state_kernel<<<eg, 256, 0, ctx->stream>>>(ctx->n, np, rs, ctx->y, ctx->tk, ctx->rho, ctx->soot,
+                                                      ctx->cpasses);
     CK(cudaGetLastError());
     return UC_OK;
 }
@@ -1946,9 +1969,9 @@ static int integrate_prepare(uc_ctx *ctx, int precision, const uc_integrate_opts
     if (precision == UC_FP64) {
         // the rounds form: its state copy in n_sub order, the RC plane and its tensor maps
         const size_t np = ctx->npad;
-        if (!ctx->rnd_state) RET_IF(dalloc(ctx, &ctx->rnd_state, (size_t)(LSP + 6) * np));
+        if (!ctx->rnd_state) RET_IF(dalloc(ctx, &ctx->rnd_state, round_state_doubles(ctx)));
         if (!ctx->rnd_int) {
-            cudaError_t e = cudaMalloc((void **)&ctx->rnd_int, (2 * np + 2 * SORT_MAXBIN + ctx->ntile) * sizeof(int));
+            cudaError_t e = cudaMalloc((void **)&ctx->rnd_int, round_ints(ctx) * sizeof(int));
             if (e != cudaSuccess) {
                 ctx->rnd_int = nullptr;
                 return set_err(ctx, UC_E_NOMEM, "integration rounds buffers: %s", cudaGetErrorString(e));

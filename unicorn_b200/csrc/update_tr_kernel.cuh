@@ -373,11 +373,12 @@ update_tr_kernel(const UpdArgs a, const TrArgs t, const __grid_constant__ CUtens
 // orders the cells so that the ones still integrating come first); tiles beyond them are not touched.
 // The old time level (a.y0, a.soot0) is the state at the sub-step start, and the caller may pass the
 // state arrays themselves: each warp reads its tile's rows before it writes them. passes[cell] is
-// incremented by the passes the cell ran. No grid barrier: warps take tiles gwarp, gwarp + nwarp, ...
+// incremented by the passes the cell ran, last[cell] set to them. No grid barrier: warps take tiles gwarp,
+// gwarp + nwarp, ...
 // The arithmetic of a pass is that of update_tr_kernel; a lane that has converged keeps its Y while the
 // others of its warp run on (its values are computed and dropped).
 __global__ void __launch_bounds__(TR_WARPS * 32, 1)
-update_cells_kernel(const UpdArgs a, const int *nlive, const int *nsub, int *passes, int *status,
+update_cells_kernel(const UpdArgs a, const int *nlive, const int *nsub, int *passes, int *last, int *status,
                     const __grid_constant__ CUtensorMap map_t, const __grid_constant__ CUtensorMap map_s)
 {
     extern __shared__ __align__(128) double s_rc[];          // [TR_WARPS][UC_TR_NS][32]
@@ -511,6 +512,7 @@ update_cells_kernel(const UpdArgs a, const int *nlive, const int *nsub, int *pas
             a.soot[cell] = st1;
             a.soot[np + cell] = st2;
             passes[cell] += npass;
+            last[cell] = npass;
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
