@@ -109,3 +109,35 @@ def test_inplace_mixed_matches_twoset(cuda, oracle, monkeypatch, c1):
             out[kind] = (passes, u.download()[2])
     assert out["twoset"][0] == out["inplace"][0]
     assert_rel(out["inplace"][1], out["twoset"][1], 1e-9, 1e-18, "mixed Y in place vs two Y sets")
+
+
+def test_resident_chunk_schedule_from_the_last_call(cuda, oracle, monkeypatch):
+    """By default the tile-resident update lengthens its chunks (up to 32 passes) while the previous
+    call's pass count says more passes are to come; UNICHEM_TR_CHUNK fixes them. The schedule changes
+    only which passes run beyond the stopping one, so two runs of the same call sequence -- a converging
+    update, a second one from its result, and two that run every pass -- agree bit for bit."""
+    tk1, rho1, y1 = random_state(oracle, 2000, 4, 1000, 2000)
+    tk, rho, y = np.tile(tk1, 32), np.tile(rho1, 32), np.tile(y1, (1, 32))
+
+    def run(fixed):
+        monkeypatch.setenv("UNICHEM_UPDATE", "resident")
+        if fixed:
+            monkeypatch.setenv("UNICHEM_TR_CHUNK", "16")
+        else:
+            monkeypatch.delenv("UNICHEM_TR_CHUNK", raising=False)
+        out = []
+        with cuda.UniChem(len(tk)) as u:
+            u.upload(tk, rho, y)
+            for isor, tol in ((100, 1e-3), (100, 1e-3), (100, 0.0), (100, 0.0)):
+                u.ckrates()
+                p = u.solvesp(1e-3, isor=isor, relx=0.99, tol=tol)
+                _, _, yg, s1, _ = u.download()
+                out.append((p, yg, s1))
+        return out
+
+    a, b = run(True), run(False)
+    print("\npasses per call:", [x[0] for x in a])
+    assert a[2][0] == a[3][0] == 101 and 5 <= a[0][0] <= 60
+    for (pa, ya, sa), (pb, yb, sb) in zip(a, b):
+        assert pa == pb
+        assert np.array_equal(ya, yb) and np.array_equal(sa, sb)

@@ -70,6 +70,8 @@ struct uc_ctx {
     int upd_kind = 0;                  // 0: tile-resident (default), 1: Y in place per pass, 2: two Y sets per pass
     int tr_chunk = 16;                 // tile-resident update: passes per chunk (1M cells, 100 passes:
                                        // chunks of 4, 8, 16 took 234, 202, 182 ms)
+    bool tr_adapt = true;              // ... longer while the last call's pass count says more are to come
+                                       // (off when UNICHEM_TR_CHUNK fixes the chunk)
     bool tr_lock = false;              // ... with the warps of a block in step species by species
                                        // (measured on 1M cells, 100 passes: 227 ms in step, 221 ms free)
     double *tr_snap = nullptr, *tr_partial = nullptr;
@@ -580,6 +582,7 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
             break;
         }
         cudaMemcpy(ctx->dP, ctx->hP, sizeof(DevParams), cudaMemcpyHostToDevice);
+        cudaMemset(ctx->passes, 0, sizeof(int));        // no previous update: fixed chunks on the first call
         cudaMemcpy(ctx->dTab, tab.data(), PAIRTAB_BYTES, cudaMemcpyHostToDevice);
         cudaMemcpy(ctx->dTabM, tabm.data(), PAIRTABM_BYTES, cudaMemcpyHostToDevice);
         cudaMemset(ctx->status, 0, sizeof(int));
@@ -611,7 +614,10 @@ extern "C" int uc_init(const uc_inputs *in, int ncell, int device, uc_ctx **out)
             if (!strcmp(k, "twoset")) { ctx->upd_ip = 0; ctx->upd_kind = 2; }
             else if (!strcmp(k, "inplace")) ctx->upd_kind = 1;
         }
-        if (const char *k = getenv("UNICHEM_TR_CHUNK")) ctx->tr_chunk = std::max(1, std::min(TR_CHUNK_MAX, atoi(k)));
+        if (const char *k = getenv("UNICHEM_TR_CHUNK")) {
+            ctx->tr_chunk = std::max(1, std::min(TR_CHUNK_MAX, atoi(k)));
+            ctx->tr_adapt = false;
+        }
         // shape of the batched integration until uc_integrate_tune picks one: 16 or 8 (persistent kernel), 3 (rounds).
         // By default the rounds form once every SM has four tiles or more (1M cells: 4.1 s per step against 7.4 s
         // for the persistent kernel; 333 cells: the persistent kernel is faster)
@@ -1058,7 +1064,8 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
     int slot;
     if (ctx->upd_kind == 0 && ctx->rc_prec == UC_FP64) {
         const int C = std::min(ctx->tr_chunk, isor);
-        const size_t need = (size_t)std::max(1, C - 1) * TR_SNAP_ROWS * ctx->npad;
+        const int cmax = std::min(ctx->tr_adapt ? TR_CHUNK_MAX : C, isor);     // longest chunk of the call
+        const size_t need = (size_t)std::max(1, cmax - 1) * TR_SNAP_ROWS * ctx->npad;
         if (ctx->tr_snap_cap < need) {
             if (ctx->tr_snap) cudaFree(ctx->tr_snap);
             ctx->tr_snap = nullptr;
@@ -1067,7 +1074,7 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
             ctx->tr_snap_cap = need;
         }
         RET_IF(dalloc(ctx, &ctx->tr_partial, 2 * (size_t)TR_CHUNK_MAX * ctx->nsm));
-        TrArgs t{ctx->tr_snap, ctx->tr_partial, C, ctx->status};
+        TrArgs t{ctx->tr_snap, ctx->tr_partial, C, ctx->status, ctx->tr_adapt ? 1 : 0};
         RET_IF(encode_rc_map(ctx));
         void *targs[] = {&a, &t, &ctx->tr_map[0], &ctx->tr_map[1]};
         prof_begin(ctx, UC_K_UPDATE, slot);

@@ -45,7 +45,7 @@
 namespace uc {
 
 constexpr int TR_WARPS = 3;
-constexpr int TR_CHUNK_MAX = 16;
+constexpr int TR_CHUNK_MAX = 32;
 constexpr int TR_SNAP_ROWS = LSP - 1 + 2;          // Y of species 1..51 and the two soot scalars
 constexpr size_t TR_SLOT_DOUBLES = (size_t)UC_TR_NS * TILE;
 constexpr size_t TR_SMEM = TR_WARPS * TR_SLOT_DOUBLES * sizeof(double);
@@ -60,6 +60,8 @@ struct TrArgs {
     double *partial;       // [2][TR_CHUNK_MAX][gridDim.x]
     int chunk;             // passes per chunk, 1..TR_CHUNK_MAX
     int *status;
+    int adapt;             // longer chunks (up to TR_CHUNK_MAX) while the previous call's count says that
+                           // many passes are still to come
 };
 
 #ifndef UC_TR_WAIT_TRIES
@@ -169,7 +171,7 @@ update_tr_kernel(const UpdArgs a, const TrArgs t, const __grid_constant__ CUtens
     __shared__ double s_cell[TR_WARPS][8][TILE];            // SOUR 1..6 and the two soot values of the old level
     __shared__ __align__(8) uint64_t s_bar[TR_WARPS];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_stop;
+    __shared__ int s_stop, s_pred;
     const DevParams &P = *a.P;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const size_t np = a.npad;
@@ -182,6 +184,10 @@ update_tr_kernel(const UpdArgs a, const TrArgs t, const __grid_constant__ CUtens
     }
     if (threadIdx.x < TR_WARPS) mbar_init(&s_bar[threadIdx.x], 1);
     for (int k = threadIdx.x; k < LSP; k += blockDim.x) s_wm[k] = P.WM[k];
+    // the pass count of the previous call (*a.passes, written by block 0 at the end: every block reads it
+    // before the first grid barrier). Only the chunk schedule depends on it, not the result: a chunk runs
+    // passes beyond the stopping pass at most, whose Y is dropped for the snapshot of the stopping pass.
+    if (threadIdx.x == 0) s_pred = t.adapt ? __ldcg(a.passes) : 0;
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -196,7 +202,9 @@ update_tr_kernel(const UpdArgs a, const TrArgs t, const __grid_constant__ CUtens
 
     int p0 = 0, passes = 0, cpar = 0;
     for (;;) {
-        const int C = min(t.chunk, a.isor - p0);
+        int want = t.chunk;
+        if (s_pred > 0) want = max(want, min(TR_CHUNK_MAX, s_pred - p0 - 4));
+        const int C = min(want, a.isor - p0);
         if (lane < TR_CHUNK_MAX) s_part[w][lane] = 0.0;
         __syncwarp();
         for (int round = 0; round < rounds; ++round) {
