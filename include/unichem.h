@@ -495,8 +495,10 @@ void uc_mlp_destroy(uc_mlp *mlp);
  *    on the context's stream) before reading y or soot.
  *  - It runs the two-Y-set form of the update kernel (8 warps per block, the
  *    kernel UNICHEM_UPDATE=twoset selects for uc_species_update), whose only
- *    scratch is the per-block partial sums; its results are bit for bit those
- *    of uc_species_update.
+ *    scratch is the per-block partial sums; the tile-resident kernel that
+ *    uc_species_update runs by default would need Y snapshots and tensor maps
+ *    of the caller's RC array. Same pass count as uc_species_update, Y within
+ *    1e-12 relative (bit for bit against UNICHEM_UPDATE=twoset).
  */
 #define UC_NOALLOC_MAX_BLOCKS 1024
 typedef struct {
