@@ -71,7 +71,8 @@ struct uc_ctx {
     int tr_chunk = 16;                 // tile-resident update: passes per chunk (1M cells, 100 passes:
                                        // chunks of 4, 8, 16 took 234, 202, 182 ms)
     bool tr_adapt = true;              // ... longer while the last call's pass count says more are to come
-                                       // (off when UNICHEM_TR_CHUNK fixes the chunk)
+                                       // (off when UNICHEM_TR_CHUNK fixes the chunk, or when the snapshots
+    bool tr_adapt_nomem = false;       // of the longer chunks did not fit in device memory)
     bool tr_lock = false;              // ... with the warps of a block in step species by species
                                        // (measured on 1M cells, 100 passes: 227 ms in step, 221 ms free)
     double *tr_snap = nullptr, *tr_partial = nullptr;
@@ -1064,17 +1065,26 @@ extern "C" int uc_species_update(uc_ctx *ctx, double dt, int isor, double relx, 
     int slot;
     if (ctx->upd_kind == 0 && ctx->rc_prec == UC_FP64) {
         const int C = std::min(ctx->tr_chunk, isor);
-        const int cmax = std::min(ctx->tr_adapt ? TR_CHUNK_MAX : C, isor);     // longest chunk of the call
-        const size_t need = (size_t)std::max(1, cmax - 1) * TR_SNAP_ROWS * ctx->npad;
+        // Y snapshots for the longest chunk of the call: TR_CHUNK_MAX passes where the chunk schedule may
+        // lengthen chunks, else C. Where those do not fit in device memory, fixed chunks of C from then on.
+        auto snaps = [&](int c) { return (size_t)std::max(1, std::min(c, isor) - 1) * TR_SNAP_ROWS * ctx->npad; };
+        bool adapt = ctx->tr_adapt && !ctx->tr_adapt_nomem;
+        size_t need = snaps(adapt ? TR_CHUNK_MAX : C);
         if (ctx->tr_snap_cap < need) {
             if (ctx->tr_snap) cudaFree(ctx->tr_snap);
             ctx->tr_snap = nullptr;
             ctx->tr_snap_cap = 0;
-            RET_IF(dalloc(ctx, &ctx->tr_snap, need));
+            if (dalloc(ctx, &ctx->tr_snap, need) != UC_OK && adapt) {
+                cudaGetLastError();           // a failed cudaMalloc leaves the context usable: clear the error
+                ctx->tr_adapt_nomem = true;
+                adapt = false;
+                need = snaps(C);
+            }
+            RET_IF(dalloc(ctx, &ctx->tr_snap, need));   // no-op when the first allocation succeeded
             ctx->tr_snap_cap = need;
         }
         RET_IF(dalloc(ctx, &ctx->tr_partial, 2 * (size_t)TR_CHUNK_MAX * ctx->nsm));
-        TrArgs t{ctx->tr_snap, ctx->tr_partial, C, ctx->status, ctx->tr_adapt ? 1 : 0};
+        TrArgs t{ctx->tr_snap, ctx->tr_partial, C, ctx->status, adapt ? 1 : 0};
         RET_IF(encode_rc_map(ctx));
         void *targs[] = {&a, &t, &ctx->tr_map[0], &ctx->tr_map[1]};
         prof_begin(ctx, UC_K_UPDATE, slot);
