@@ -64,3 +64,22 @@ def test_one_substep_is_the_reference_chain(oracle, c3):
         yn, sn, p = oracle.species_update(rho[c:c + 1], f.y[:, c:c + 1], rc, sour, DT, spnorm=51.0)
         assert np.array_equal(yn[:, 0], y1[:, j]) and np.array_equal(sn[:, 0], s1[:, j])
         assert min(p, 100) == passes[j]
+
+
+def test_cells_integrate_independently_of_their_order(oracle, c3):
+    """The batched integration advances each cell as a one-cell field: a cell's result does not depend on
+    the other cells of the batch or on their order. The device's rounds form relies on this when it
+    gathers the cells in sub-step order and re-orders them between rounds."""
+    f, tk, rho, pnd = c3
+    q = oracle.omega(tk, rho, f.y)[0]
+    ns, _ = oracle.nsub(rho, f.y, q, DT)
+    a = oracle.integrate(tk, rho, f.y, pnd, ns, DT)
+    perm = np.random.default_rng(5).permutation(len(tk))
+    b = oracle.integrate(tk[perm], rho[perm], f.y[:, perm], pnd[perm], ns[perm], DT)
+    inv = np.argsort(perm)
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v[..., inv])
+    half = perm[: len(perm) // 2]                     # and a cell alone in a smaller batch
+    c = oracle.integrate(tk[half], rho[half], f.y[:, half], pnd[half], ns[half], DT)
+    for u, v in zip(a, c):
+        assert np.array_equal(u[..., half], v)
